@@ -1,0 +1,314 @@
+#!/usr/bin/env python
+"""Benchmark of the unsplit Godunov update on the 2D shear-layer workload.
+
+Workload (the headline configuration): 2D unsplit CTU hydro, Kelvin-Helmholtz
+shear layer on a 1024 x 1024 periodic unit square, gamma = 5/3, HLLC,
+MUSCL-Hancock with the van Leer limiter, CFL 0.3, FP64 (bit-faithful path).
+A step is one CFL-limited unsplit step of the whole grid (ghost fill, CFL dt,
+fused update). Metric: cell-updates/s (interior cells x steps / time).
+
+  value      device time of K steps with the state resident in HBM, L2 flushed
+             before every step (the 84 MB double-buffered state fits in L2);
+  e2e        the same steps through the C ABI with the state uploaded from
+             pinned host memory and downloaded back every step;
+  roofline   the fused step kernel's algorithmic HBM bytes (80 B per cell
+             update: 5 FP64 fields read + written) over its CUDA-event time;
+  cpu_baseline  the DRAGON reference itself (oracle/_ref, DistGrid2D with
+             core_count = host threads) on a bounded number of full steps.
+
+``--impl reference`` times only the reference on the host cores and prints its
+own line. Multi-GPU (torchrun): every rank advances its own 1024^2 grid
+(replicas, weak scaling), timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N = 1024
+CELL_BYTES = 80  # 5 FP64 primitive fields read + written per cell update
+METRIC = "cell-updates/s (2D unsplit CTU hydro, FP64)"
+WORKLOAD = "kelvin_helmholtz_2d_1024sq_hllc_vanleer_cfl0.3_periodic"
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_from_profile():
+    p = os.path.join(ROOT, "profiles", "step2d_hydro_kh.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("dram_bytes_per_launch_full")
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower() == "active":
+                    reasons.add(nm)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def reference_baseline(steps: int, warmup: int, budget_s: float | None = None):
+    """Times the DRAGON reference (oracle/_ref) on the host: DistGrid2D with
+    core_count = host threads, full 1024^2 steps. With budget_s, runs as many
+    steps as fit (at least one)."""
+    from dragon_b200 import problems
+    from oracle import refgrid
+    if not refgrid.available("hydro"):
+        return None, "reference library not built"
+    cores = os.cpu_count() or 1
+    w0, dx, dy = problems.kelvin_helmholtz_2d(N, ghosts=3)
+    R = refgrid.RefGrid(2, (N, N), (dx, dy), ghosts=3, dist=True, riemann=2, limiter=2, cfl=1, core_count=cores)
+    R.set_prim(w0)
+    R.set_boundary([(4, 63, 1, None)])
+    for _ in range(warmup):
+        R.step_cfl()
+    t0 = time.perf_counter()
+    done = 0
+    while True:
+        R.step_cfl()
+        done += 1
+        el = time.perf_counter() - t0
+        if budget_s is None and done >= steps:
+            break
+        if budget_s is not None and (el >= budget_s or done >= steps):
+            break
+    el = time.perf_counter() - t0
+    R.close()
+    return {"value": N * N * done / el, "unit": "cell-updates/s", "cores": cores, "kind": "reference",
+            "sample": f"{done} full 1024x1024 steps of the reference DistGrid2D (core_count={cores}), "
+                      f"{el:.1f} s wall"}, None
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    base = {"metric": METRIC, "unit": "cell-updates/s", "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "grid": [N, N], "parallelism": "host threads"}}
+    cb, why = reference_baseline(args.steps, args.warmup)
+    if cb is None:
+        base["unavailable"] = why
+        print(json.dumps(base))
+        return
+    base["value"] = cb["value"]
+    base["ms_per_step"] = 1e3 * N * N / cb["value"]
+    base["cpu_baseline"] = cb
+    base["e2e"] = {"value": cb["value"], "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    print(json.dumps(base))
+
+
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+
+    import dragon_b200 as dg
+    from dragon_b200 import _lib, problems
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    cfg = dg.Config(riemann=dg.RIEMANN_HLLC, limiter=dg.LIMITER_VANLEER, cfl=dg.CFL_ADD,
+                    precision=dg.PREC_MIXED if args.mixed else dg.PREC_FP64)
+    w0, dx, dy = problems.kelvin_helmholtz_2d(N, ghosts=2, seed=1234 + rank)
+    G = dg.Grid2D(N, N, dx, dy, ghosts=2, config=cfg)
+    G.w[...] = w0
+    G.boundary = dg.Periodic()
+    L = G._lib
+    h = G._h
+    stream = torch.cuda.ExternalStream(L.dragon_gpu_stream(h), device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
+
+    # warm-up (also uploads the state and compiles nothing: kernels are prebuilt)
+    G.advance_steps(max(args.warmup, 1))
+    torch.cuda.synchronize()
+
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+
+    # ---- value: K steps, state resident in HBM, L2 flushed before each step
+    L.dragon_gpu_profile_enable(h, 1)
+    L.dragon_gpu_profile_read(h, None, None, 1)
+    launches0 = G.launch_count()
+    step_ms = []
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        t_wall = time.perf_counter()
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            st = _lib.AdvanceStats()
+            _lib.check(L.dragon_gpu_advance_steps(h, 1, __import__("ctypes").byref(st)))
+            e1.record(stream)
+            step_ms.append((e0, e1))
+        torch.cuda.synchronize()
+        t_wall = time.perf_counter() - t_wall
+    barrier()
+    ms = sum(a.elapsed_time(b) for a, b in step_ms)
+    launches = G.launch_count() - launches0
+    kms = __import__("ctypes").c_double()
+    kn = __import__("ctypes").c_longlong()
+    L.dragon_gpu_profile_read(h, __import__("ctypes").byref(kms), __import__("ctypes").byref(kn), 1)
+    L.dragon_gpu_profile_enable(h, 0)
+    if ws > 1:
+        t = torch.tensor([ms, kms.value], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, kmax = t[0].item(), t[1].item()
+    else:
+        kmax = kms.value
+    ms_per_step = ms / args.steps
+    value = ws * N * N * args.steps / (ms / 1e3)
+
+    # ---- e2e: through the C ABI from pinned host memory, every step
+    host_in = torch.from_numpy(G.w.copy()).pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    pin_in = host_in.numpy()
+    pin_out = host_out.numpy()
+    dptr = _lib.c_double_p
+    e2e_steps = max(1, min(args.steps, 10))
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        _lib.check(L.dragon_gpu_upload_prim(h, pin_in.ctypes.data_as(dptr)))
+        _lib.check(L.dragon_gpu_advance_steps(h, 1, None))
+        _lib.check(L.dragon_gpu_download_prim(h, pin_out.ctypes.data_as(dptr)))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if ws > 1:
+        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = t.item()
+    e2e_value = ws * N * N * e2e_steps / (e2e_ms / 1e3)
+    bytes_step = pin_in.nbytes
+
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        k_avg_ms = kms.value / max(1, kn.value)
+        achieved = N * N * CELL_BYTES / (k_avg_ms / 1e3) / 1e9 if k_avg_ms > 0 else None
+        traffic = traffic_from_profile()
+        clocks = clk.summary()
+        line = {
+            "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if not args.mixed else "f32/f64",
+            "data": "synthetic (seeded KH shear layer, numpy PCG64 seed 1234 + rank)",
+            "config": {"workload": WORKLOAD, "grid": [N, N], "solver": "HLLC", "limiter": "vanLeer",
+                       "precision": "mixed" if args.mixed else "fp64", "l2": "flushed before every timed step",
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
+            "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": bytes_step,
+                    "d2h_bytes_per_step": bytes_step, "steps": e2e_steps},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                         "kernel": "k_step2d_hydro", "kernel_ms_avg": k_avg_ms,
+                         "bytes_per_cell": CELL_BYTES, "peak_source": peak_kind},
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "wall_s_timed": t_wall,
+        }
+        if not args.no_cpu_baseline:
+            cb, why = reference_baseline(1000, 0, budget_s=args.cpu_budget)
+            line["cpu_baseline"] = cb if cb else {"unavailable": why}
+        print(json.dumps(line))
+    G.close()
+    if ws > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="dragon_b200", choices=["dragon_b200", "reference"])
+    ap.add_argument("--mixed", action="store_true", help="mixed FP32/FP64 path")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

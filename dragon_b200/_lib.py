@@ -1,0 +1,152 @@
+"""ctypes binding of the C ABI in include/dragon_gpu.h.
+
+The shared library is built in-tree (dragon_b200/libdragon_gpu.so) by
+``dragon_b200.build.build()``. There is no CPU fallback: importing the binding
+without the library, or calling into it without a CUDA device, raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libdragon_gpu.so")
+
+c_double_p = ctypes.POINTER(ctypes.c_double)
+
+
+class DragonConfig(ctypes.Structure):
+    """dragon_config (include/dragon_gpu.h)."""
+
+    _fields_ = [
+        ("mhd", ctypes.c_int),
+        ("riemann", ctypes.c_int),
+        ("limiter", ctypes.c_int),
+        ("cfl", ctypes.c_int),
+        ("ct_energy", ctypes.c_int),
+        ("exact_max_iters", ctypes.c_int),
+        ("exact_tol", ctypes.c_double),
+        ("cfl_coeff", ctypes.c_double),
+        ("timestep_tol", ctypes.c_double),
+        ("precision", ctypes.c_int),
+        ("reserved", ctypes.c_int * 7),
+    ]
+
+
+class BCDesc(ctypes.Structure):
+    """dragon_bc_desc."""
+
+    _fields_ = [
+        ("type", ctypes.c_int),
+        ("faces", ctypes.c_int),
+        ("corners", ctypes.c_int),
+        ("reserved", ctypes.c_int),
+        ("state", ctypes.c_double * 8),
+    ]
+
+
+class StepStatus(ctypes.Structure):
+    """dragon_step_status."""
+
+    _fields_ = [
+        ("code", ctypes.c_int),
+        ("stage", ctypes.c_int),
+        ("cell", ctypes.c_longlong),
+        ("dt", ctypes.c_double),
+    ]
+
+
+class AdvanceStats(ctypes.Structure):
+    """dragon_advance_stats."""
+
+    _fields_ = [
+        ("steps", ctypes.c_int),
+        ("retries", ctypes.c_int),
+        ("last_dt", ctypes.c_double),
+        ("time_advanced", ctypes.c_double),
+        ("pivots_exact", ctypes.c_ulonglong),
+        ("hlld_to_hlle", ctypes.c_ulonglong),
+        ("newton_iters", ctypes.c_ulonglong),
+        ("exact_calls", ctypes.c_ulonglong),
+        ("trrs", ctypes.c_ulonglong),
+        ("muscl_first_order", ctypes.c_ulonglong),
+        ("failure", StepStatus),
+    ]
+
+
+# Every symbol include/dragon_gpu.h declares, with its ctypes signature.
+SIGNATURES = {
+    "dragon_gpu_default_config": (None, [ctypes.POINTER(DragonConfig), ctypes.c_int]),
+    "dragon_gpu_grid_create": (
+        ctypes.c_int,
+        [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+         ctypes.c_double, ctypes.c_int, ctypes.POINTER(DragonConfig), ctypes.POINTER(ctypes.c_void_p)],
+    ),
+    "dragon_gpu_grid_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "dragon_gpu_grid_info": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+         ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
+    ),
+    "dragon_gpu_prim_count": (ctypes.c_size_t, [ctypes.c_void_p]),
+    "dragon_gpu_faceB_count": (ctypes.c_size_t, [ctypes.c_void_p]),
+    "dragon_gpu_upload_prim": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
+    "dragon_gpu_download_prim": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
+    "dragon_gpu_upload_faceB": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
+    "dragon_gpu_download_faceB": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
+    "dragon_gpu_set_boundary": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(BCDesc), ctypes.c_int]),
+    "dragon_gpu_apply_boundary": (ctypes.c_int, [ctypes.c_void_p]),
+    "dragon_gpu_initialize_B_fields": (ctypes.c_int, [ctypes.c_void_p]),
+    "dragon_gpu_cfl_time": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
+    "dragon_gpu_unsplit_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(StepStatus)]),
+    "dragon_gpu_advance": (
+        ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.POINTER(AdvanceStats)]),
+    "dragon_gpu_advance_steps": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(AdvanceStats)]),
+    "dragon_gpu_stream": (ctypes.c_void_p, [ctypes.c_void_p]),
+    "dragon_gpu_device_state": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_longlong),
+         ctypes.POINTER(ctypes.c_longlong)],
+    ),
+    "dragon_gpu_launch_count": (ctypes.c_ulonglong, [ctypes.c_void_p]),
+    "dragon_gpu_profile_enable": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "dragon_gpu_profile_read": (
+        ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong),
+                       ctypes.c_int]),
+    "dragon_gpu_last_error": (ctypes.c_char_p, []),
+}
+
+_lib = None
+
+
+def load(path: str | None = None) -> ctypes.CDLL:
+    """Loads the in-tree C-ABI library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(
+            f"{p} is missing: build the CUDA extension first (python -c 'import __graft_entry__ as g; g.build()')")
+    lib = ctypes.CDLL(p)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+class DragonGPUError(RuntimeError):
+    """A C-ABI call returned a non-zero status."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def check(rc: int) -> None:
+    if rc != 0:
+        msg = _lib.dragon_gpu_last_error().decode() if _lib is not None else "unknown"
+        raise DragonGPUError(rc, msg)

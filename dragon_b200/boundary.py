@@ -1,0 +1,205 @@
+"""Ghost-fill API mirroring DRAGON's Boundary namespace.
+
+Same names, arguments and composition rules as the reference
+(DRAGON/Boundary/Boundary.hpp:119-229, BoundaryList.hpp:22-128): elements
+combine with ``+`` into a BoundaryList applied in order, after an implicit
+Outflow over every face no element covers. The list is compiled into
+dragon_bc_desc records and executed on the device.
+
+Example (the reference's ``Boundary::Reflective("X") + Boundary::Periodic("YZ")``)::
+
+    grid.boundary = Reflective("X") + Periodic("YZ")
+"""
+from __future__ import annotations
+
+from typing import Iterable, Sequence
+
+# Face bits (Boundary.hpp:139-149)
+X_negative = 1 << 0
+X_positive = 1 << 1
+X = X_negative | X_positive
+Y_negative = 1 << 2
+Y_positive = 1 << 3
+Y = Y_negative | Y_positive
+Z_negative = 1 << 4
+Z_positive = 1 << 5
+Z = Z_negative | Z_positive
+
+OUTFLOW, OUTFLOW_GATED, FIXED, REFLECTIVE, PERIODIC, IGNORE = range(6)
+
+
+def face_mask(s: str) -> int:
+    """Boundary::face_mask (GhostFill.cpp:14-48): "X", "X-", "YZ+", "L/R/U/D"."""
+    mask = 0
+    s = s + " "
+    for cur, nxt in zip(s, s[1:]):
+        c = cur.upper()
+        if c in "XYZ":
+            neg, pos, both = {"X": (X_negative, X_positive, X), "Y": (Y_negative, Y_positive, Y),
+                              "Z": (Z_negative, Z_positive, Z)}[c]
+            mask |= pos if nxt == "+" else (neg if nxt == "-" else both)
+        elif c == "L":
+            mask |= X_negative
+        elif c == "R":
+            mask |= X_positive
+        elif c == "U":
+            mask |= Y_positive
+        elif c == "D":
+            mask |= Y_negative
+    return mask
+
+
+def _faces(f) -> int:
+    return face_mask(f) if isinstance(f, str) else int(f)
+
+
+class GhostFill:
+    """A boundary element (GhostFill.hpp:16-30): face mask + corner flag."""
+
+    kind = IGNORE
+
+    def __init__(self, faces=X | Y | Z, corner_ghosts: bool = True):
+        self.faces = _faces(faces)
+        self.corners = bool(corner_ghosts)
+
+    def get_faces(self) -> int:
+        return self.faces
+
+    def state(self) -> Sequence[float]:
+        return ()
+
+    def __add__(self, other):
+        return BoundaryList(self) + other
+
+    def __radd__(self, other):
+        if other == 0:
+            return BoundaryList(self)
+        return NotImplemented
+
+    def __repr__(self):
+        return f"{type(self).__name__}(faces={self.faces}, corners={self.corners})"
+
+
+class Outflow(GhostFill):
+    """Outflow (Outflow.cpp): ghosts copy the nearest interior cell; Gated
+    variants zero inflowing normal velocity."""
+
+    def __init__(self, faces=X | Y | Z, corner_ghosts: bool = True, gated: bool = False):
+        super().__init__(faces, corner_ghosts)
+        self.gated = bool(gated)
+
+    @property
+    def kind(self):
+        return OUTFLOW_GATED if self.gated else OUTFLOW
+
+    @staticmethod
+    def Gated(faces=X | Y | Z, corner_ghosts: bool = True) -> "Outflow":
+        return Outflow(faces, corner_ghosts, True)
+
+
+class Fixed(GhostFill):
+    """Fixed (Fixed.cpp): ghosts take a fixed primitive state
+    (rho, p, vx, vy, vz[, Bx, By, Bz])."""
+
+    kind = FIXED
+
+    def __init__(self, state: Sequence[float], faces=X | Y | Z, corner_ghosts: bool = True):
+        super().__init__(faces, corner_ghosts)
+        st = [float(v) for v in state]
+        if len(st) not in (5, 8):
+            raise ValueError("Fixed state needs 5 (hydro) or 8 (MHD) primitive values")
+        self._state = st + [0.0] * (8 - len(st))
+
+    def state(self):
+        return self._state
+
+
+class Reflective(GhostFill):
+    """Reflective (Reflective.cpp): mirrored cells, normal velocity flipped."""
+
+    kind = REFLECTIVE
+
+
+class Periodic(GhostFill):
+    """Periodic (Periodic.cpp): either face of an axis selects both."""
+
+    kind = PERIODIC
+
+    def __init__(self, faces=X | Y | Z, corner_ghosts: bool = True):
+        super().__init__(faces, corner_ghosts)
+        f = self.faces
+        self.faces = (X if f & X else 0) | (Y if f & Y else 0) | (Z if f & Z else 0)
+
+
+class Ignore(GhostFill):
+    """Ignore (Ignore.cpp): fills nothing but counts as covering its faces."""
+
+    kind = IGNORE
+
+
+class BoundaryList:
+    """Ordered boundary elements plus the implicit Outflow (BoundaryList.hpp)."""
+
+    def __init__(self, *elements: GhostFill):
+        self.elements: list[GhostFill] = []
+        for e in elements:
+            self.append(e)
+
+    def append(self, e) -> None:
+        if isinstance(e, BoundaryList):
+            self.elements.extend(e.elements)
+        elif isinstance(e, GhostFill):
+            self.elements.append(e)
+        else:
+            raise TypeError(f"not a boundary element: {e!r}")
+
+    def prepend(self, e) -> None:
+        if isinstance(e, BoundaryList):
+            self.elements[:0] = e.elements
+        else:
+            self.elements.insert(0, e)
+
+    def clear(self) -> None:
+        self.elements.clear()
+
+    def __add__(self, other):
+        out = BoundaryList(*self.elements)
+        out.append(other)
+        return out
+
+    def __radd__(self, other):
+        out = BoundaryList()
+        out.append(other)
+        out.append(self)
+        return out
+
+    def __iadd__(self, other):
+        self.append(other)
+        return self
+
+    def uncovered_faces(self) -> int:
+        m = X | Y | Z
+        for e in self.elements:
+            m &= ~e.get_faces()
+        return m
+
+    def __iter__(self):
+        return iter(self.elements)
+
+    def __len__(self):
+        return len(self.elements)
+
+    def __repr__(self):
+        return "BoundaryList(" + " + ".join(map(repr, self.elements)) + ")"
+
+
+def as_list(b) -> BoundaryList:
+    if b is None:
+        return BoundaryList()
+    if isinstance(b, BoundaryList):
+        return b
+    if isinstance(b, GhostFill):
+        return BoundaryList(b)
+    if isinstance(b, Iterable):
+        return BoundaryList(*b)
+    raise TypeError(f"cannot use {b!r} as a boundary")

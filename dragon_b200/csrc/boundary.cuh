@@ -1,0 +1,359 @@
+// Ghost fills (DRAGON/Boundary) and the per-step prologue.
+//
+// A boundary list is compiled on the host into BCEntry records in application
+// order: the implicit Outflow over uncovered faces first, then the user's
+// entries (BoundaryList.hpp:79-104). Each entry is applied axis by axis (X, Y,
+// Z) exactly as the reference's GhostFill::apply loops run, because later
+// axes read corner ghosts written by earlier ones; within one axis the two
+// sides touch disjoint cells and run in parallel. MHD face-B ghosts follow the
+// cell ghosts of the same entry (Outflow.cpp:78-117, Reflective.cpp:99-137,
+// Periodic.cpp:311-331, Fixed.cpp:372-406).
+#pragma once
+
+#include "grid.cuh"
+
+namespace dgpu {
+
+enum BCType : int { BC_OUTFLOW = 0, BC_OUTFLOW_GATED = 1, BC_FIXED = 2, BC_REFLECTIVE = 3, BC_PERIODIC = 4, BC_IGNORE = 5 };
+// Face bits (Boundary.hpp:139-149)
+constexpr int FX_NEG = 1, FX_POS = 2, FY_NEG = 4, FY_POS = 8, FZ_NEG = 16, FZ_POS = 32;
+
+struct BCEntry {
+    int type;
+    int faces;
+    int corners;
+    int pad;
+    double state[8];   // Fixed: primitive state rho, p, vx, vy, vz, Bx, By, Bz
+};
+
+struct PrologueArgs {
+    double dx, dy, dz;
+    double cfl_coeff;
+    double tol;
+    int cfl;
+    int slot_in;        // interior max written by the previous step (or the initial CFL pass)
+    int slot_out;       // slot the coming step accumulates into (zeroed here)
+    int bookkeeping;    // account for the previous step (advance loop)
+    int apply_bc;       // fill ghosts
+    int compute_dt;     // compute t1 from the CFL limit
+    int nbc;
+};
+
+// ---------------------------------------------------------------------------
+// Cell ghosts of one entry along one axis. The axis index a in 0..dim-1; the
+// remaining axes are transverse. Thread-strided over (side, transverse point,
+// ghost layer).
+template <bool MHD>
+__device__ void bc_cells_axis(const Geo& G, double* __restrict__ w, const BCEntry& e, int a) {
+    const int dim = G.dim, ng = G.g;
+    const int na = G.n[a];
+    const bool negOn = e.faces & (1 << (2 * a)), posOn = e.faces & (1 << (2 * a + 1));
+    const bool periodic = e.type == BC_PERIODIC;
+    if (e.type == BC_IGNORE) return;
+    if (!negOn && !posOn) return;
+    // transverse ranges
+    int t0[2] = {0, 0}, tn[2] = {1, 1};
+    int ta[2] = {-1, -1};
+    int nt = 0;
+    for (int b = 0; b < dim; b++) {
+        if (b == a) continue;
+        ta[nt] = b;
+        // 1D grids have no corners; 2D/3D extend transverse ranges into ghosts when corners are on.
+        t0[nt] = e.corners ? -ng : 0;
+        tn[nt] = e.corners ? G.n[b] + ng : G.n[b];
+        nt++;
+    }
+    const long long span0 = tn[0] - t0[0], span1 = tn[1] - t0[1];
+    const long long per_side = span0 * span1 * ng;
+    const long long total = 2 * per_side;
+    for (long long t = threadIdx.x; t < total; t += blockDim.x) {
+        const int side = (int)(t / per_side);  // 0 negative, 1 positive
+        long long r = t - side * per_side;
+        const int gl = (int)(r % ng) + 1;
+        r /= ng;
+        const int c1 = (int)(r % span1) + t0[1];
+        const int c0 = (int)(r / span1) + t0[0];
+        if (side == 0 && !negOn) continue;
+        if (side == 1 && !posOn) continue;
+        int dst[3] = {0, 0, 0}, src[3] = {0, 0, 0};
+        if (nt > 0) { dst[ta[0]] = src[ta[0]] = c0; }
+        if (nt > 1) { dst[ta[1]] = src[ta[1]] = c1; }
+        int sa;
+        if (side == 0) {
+            dst[a] = -gl;
+            if (e.type == BC_REFLECTIVE) sa = gl - 1;
+            else if (periodic) sa = na - gl;
+            else sa = 0;
+        } else {
+            dst[a] = na - 1 + gl;
+            if (e.type == BC_REFLECTIVE) sa = na - gl;
+            else if (periodic) sa = gl - 1;
+            else sa = na - 1;
+        }
+        src[a] = sa;
+        long long md, ms;
+        if (dim == 1) { md = gidx1(G, dst[0]); ms = gidx1(G, src[0]); }
+        else if (dim == 2) { md = gidx2(G, dst[0], dst[1]); ms = gidx2(G, src[0], src[1]); }
+        else { md = gidx3(G, dst[0], dst[1], dst[2]); ms = gidx3(G, src[0], src[1], src[2]); }
+        Prim<double> v;
+        if (e.type == BC_FIXED) {
+            v = Prim<double>{e.state[0], e.state[1], e.state[2], e.state[3], e.state[4],
+                             e.state[5], e.state[6], e.state[7]};
+        } else {
+            v = load_prim<MHD>(w, G.plane, ms);
+        }
+        double* vel = (a == 0) ? &v.vx : (a == 1 ? &v.vy : &v.vz);
+        if (e.type == BC_OUTFLOW_GATED) {
+            // Outflow.cpp:26,33,50,58: kill inflow through the face
+            if (side == 0 && *vel > 0) *vel = 0;
+            if (side == 1 && *vel < 0) *vel = 0;
+        } else if (e.type == BC_REFLECTIVE) {
+            *vel *= -1;
+            if constexpr (MHD) {
+                v.Bx *= -1; v.By *= -1; v.Bz *= -1;
+                double* bn = (a == 0) ? &v.Bx : (a == 1 ? &v.By : &v.Bz);
+                *bn *= -1;
+            }
+        }
+        store_prim<MHD>(w, G.plane, md, v);
+    }
+}
+
+// Face-B ghosts of one entry along one axis. FG is the face geometry (n+1 per
+// axis); n_cells the cell extents. One thread per (side, transverse point)
+// runs the sequential ghost-layer recurrence.
+__device__ inline void bc_faces_axis(const Geo& FG, const int* ncell, double* __restrict__ B, const BCEntry& e, int a) {
+    const int dim = FG.dim, ng = FG.g;
+    const int na = ncell[a];
+    const bool negOn = e.faces & (1 << (2 * a)), posOn = e.faces & (1 << (2 * a + 1));
+    if (e.type == BC_IGNORE) return;
+    if (!negOn && !posOn) return;
+    int t0[2] = {0, 0}, tn[2] = {0, 0};
+    int ta[2] = {-1, -1};
+    int nt = 0;
+    for (int b = 0; b < dim; b++) {
+        if (b == a) continue;
+        ta[nt] = b;
+        t0[nt] = e.corners ? -ng : 0;
+        tn[nt] = e.corners ? ncell[b] + ng : ncell[b];   // inclusive bound
+        nt++;
+    }
+    const long long span0 = tn[0] - t0[0] + 1, span1 = (nt > 1) ? (tn[1] - t0[1] + 1) : 1;
+    const long long per_side = span0 * span1;
+    const long long plane = FG.plane;
+    auto idx = [&](int ia, int c0, int c1) -> long long {
+        int q[3] = {0, 0, 0};
+        q[a] = ia;
+        q[ta[0]] = c0;
+        if (nt > 1) q[ta[1]] = c1;
+        if (dim == 2) return gidx2(FG, q[0], q[1]);
+        return gidx3(FG, q[0], q[1], q[2]);
+    };
+    const int tr0 = (a == 0) ? 1 : 0;          // first transverse component
+    const int tr1 = (a == 2) ? 1 : 2;          // second transverse component
+    for (long long t = threadIdx.x; t < 2 * per_side; t += blockDim.x) {
+        const int side = (int)(t / per_side);
+        long long r = t - side * per_side;
+        const int c1 = (int)(r % span1) + t0[1];
+        const int c0 = (int)(r / span1) + t0[0];
+        if (side == 0 && !negOn) continue;
+        if (side == 1 && !posOn) continue;
+        if (e.type == BC_OUTFLOW || e.type == BC_OUTFLOW_GATED) {
+            if (side == 0) {
+                for (int gl = 1; gl <= ng; gl++) {
+                    long long d = idx(-gl, c0, c1), s0 = idx(0, c0, c1);
+                    for (int c = 0; c < 3; c++) B[c * plane + d] = B[c * plane + s0];
+                    B[a * plane + d] = 2 * B[a * plane + idx(-gl + 1, c0, c1)] - B[a * plane + idx(-gl + 2, c0, c1)];
+                }
+            } else {
+                long long bn = idx(na, c0, c1), bm = idx(na - 1, c0, c1);
+                B[tr0 * plane + bn] = B[tr0 * plane + bm];
+                B[tr1 * plane + bn] = B[tr1 * plane + bm];
+                for (int gl = 1; gl <= ng; gl++) {
+                    long long d = idx(na + gl, c0, c1);
+                    for (int c = 0; c < 3; c++) B[c * plane + d] = B[c * plane + bn];
+                    B[a * plane + d] = 2 * B[a * plane + idx(na + gl - 1, c0, c1)] - B[a * plane + idx(na + gl - 2, c0, c1)];
+                }
+            }
+        } else if (e.type == BC_REFLECTIVE) {
+            if (side == 0) {
+                for (int gl = 1; gl <= ng; gl++) {
+                    long long d = idx(-gl, c0, c1), s = idx(gl - 1, c0, c1);
+                    for (int c = 0; c < 3; c++) B[c * plane + d] = B[c * plane + s] * -1;
+                    B[a * plane + d] = B[a * plane + idx(gl, c0, c1)];
+                }
+            } else {
+                long long bn = idx(na, c0, c1), bm = idx(na - 1, c0, c1);
+                for (int c = 0; c < 3; c++) B[c * plane + bn] = B[c * plane + bm] * -1;
+                for (int gl = 1; gl <= ng; gl++) {
+                    long long d = idx(na + gl, c0, c1), s = idx(na - gl - 1, c0, c1);
+                    for (int c = 0; c < 3; c++) B[c * plane + d] = B[c * plane + s] * -1;
+                    B[a * plane + d] = B[a * plane + idx(na - gl, c0, c1)];
+                }
+            }
+        } else if (e.type == BC_PERIODIC) {
+            for (int gl = 1; gl <= ng; gl++) {
+                long long d, s;
+                if (side == 0) { d = idx(-gl, c0, c1); s = idx(na - gl, c0, c1); }
+                else { d = idx(na - 1 + gl, c0, c1); s = idx(gl - 1, c0, c1); }
+                for (int c = 0; c < 3; c++) B[c * plane + d] = B[c * plane + s];
+            }
+        } else if (e.type == BC_FIXED) {
+            if (side == 0) {
+                B[a * plane + idx(0, c0, c1)] = e.state[5 + a];
+                for (int gl = 1; gl <= ng; gl++) {
+                    long long d = idx(-gl, c0, c1);
+                    for (int c = 0; c < 3; c++) B[c * plane + d] = e.state[5 + c];
+                }
+            } else {
+                for (int gl = 0; gl < ng; gl++) {
+                    long long d = idx(na + gl, c0, c1);
+                    for (int c = 0; c < 3; c++) B[c * plane + d] = e.state[5 + c];
+                }
+            }
+        }
+    }
+}
+
+// Per-step prologue, one CTA: step bookkeeping of the previous step, ghost
+// fill, CFL over the ghost ring combined with the interior max the previous
+// step's epilogue produced, and this step's dt (CFL.cpp:188-213).
+template <bool MHD>
+__global__ void __launch_bounds__(1024) k_prologue(Geo G, Geo FG, double* __restrict__ w, double* __restrict__ B,
+                                                   const BCEntry* __restrict__ bcs, StepCtl* ctl, PrologueArgs pa) {
+    __shared__ int s_skip;
+    __shared__ double s_red[32];
+    if (threadIdx.x == 0) {
+        int skip = 0;
+        if (ctl->err) skip = 1;
+        else if (pa.bookkeeping) {
+            if (ctl->done) skip = 1;
+            else {
+                if (ctl->have_prev) {
+                    ctl->remaining -= ctl->t1;
+                    ctl->steps_done += 1;
+                }
+                ctl->have_prev = 1;
+                if (!(ctl->remaining > pa.tol) || (ctl->max_steps > 0 && ctl->steps_done >= ctl->max_steps)) {
+                    ctl->done = 1;
+                    skip = 1;
+                }
+            }
+        }
+        s_skip = skip;
+    }
+    __syncthreads();
+    if (s_skip) return;
+
+    if (pa.apply_bc) {
+        for (int e = 0; e < pa.nbc; e++) {
+            const BCEntry be = bcs[e];
+            for (int a = 0; a < G.dim; a++) {
+                bc_cells_axis<MHD>(G, w, be, a);
+                __syncthreads();
+            }
+            if constexpr (MHD) {
+                if (G.dim >= 2) {
+                    for (int a = 0; a < G.dim; a++) {
+                        bc_faces_axis(FG, G.n, B, be, a);
+                        __syncthreads();
+                    }
+                }
+            }
+        }
+    }
+
+    if (!pa.compute_dt) return;
+    // CFL over the one-cell ghost ring (CFL.cpp:91,110,125: ng = min(1, ghosts)).
+    double m = 0.0;
+    if (G.dim == 1) {
+        if (threadIdx.x < 2) {
+            int i = threadIdx.x == 0 ? -1 : G.n[0];
+            Prim<double> W = load_prim<MHD>(w, G.plane, gidx1(G, i));
+            m = cfl_speed_1d<MHD>(W);
+        }
+    } else if (G.dim == 2) {
+        const int nx = G.n[0], ny = G.n[1];
+        const long long rows = 2LL * (ny + 2), total = rows + 2LL * nx;
+        for (long long r = threadIdx.x; r < total; r += blockDim.x) {
+            int i, j;
+            if (r < ny + 2) { i = -1; j = (int)r - 1; }
+            else if (r < rows) { i = nx; j = (int)(r - (ny + 2)) - 1; }
+            else {
+                long long q = r - rows;
+                if (q < nx) { i = (int)q; j = -1; }
+                else { i = (int)(q - nx); j = ny; }
+            }
+            Prim<double> W = load_prim<MHD>(w, G.plane, gidx2(G, i, j));
+            m = speed_max(m, cfl_speed<MHD>(W, pa.cfl, pa.dx, pa.dy, 0.0));
+        }
+    } else {
+        const int nx = G.n[0], ny = G.n[1], nz = G.n[2];
+        const long long ey = ny + 2, ez = nz + 2;
+        // ring = two i-slabs, then two j-strips per interior i, then two k-cells per interior (i,j)
+        const long long nA = 2 * ey * ez, nB = (long long)nx * 2 * ez, nC = (long long)nx * ny * 2;
+        for (long long r = threadIdx.x; r < nA + nB + nC; r += blockDim.x) {
+            int i, j, k;
+            if (r < nA) {
+                i = (r < ey * ez) ? -1 : nx;
+                long long q = r % (ey * ez);
+                j = (int)(q / ez) - 1;
+                k = (int)(q % ez) - 1;
+            } else if (r < nA + nB) {
+                long long q = r - nA;
+                i = (int)(q / (2 * ez));
+                long long s = q % (2 * ez);
+                j = (s < ez) ? -1 : ny;
+                k = (int)(s % ez) - 1;
+            } else {
+                long long q = r - nA - nB;
+                i = (int)(q / (2LL * ny));
+                long long s = q % (2LL * ny);
+                j = (int)(s >> 1);
+                k = (s & 1) ? nz : -1;
+            }
+            Prim<double> W = load_prim<MHD>(w, G.plane, gidx3(G, i, j, k));
+            m = speed_max(m, cfl_speed<MHD>(W, pa.cfl, pa.dx, pa.dy, pa.dz));
+        }
+    }
+    m = block_max(m, s_red);
+    if (threadIdx.x == 0) {
+        double inner = __longlong_as_double((long long)ctl->vmax[pa.slot_in]);
+        double maxs = speed_max(inner, m);
+        ctl->max_speed = maxs;
+        ctl->vmax[pa.slot_out] = 0ull;
+        if (ctl->check_cfl) {
+            if (maxs <= 0) {
+                record_error(ctl, ST_CFL_ZERO, 0);
+            } else {
+                double cfl_dt = (G.dim == 1) ? pa.cfl_coeff * pa.dx / maxs : pa.cfl_coeff / maxs;
+                ctl->t1 = smin(ctl->remaining, cfl_dt);
+            }
+        } else {
+            ctl->t1 = ctl->remaining;
+        }
+    }
+}
+
+// Interior CFL maximum over all interior cells (multi-CTA), accumulated into
+// ctl->vmax[slot]. Used before the first step of an advance and by cfl_time.
+template <bool MHD>
+__global__ void k_interior_cfl(Geo G, const double* __restrict__ w, StepCtl* ctl, int slot, int cfl, double dx,
+                               double dy, double dz) {
+    __shared__ double s_red[32];
+    const long long nx = G.n[0], ny = G.n[1], nz = G.n[2];
+    const long long total = nx * ny * nz;
+    double m = 0.0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        long long mi;
+        if (G.dim == 1) mi = gidx1(G, (int)t);
+        else if (G.dim == 2) mi = gidx2(G, (int)(t / ny), (int)(t % ny));
+        else mi = gidx3(G, (int)(t / (ny * nz)), (int)((t / nz) % ny), (int)(t % nz));
+        Prim<double> W = load_prim<MHD>(w, G.plane, mi);
+        m = speed_max(m, grid_cfl_speed<MHD>(W, G.dim, cfl, dx, dy, dz));
+    }
+    m = block_max(m, s_red);
+    if (threadIdx.x == 0) atomic_max_speed(&ctl->vmax[slot], m);
+}
+
+}  // namespace dgpu

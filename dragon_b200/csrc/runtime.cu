@@ -1,0 +1,692 @@
+// Host runtime behind include/dragon_gpu.h: grid handles, host<->device
+// transfers in the reference's AoS order, the boundary program, and the
+// device-resident advance loop (Grid::advance_unsplit, CFL.cpp:188-213).
+//
+// The advance loop enqueues batches of (prologue, step) kernel pairs without
+// host synchronisation. The prologue does the previous step's bookkeeping
+// (dt -= t1), the ghost fill and the CFL dt; the step kernel reads t1 from the
+// control block. A failed step raises the device error word, after which every
+// later kernel of the batch returns at once, so the failed step's input buffer
+// is still intact; the host then halves dt and retries exactly like the
+// reference's catch block (CFL.cpp:194-209).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/dragon_gpu.h"
+#include "boundary.cuh"
+#include "step_hydro.cuh"
+#include "step_mhd.cuh"
+
+using namespace dgpu;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define CK(x)                                                                                  \
+    do {                                                                                       \
+        cudaError_t e_ = (x);                                                                  \
+        if (e_ != cudaSuccess)                                                                 \
+            return fail(DRAGON_GPU_ECUDA, std::string(#x) + ": " + cudaGetErrorString(e_));   \
+    } while (0)
+
+constexpr int kBatch = 64;
+constexpr int k2dTI = 8, k2dTJ = 32, k2dNT = 256;
+constexpr int k1dTS = 128;
+
+long long round_up(long long a, long long b) { return (a + b - 1) / b * b; }
+
+Geo make_geo(int dim, const int* n, int g) {
+    Geo G;
+    G.dim = dim;
+    G.g = g;
+    for (int a = 0; a < 3; a++) {
+        G.n[a] = a < dim ? n[a] : 1;
+        G.ext[a] = a < dim ? n[a] + 2 * g : 1;
+    }
+    if (dim == 1) {
+        G.pitch = 1;
+        G.pitch2 = 1;
+        G.plane = round_up(G.ext[0], 32);
+    } else if (dim == 2) {
+        G.pitch = round_up(G.ext[1], 32);
+        G.pitch2 = G.pitch;
+        G.plane = (long long)G.ext[0] * G.pitch;
+    } else {
+        G.pitch = round_up(G.ext[2], 32);
+        G.pitch2 = (long long)G.ext[1] * G.pitch;
+        G.plane = (long long)G.ext[0] * G.pitch2;
+    }
+    return G;
+}
+
+// AoS (reference order, dense padded) <-> SoA (device planes).
+__global__ void k_aos_to_soa(const double* __restrict__ aos, double* __restrict__ soa, Geo G, int nf) {
+    const long long ey = G.ext[1], ez = G.ext[2];
+    const long long total = (long long)G.ext[0] * ey * ez;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        const long long k = t % ez, j = (t / ez) % ey, i = t / (ey * ez);
+        long long m;
+        if (G.dim == 1) m = i;
+        else if (G.dim == 2) m = i * G.pitch + j;
+        else m = i * G.pitch2 + j * G.pitch + k;
+        for (int f = 0; f < nf; f++) soa[f * G.plane + m] = aos[t * nf + f];
+    }
+}
+__global__ void k_soa_to_aos(const double* __restrict__ soa, double* __restrict__ aos, Geo G, int nf) {
+    const long long ey = G.ext[1], ez = G.ext[2];
+    const long long total = (long long)G.ext[0] * ey * ez;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        const long long k = t % ez, j = (t / ez) % ey, i = t / (ey * ez);
+        long long m;
+        if (G.dim == 1) m = i;
+        else if (G.dim == 2) m = i * G.pitch + j;
+        else m = i * G.pitch2 + j * G.pitch + k;
+        for (int f = 0; f < nf; f++) aos[t * nf + f] = soa[f * G.plane + m];
+    }
+}
+
+int solver_id(const dragon_config& c) {
+    if (c.mhd) {
+        if (c.riemann == RS_HLL) return RS_HLL;
+        if (c.riemann == RS_HLLE) return RS_HLLE;
+        return RS_HLLD;
+    }
+    switch (c.riemann) {
+        case RS_HLLX:
+        case RS_HLLC: return RS_HLLC;
+        case RS_HLL: return RS_HLL;
+        case RS_HLLE: return RS_HLLE;
+        case RS_ROE: return RS_ROE;
+        default: return RS_EXACT;  // Flux.cpp:20-34 runtime switch default
+    }
+}
+
+}  // namespace
+
+struct dragon_grid {
+    int dim = 0;
+    int n[3] = {1, 1, 1};
+    int g = 0;
+    double d[3] = {0, 0, 0};
+    int nf = 5;
+    bool mhd = false;
+    dragon_config cfg{};
+    int solver = RS_HLLC;
+    Geo cg{}, fg{};
+    double* w[2] = {nullptr, nullptr};
+    double* B[2] = {nullptr, nullptr};
+    int cur = 0;
+    StepCtl* ctl = nullptr;
+    StepCtl* hctl = nullptr;
+    BCEntry* dbcs = nullptr;
+    int nbc = 0;
+    std::vector<BCEntry> hbcs;
+    double* stage = nullptr;
+    size_t stage_elems = 0;
+    cudaStream_t stream = nullptr;
+    bool imax_valid = false;
+    unsigned long long launches = 0;
+    // step-kernel timing (dragon_gpu_profile_*)
+    bool prof = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending;
+    double prof_ms = 0;
+    long long prof_n = 0;
+};
+
+namespace {
+
+size_t dense_count(const Geo& G) { return (size_t)G.ext[0] * G.ext[1] * G.ext[2]; }
+
+StepArgs step_args(const dragon_grid* h, int slot_out) {
+    StepArgs a;
+    a.dx = h->d[0];
+    a.dy = h->d[1];
+    a.dz = h->d[2];
+    a.limiter = h->cfg.limiter;
+    a.cfl = h->cfg.cfl;
+    a.exact_max_iters = h->cfg.exact_max_iters;
+    a.exact_tol = h->cfg.exact_tol;
+    a.ct_energy = h->cfg.ct_energy;
+    a.slot_out = slot_out;
+    a.forced = 0;
+    return a;
+}
+
+cudaEvent_t take_event(dragon_grid* h) {
+    if (!h->ev_pool.empty()) {
+        cudaEvent_t e = h->ev_pool.back();
+        h->ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// Folds finished step-kernel timings into the running total.
+void collect_profile(dragon_grid* h) {
+    for (auto& p : h->ev_pending) {
+        float ms = 0;
+        if (cudaEventSynchronize(p.second) == cudaSuccess && cudaEventElapsedTime(&ms, p.first, p.second) == cudaSuccess) {
+            h->prof_ms += ms;
+            h->prof_n += 1;
+        }
+        h->ev_pool.push_back(p.first);
+        h->ev_pool.push_back(p.second);
+    }
+    h->ev_pending.clear();
+}
+
+template <bool MHD, int S>
+int launch_step_t(dragon_grid* h, int c) {
+    const StepArgs sa = step_args(h, c ^ 1);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (h->prof) {
+        e0 = take_event(h);
+        e1 = take_event(h);
+        cudaEventRecord(e0, h->stream);
+    }
+    if (h->dim == 1) {
+        const int np = h->n[0] + 2 * h->g;
+        k_step1d<MHD, S, k1dTS><<<(np + k1dTS - 1) / k1dTS, k1dTS, 0, h->stream>>>(h->cg, h->w[c], h->w[c ^ 1], h->ctl, sa);
+    } else if (h->dim == 2 && !MHD) {
+        auto kern = k_step2d_hydro<S, k2dTI, k2dTJ, k2dNT>;
+        const size_t smem = sizeof(Smem2DH<k2dTI, k2dTJ>);
+        static bool attr_set = false;
+        if (!attr_set) {
+            CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            attr_set = true;
+        }
+        dim3 grid((h->n[1] + k2dTJ - 1) / k2dTJ, (h->n[0] + k2dTI - 1) / k2dTI);
+        kern<<<grid, k2dNT, smem, h->stream>>>(h->cg, h->w[c], h->w[c ^ 1], h->ctl, sa);
+    } else if (h->dim == 2 && MHD) {
+        int rc = launch_step2d_mhd<S>(h->cg, h->fg, h->w[c], h->w[c ^ 1], h->B[c], h->B[c ^ 1], h->ctl, sa, h->stream);
+        if (rc == -1) return fail(DRAGON_GPU_EUNSUPPORTED, "2D MHD step is not built in this version");
+        if (rc) return fail(DRAGON_GPU_ECUDA, "MHD step launch failed");
+    } else {
+        return fail(DRAGON_GPU_EUNSUPPORTED, "3D unsplit step is not built in this version");
+    }
+    CK(cudaGetLastError());
+    if (h->prof) {
+        cudaEventRecord(e1, h->stream);
+        h->ev_pending.push_back({e0, e1});
+    }
+    h->launches++;
+    return 0;
+}
+
+int launch_step(dragon_grid* h, int c) {
+    if (h->mhd) {
+        switch (h->solver) {
+            case RS_HLL: return launch_step_t<true, RS_HLL>(h, c);
+            case RS_HLLE: return launch_step_t<true, RS_HLLE>(h, c);
+            default: return launch_step_t<true, RS_HLLD>(h, c);
+        }
+    }
+    switch (h->solver) {
+        case RS_HLLC: return launch_step_t<false, RS_HLLC>(h, c);
+        case RS_HLL: return launch_step_t<false, RS_HLL>(h, c);
+        case RS_HLLE: return launch_step_t<false, RS_HLLE>(h, c);
+        case RS_ROE: return launch_step_t<false, RS_ROE>(h, c);
+        default: return launch_step_t<false, RS_EXACT>(h, c);
+    }
+}
+
+int launch_prologue(dragon_grid* h, int c, int bookkeeping, int apply_bc, int compute_dt, int slot_in, int slot_out) {
+    PrologueArgs pa;
+    pa.dx = h->d[0];
+    pa.dy = h->d[1];
+    pa.dz = h->d[2];
+    pa.cfl_coeff = h->cfg.cfl_coeff;
+    pa.tol = h->cfg.timestep_tol;
+    pa.cfl = h->cfg.cfl;
+    pa.slot_in = slot_in;
+    pa.slot_out = slot_out;
+    pa.bookkeeping = bookkeeping;
+    pa.apply_bc = apply_bc;
+    pa.compute_dt = compute_dt;
+    pa.nbc = h->nbc;
+    if (h->mhd) k_prologue<true><<<1, 1024, 0, h->stream>>>(h->cg, h->fg, h->w[c], h->B[c], h->dbcs, h->ctl, pa);
+    else k_prologue<false><<<1, 1024, 0, h->stream>>>(h->cg, h->fg, h->w[c], h->B[c], h->dbcs, h->ctl, pa);
+    CK(cudaGetLastError());
+    h->launches++;
+    return 0;
+}
+
+int launch_interior_cfl(dragon_grid* h, int c, int slot) {
+    const long long total = (long long)h->n[0] * h->n[1] * h->n[2];
+    int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 8);
+    if (blocks < 1) blocks = 1;
+    if (h->mhd) k_interior_cfl<true><<<blocks, 256, 0, h->stream>>>(h->cg, h->w[c], h->ctl, slot, h->cfg.cfl, h->d[0], h->d[1], h->d[2]);
+    else k_interior_cfl<false><<<blocks, 256, 0, h->stream>>>(h->cg, h->w[c], h->ctl, slot, h->cfg.cfl, h->d[0], h->d[1], h->d[2]);
+    CK(cudaGetLastError());
+    h->launches++;
+    return 0;
+}
+
+// Writes the control block's header (everything before vmax) from the host mirror.
+int push_ctl(dragon_grid* h) {
+    CK(cudaMemcpyAsync(h->ctl, h->hctl, offsetof(StepCtl, vmax), cudaMemcpyHostToDevice, h->stream));
+    return 0;
+}
+int pull_ctl(dragon_grid* h) {
+    CK(cudaMemcpyAsync(h->hctl, h->ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+int zero_slot(dragon_grid* h, int slot) {
+    CK(cudaMemsetAsync(&h->ctl->vmax[slot], 0, sizeof(unsigned long long), h->stream));
+    return 0;
+}
+
+void reset_ctl(dragon_grid* h, double remaining, int max_steps, int check_cfl) {
+    StepCtl& c = *h->hctl;
+    unsigned long long keep[3] = {c.vmax[0], c.vmax[1], c.vmax[2]};
+    std::memset(&c, 0, sizeof(StepCtl));
+    c.remaining = remaining;
+    c.err_key = ~0ull;
+    c.max_steps = max_steps;
+    c.check_cfl = check_cfl;
+    for (int i = 0; i < 3; i++) c.vmax[i] = keep[i];
+}
+
+void fill_failure(const StepCtl& c, dragon_step_status* st, int code) {
+    if (!st) return;
+    st->code = code;
+    st->stage = (c.err_key == ~0ull) ? 0 : (int)(c.err_key >> 56);
+    st->cell = (c.err_key == ~0ull) ? -1 : (long long)(c.err_key & 0x00FFFFFFFFFFFFFFull);
+    st->dt = c.t1;
+}
+
+void fill_stats(const StepCtl& c, dragon_advance_stats* st) {
+    if (!st) return;
+    st->pivots_exact += c.pivots_exact;
+    st->hlld_to_hlle += c.hlld_to_hlle;
+    st->newton_iters += c.newton_iters;
+    st->exact_calls += c.exact_calls;
+    st->trrs += c.trrs;
+    st->muscl_first_order += c.muscl_first_order;
+}
+
+const char* stage_name(int s) {
+    switch (s) {
+        case ST_PRELIM_FLUX: return "Riemann Solution to physical inputs is unphysical (predictor flux)";
+        case ST_FINAL_FLUX: return "Riemann Solution to physical inputs is unphysical";
+        case ST_NAN: return "NaN state would be produced";
+        case ST_UNPHYSICAL: return "Unphysical state would be produced";
+        case ST_CFL_ZERO: return "CFL timestep failed: max signal speed is zero";
+        default: return "step failed";
+    }
+}
+
+// Shared advance loop. remaining/max_steps select advance(interval) or a step count.
+int advance_impl(dragon_grid* h, double remaining, int max_steps, int check_cfl, dragon_advance_stats* st) {
+    if (st) std::memset(st, 0, sizeof(*st));
+    const int cur0 = h->cur;
+    reset_ctl(h, remaining, max_steps, check_cfl);
+    int rc = push_ctl(h);
+    if (rc) return rc;
+    if (!h->imax_valid) {
+        if ((rc = zero_slot(h, cur0))) return rc;
+        if ((rc = launch_interior_cfl(h, cur0, cur0))) return rc;
+    }
+    long long k = 0;  // advance-local index of the next step to launch
+    int retries = 0;
+    for (;;) {
+        int nb = kBatch;
+        if (max_steps > 0) nb = (int)std::min<long long>(kBatch, (long long)max_steps + 1 - k);
+        if (nb < 1) nb = 1;
+        for (int b = 0; b < nb; b++) {
+            const int c = cur0 ^ (int)((k + b) & 1);
+            if ((rc = launch_prologue(h, c, 1, 1, 1, c, c ^ 1))) return rc;
+            // with a step budget, the prologue after the last step only accounts it
+            if (max_steps > 0 && k + b >= max_steps) continue;
+            if ((rc = launch_step(h, c))) return rc;
+        }
+        k += nb;
+        if ((rc = pull_ctl(h))) return rc;
+        StepCtl& C = *h->hctl;
+        if (C.err) {
+            const long long ks = C.steps_done;  // index of the failed step
+            const int c = cur0 ^ (int)(ks & 1);
+            h->cur = c;
+            h->imax_valid = true;
+            const int stage = (int)(C.err_key >> 56);
+            fill_stats(C, st);
+            if (st) { st->steps = (int)ks; fill_failure(C, &st->failure, DRAGON_GPU_ESTEP); }
+            if (stage == ST_CFL_ZERO) {
+                if (st) st->failure.code = DRAGON_GPU_ECFL;
+                return fail(DRAGON_GPU_ECFL, stage_name(stage));
+            }
+            // CFL.cpp:198-208: halve t1 and retry the same step on the same ghosts.
+            double t1 = C.t1;
+            for (;;) {
+                retries++;
+                t1 *= 0.5;
+                if (t1 < h->cfg.timestep_tol) {
+                    if (st) { st->retries = retries; st->failure.code = DRAGON_GPU_EDT; }
+                    return fail(DRAGON_GPU_EDT, std::string("Timestep has fallen below minimum after: ") + stage_name(stage));
+                }
+                C.t1 = t1;
+                C.err = 0;
+                C.err_key = ~0ull;
+                C.pivots_exact = C.hlld_to_hlle = C.newton_iters = C.exact_calls = C.trrs = C.muscl_first_order = 0;
+                if ((rc = push_ctl(h))) return rc;
+                if ((rc = zero_slot(h, c ^ 1))) return rc;
+                if ((rc = launch_step(h, c))) return rc;
+                if ((rc = pull_ctl(h))) return rc;
+                if (!C.err) break;
+                fill_stats(C, st);
+            }
+            // success: the next prologue accounts the retried step
+            k = ks + 1;
+            // keep cur0 parity consistent: step k reads buffer cur0 ^ (k & 1) == c ^ 1
+            continue;
+        }
+        if (C.done) {
+            h->cur = cur0 ^ (int)(C.steps_done & 1);
+            h->imax_valid = true;
+            fill_stats(C, st);
+            if (st) {
+                st->steps = C.steps_done;
+                st->retries = retries;
+                st->last_dt = C.t1;
+                st->time_advanced = (remaining - C.remaining);
+            }
+            return 0;
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* dragon_gpu_last_error(void) { return g_last_error.c_str(); }
+
+void dragon_gpu_default_config(dragon_config* c, int mhd) {
+    std::memset(c, 0, sizeof(*c));
+    c->mhd = mhd ? 1 : 0;
+    c->riemann = RS_HLLX;
+    c->limiter = LIM_MC;
+    c->cfl = 1;
+    c->ct_energy = 2;
+    c->exact_max_iters = 6;
+    c->exact_tol = 1e-12;
+    c->cfl_coeff = 0.3;
+    c->timestep_tol = 1e-14;
+    c->precision = 0;
+}
+
+int dragon_gpu_grid_create(int dim, int nx, int ny, int nz, double dx, double dy, double dz, int ghosts,
+                           const dragon_config* cfg, dragon_grid** out) {
+    if (!out || dim < 1 || dim > 3 || nx < 1 || (dim >= 2 && ny < 1) || (dim >= 3 && nz < 1))
+        return fail(DRAGON_GPU_EINVAL, "invalid grid extents");
+    int dev_count = 0;
+    if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count < 1)
+        return fail(DRAGON_GPU_ECUDA, "no CUDA device available");
+    dragon_grid* h = new dragon_grid();
+    if (cfg) h->cfg = *cfg;
+    else dragon_gpu_default_config(&h->cfg, 0);
+    h->mhd = h->cfg.mhd != 0;
+    h->nf = h->mhd ? 8 : 5;
+    h->dim = dim;
+    h->n[0] = nx;
+    h->n[1] = dim >= 2 ? ny : 1;
+    h->n[2] = dim >= 3 ? nz : 1;
+    h->d[0] = dx;
+    h->d[1] = dim >= 2 ? dy : 0.0;
+    h->d[2] = dim >= 3 ? dz : 0.0;
+    // validGhosts (Splitting.cpp:23-31): MHD + CTU needs 3, MUSCL-Hancock 2
+    const int gmin = (h->mhd && dim >= 2) ? 3 : 2;
+    h->g = ghosts > gmin ? ghosts : gmin;
+    if (h->mhd && dim == 1) h->g = ghosts > 3 ? ghosts : 3;
+    h->solver = solver_id(h->cfg);
+    h->cg = make_geo(dim, h->n, h->g);
+    int nfc[3] = {h->n[0] + 1, h->n[1] + 1, h->n[2] + 1};
+    h->fg = make_geo(dim, nfc, h->g);
+    auto cleanup = [&](int code) {
+        dragon_gpu_grid_destroy(h);
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return cleanup(fail(DRAGON_GPU_ECUDA, "cudaStreamCreate failed"));
+    for (int b = 0; b < 2; b++) {
+        if (cudaMalloc(&h->w[b], sizeof(double) * h->nf * h->cg.plane) != cudaSuccess)
+            return cleanup(fail(DRAGON_GPU_ECUDA, "cudaMalloc state failed"));
+        cudaMemsetAsync(h->w[b], 0, sizeof(double) * h->nf * h->cg.plane, h->stream);
+        if (h->mhd && dim >= 2) {
+            if (cudaMalloc(&h->B[b], sizeof(double) * 3 * h->fg.plane) != cudaSuccess)
+                return cleanup(fail(DRAGON_GPU_ECUDA, "cudaMalloc faceB failed"));
+            cudaMemsetAsync(h->B[b], 0, sizeof(double) * 3 * h->fg.plane, h->stream);
+        }
+    }
+    if (cudaMalloc(&h->ctl, sizeof(StepCtl)) != cudaSuccess) return cleanup(fail(DRAGON_GPU_ECUDA, "cudaMalloc ctl failed"));
+    cudaMemsetAsync(h->ctl, 0, sizeof(StepCtl), h->stream);
+    if (cudaMallocHost(&h->hctl, sizeof(StepCtl)) != cudaSuccess) return cleanup(fail(DRAGON_GPU_ECUDA, "cudaMallocHost failed"));
+    std::memset(h->hctl, 0, sizeof(StepCtl));
+    h->stage_elems = std::max(dense_count(h->cg) * h->nf, (h->mhd && dim >= 2) ? dense_count(h->fg) * 3 : (size_t)0);
+    if (cudaMalloc(&h->stage, sizeof(double) * h->stage_elems) != cudaSuccess)
+        return cleanup(fail(DRAGON_GPU_ECUDA, "cudaMalloc staging failed"));
+    // default boundary: empty list = implicit Outflow on every face
+    int rc = dragon_gpu_set_boundary(h, nullptr, 0);
+    if (rc) return cleanup(rc);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return cleanup(fail(DRAGON_GPU_ECUDA, "init sync failed"));
+    *out = h;
+    return 0;
+}
+
+int dragon_gpu_grid_destroy(dragon_grid* h) {
+    if (!h) return 0;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    collect_profile(h);
+    for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
+    for (int b = 0; b < 2; b++) {
+        if (h->w[b]) cudaFree(h->w[b]);
+        if (h->B[b]) cudaFree(h->B[b]);
+    }
+    if (h->ctl) cudaFree(h->ctl);
+    if (h->hctl) cudaFreeHost(h->hctl);
+    if (h->dbcs) cudaFree(h->dbcs);
+    if (h->stage) cudaFree(h->stage);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return 0;
+}
+
+int dragon_gpu_grid_info(const dragon_grid* h, int* dim, int* n3, int* ghosts, int* nfields) {
+    if (!h) return fail(DRAGON_GPU_EINVAL, "null handle");
+    if (dim) *dim = h->dim;
+    if (n3) { n3[0] = h->n[0]; n3[1] = h->n[1]; n3[2] = h->n[2]; }
+    if (ghosts) *ghosts = h->g;
+    if (nfields) *nfields = h->nf;
+    return 0;
+}
+
+size_t dragon_gpu_prim_count(const dragon_grid* h) { return h ? dense_count(h->cg) * h->nf : 0; }
+size_t dragon_gpu_faceB_count(const dragon_grid* h) {
+    return (h && h->mhd && h->dim >= 2) ? dense_count(h->fg) * 3 : 0;
+}
+
+static int transfer(dragon_grid* h, bool up, bool faces, double* host) {
+    if (!h || !host) return fail(DRAGON_GPU_EINVAL, "null argument");
+    if (faces && !(h->mhd && h->dim >= 2)) return fail(DRAGON_GPU_EINVAL, "grid has no face-centred B");
+    const Geo& G = faces ? h->fg : h->cg;
+    const int nf = faces ? 3 : h->nf;
+    double* dev = faces ? h->B[h->cur] : h->w[h->cur];
+    const size_t cnt = dense_count(G) * nf;
+    const int blocks = (int)std::min<size_t>((dense_count(G) + 255) / 256, 148 * 16);
+    if (up) {
+        CK(cudaMemcpyAsync(h->stage, host, cnt * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        k_aos_to_soa<<<blocks, 256, 0, h->stream>>>(h->stage, dev, G, nf);
+        CK(cudaGetLastError());
+        h->launches++;
+        h->imax_valid = false;
+    } else {
+        k_soa_to_aos<<<blocks, 256, 0, h->stream>>>(dev, h->stage, G, nf);
+        CK(cudaGetLastError());
+        h->launches++;
+        CK(cudaMemcpyAsync(host, h->stage, cnt * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int dragon_gpu_upload_prim(dragon_grid* h, const double* host) { return transfer(h, true, false, const_cast<double*>(host)); }
+int dragon_gpu_download_prim(dragon_grid* h, double* host) { return transfer(h, false, false, host); }
+int dragon_gpu_upload_faceB(dragon_grid* h, const double* host) { return transfer(h, true, true, const_cast<double*>(host)); }
+int dragon_gpu_download_faceB(dragon_grid* h, double* host) { return transfer(h, false, true, host); }
+
+int dragon_gpu_set_boundary(dragon_grid* h, const dragon_bc_desc* list, int n) {
+    if (!h || n < 0 || (n > 0 && !list)) return fail(DRAGON_GPU_EINVAL, "invalid boundary list");
+    std::vector<BCEntry> v;
+    // implicit Outflow over every face no entry covers (BoundaryList.hpp:97-104)
+    int uncovered = FX_NEG | FX_POS | FY_NEG | FY_POS | FZ_NEG | FZ_POS;
+    std::vector<BCEntry> user;
+    for (int i = 0; i < n; i++) {
+        BCEntry e{};
+        e.type = list[i].type;
+        if (e.type < BC_OUTFLOW || e.type > BC_IGNORE) return fail(DRAGON_GPU_EINVAL, "unknown boundary type");
+        e.faces = list[i].faces & 63;
+        if (e.type == BC_PERIODIC) {
+            // Periodic.cpp:14-15: a periodic axis always covers both faces
+            int f = 0;
+            if (e.faces & (FX_NEG | FX_POS)) f |= FX_NEG | FX_POS;
+            if (e.faces & (FY_NEG | FY_POS)) f |= FY_NEG | FY_POS;
+            if (e.faces & (FZ_NEG | FZ_POS)) f |= FZ_NEG | FZ_POS;
+            e.faces = f;
+        }
+        e.corners = list[i].corners ? 1 : 0;
+        for (int k = 0; k < 8; k++) e.state[k] = list[i].state[k];
+        uncovered &= ~e.faces;
+        user.push_back(e);
+    }
+    if (uncovered) {
+        BCEntry imp{};
+        imp.type = BC_OUTFLOW;
+        imp.faces = uncovered;
+        imp.corners = 1;
+        v.push_back(imp);
+    }
+    for (auto& e : user) v.push_back(e);
+    if (h->dbcs) { cudaStreamSynchronize(h->stream); cudaFree(h->dbcs); h->dbcs = nullptr; }
+    h->nbc = (int)v.size();
+    h->hbcs = v;
+    if (h->nbc) {
+        CK(cudaMalloc(&h->dbcs, sizeof(BCEntry) * v.size()));
+        CK(cudaMemcpyAsync(h->dbcs, v.data(), sizeof(BCEntry) * v.size(), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    return 0;
+}
+
+int dragon_gpu_apply_boundary(dragon_grid* h) {
+    if (!h) return fail(DRAGON_GPU_EINVAL, "null handle");
+    reset_ctl(h, 0.0, 0, 0);
+    int rc = push_ctl(h);
+    if (rc) return rc;
+    if ((rc = launch_prologue(h, h->cur, 0, 1, 0, 2, 2))) return rc;
+    CK(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int dragon_gpu_cfl_time(dragon_grid* h, double* dt_out) {
+    if (!h || !dt_out) return fail(DRAGON_GPU_EINVAL, "null argument");
+    reset_ctl(h, INFINITY, 0, 1);
+    int rc = push_ctl(h);
+    if (rc) return rc;
+    if ((rc = zero_slot(h, 2))) return rc;
+    if ((rc = launch_interior_cfl(h, h->cur, 2))) return rc;
+    if ((rc = launch_prologue(h, h->cur, 0, 0, 1, 2, 2))) return rc;
+    if ((rc = pull_ctl(h))) return rc;
+    if (h->hctl->err) return fail(DRAGON_GPU_ECFL, stage_name(ST_CFL_ZERO));
+    *dt_out = h->hctl->t1;
+    return 0;
+}
+
+int dragon_gpu_unsplit_step(dragon_grid* h, double dt, dragon_step_status* st) {
+    if (!h) return fail(DRAGON_GPU_EINVAL, "null handle");
+    if (st) std::memset(st, 0, sizeof(*st));
+    reset_ctl(h, 0.0, 0, 0);
+    h->hctl->t1 = dt;
+    int rc = push_ctl(h);
+    if (rc) return rc;
+    const int c = h->cur;
+    if ((rc = zero_slot(h, c ^ 1))) return rc;
+    if ((rc = launch_step(h, c))) return rc;
+    if ((rc = pull_ctl(h))) return rc;
+    if (h->hctl->err) {
+        fill_failure(*h->hctl, st, DRAGON_GPU_ESTEP);
+        return fail(DRAGON_GPU_ESTEP, stage_name((int)(h->hctl->err_key >> 56)));
+    }
+    h->cur = c ^ 1;
+    h->imax_valid = true;
+    if (st) st->dt = dt;
+    return 0;
+}
+
+int dragon_gpu_advance(dragon_grid* h, double interval, int check_cfl, dragon_advance_stats* st) {
+    if (!h) return fail(DRAGON_GPU_EINVAL, "null handle");
+    return advance_impl(h, interval, 0, check_cfl ? 1 : 0, st);
+}
+
+int dragon_gpu_advance_steps(dragon_grid* h, int nsteps, dragon_advance_stats* st) {
+    if (!h || nsteps < 0) return fail(DRAGON_GPU_EINVAL, "invalid argument");
+    if (nsteps == 0) { if (st) std::memset(st, 0, sizeof(*st)); return 0; }
+    return advance_impl(h, INFINITY, nsteps, 1, st);
+}
+
+void* dragon_gpu_stream(dragon_grid* h) { return h ? (void*)h->stream : nullptr; }
+
+int dragon_gpu_device_state(dragon_grid* h, double** prim, long long* plane, long long* pitch) {
+    if (!h) return fail(DRAGON_GPU_EINVAL, "null handle");
+    if (prim) *prim = h->w[h->cur];
+    if (plane) *plane = h->cg.plane;
+    if (pitch) *pitch = h->cg.pitch;
+    return 0;
+}
+
+unsigned long long dragon_gpu_launch_count(const dragon_grid* h) { return h ? h->launches : 0; }
+
+int dragon_gpu_profile_enable(dragon_grid* h, int on) {
+    if (!h) return fail(DRAGON_GPU_EINVAL, "null handle");
+    collect_profile(h);
+    h->prof = on != 0;
+    return 0;
+}
+
+int dragon_gpu_profile_read(dragon_grid* h, double* ms_total, long long* launches, int reset) {
+    if (!h) return fail(DRAGON_GPU_EINVAL, "null handle");
+    collect_profile(h);
+    if (ms_total) *ms_total = h->prof_ms;
+    if (launches) *launches = h->prof_n;
+    if (reset) { h->prof_ms = 0; h->prof_n = 0; }
+    return 0;
+}
+
+int dragon_gpu_initialize_B_fields(dragon_grid* h) {
+    if (!h) return fail(DRAGON_GPU_EINVAL, "null handle");
+    if (!(h->mhd && h->dim >= 2)) return fail(DRAGON_GPU_EINVAL, "grid has no face-centred B");
+    int rc = dragon_gpu_apply_boundary(h);
+    if (rc) return rc;
+    rc = launch_init_body_fields(h->cg, h->fg, h->w[h->cur], h->B[h->cur], h->stream);
+    if (rc) return fail(DRAGON_GPU_ECUDA, "initialize_B_fields launch failed");
+    h->launches++;
+    h->imax_valid = false;
+    CK(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+}  // extern "C"

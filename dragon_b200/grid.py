@@ -1,0 +1,332 @@
+"""Grid1D / Grid2D / Grid3D resident on the GPU, mirroring DRAGON's Grid API.
+
+The classes keep the reference's constructor arguments, ghost policy,
+``boundary`` member, ``advance(dt, check_cfl=True)``, ``unsplit_step(dt)``,
+``initialize_B_fields()`` and cell access with ghost coordinates
+(DRAGON/Hydro/Grid.hpp:19-144). A host mirror of the padded array in the
+reference's memory order (last index fastest, ghosts included) is synced
+lazily: reads after a device step download, writes mark the mirror dirty and
+the next device call uploads it.
+
+Errors follow the reference: a failing step raises (``StepFailed``), and the
+CFL-zero and timestep-underflow cases raise too, where the reference throws or
+exits (CFL.cpp:102-117,205-208).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from .boundary import BoundaryList, as_list
+
+# Config ids (DRAGON/Config.h)
+RIEMANN_EXACT, RIEMANN_HLL, RIEMANN_HLLC, RIEMANN_HLLD, RIEMANN_HLLE, RIEMANN_HLLX, RIEMANN_ROE = range(7)
+LIMITER_MINMOD, LIMITER_MC, LIMITER_VANLEER, LIMITER_SUPERBEE, LIMITER_VANALBADA = range(5)
+CFL_MAX, CFL_ADD = 0, 1
+CT_CONSV_TOTAL_E, CT_CONSV_THERMAL, CT_CONSV_BETA_GATED = 0, 1, 2
+PREC_FP64, PREC_MIXED = 0, 1
+
+
+@dataclass
+class Config:
+    """Runtime form of DRAGON/Config.h's switches; defaults are the shipped ones."""
+
+    mhd: bool = False
+    riemann: int = RIEMANN_HLLX
+    limiter: int = LIMITER_MC
+    cfl: int = CFL_ADD
+    ct_energy: int = CT_CONSV_BETA_GATED
+    exact_max_iters: int = 6
+    exact_tol: float = 1e-12
+    cfl_coeff: float = 0.3
+    timestep_tol: float = 1e-14
+    precision: int = PREC_FP64
+
+    def to_c(self) -> _lib.DragonConfig:
+        c = _lib.DragonConfig()
+        c.mhd = int(self.mhd)
+        c.riemann = self.riemann
+        c.limiter = self.limiter
+        c.cfl = self.cfl
+        c.ct_energy = self.ct_energy
+        c.exact_max_iters = self.exact_max_iters
+        c.exact_tol = self.exact_tol
+        c.cfl_coeff = self.cfl_coeff
+        c.timestep_tol = self.timestep_tol
+        c.precision = self.precision
+        return c
+
+
+class StepFailed(RuntimeError):
+    """Grid::unsplit_step threw (unphysical state / no physical flux)."""
+
+    def __init__(self, msg, status):
+        super().__init__(msg)
+        self.status = status
+
+
+@dataclass
+class AdvanceResult:
+    steps: int = 0
+    retries: int = 0
+    last_dt: float = 0.0
+    time_advanced: float = 0.0
+    pivots_exact: int = 0
+    hlld_to_hlle: int = 0
+    newton_iters: int = 0
+    exact_calls: int = 0
+    trrs: int = 0
+    muscl_first_order: int = 0
+    extra: dict = field(default_factory=dict)
+
+
+def _result(st: _lib.AdvanceStats) -> AdvanceResult:
+    return AdvanceResult(st.steps, st.retries, st.last_dt, st.time_advanced, st.pivots_exact, st.hlld_to_hlle,
+                         st.newton_iters, st.exact_calls, st.trrs, st.muscl_first_order)
+
+
+class _GridBase:
+    dim = 0
+
+    def __init__(self, n, d, ghosts, config: Config | None):
+        self.config = config or Config()
+        self._lib = _lib.load()
+        n3 = list(n) + [1] * (3 - len(n))
+        d3 = list(d) + [0.0] * (3 - len(d))
+        h = ctypes.c_void_p()
+        cfg = self.config.to_c()
+        _lib.check(self._lib.dragon_gpu_grid_create(self.dim, n3[0], n3[1], n3[2], d3[0], d3[1], d3[2], int(ghosts),
+                                                    ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+        dim = ctypes.c_int()
+        nn = (ctypes.c_int * 3)()
+        g = ctypes.c_int()
+        nf = ctypes.c_int()
+        _lib.check(self._lib.dragon_gpu_grid_info(h, ctypes.byref(dim), nn, ctypes.byref(g), ctypes.byref(nf)))
+        self.n = tuple(nn[i] for i in range(self.dim))
+        self.ghosts = g.value
+        self.nfields = nf.value
+        shape = tuple(x + 2 * self.ghosts for x in self.n) + (self.nfields,)
+        self._w = np.zeros(shape, dtype=np.float64)
+        self._B = None
+        if self.config.mhd and self.dim >= 2:
+            self._B = np.zeros(tuple(x + 1 + 2 * self.ghosts for x in self.n) + (3,), dtype=np.float64)
+        self._host_dirty = True      # host mirror newer than device
+        self._dev_dirty = False      # device newer than host mirror
+        self._boundary = BoundaryList()
+        self._push_boundary()
+
+    # -- lifecycle ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.dragon_gpu_grid_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- sync --------------------------------------------------------------
+    def _ptr(self, a):
+        return a.ctypes.data_as(_lib.c_double_p)
+
+    def upload(self):
+        _lib.check(self._lib.dragon_gpu_upload_prim(self._h, self._ptr(self._w)))
+        if self._B is not None:
+            _lib.check(self._lib.dragon_gpu_upload_faceB(self._h, self._ptr(self._B)))
+        self._host_dirty = False
+
+    def download(self):
+        _lib.check(self._lib.dragon_gpu_download_prim(self._h, self._ptr(self._w)))
+        if self._B is not None:
+            _lib.check(self._lib.dragon_gpu_download_faceB(self._h, self._ptr(self._B)))
+        self._dev_dirty = False
+
+    def _to_device(self):
+        if self._host_dirty:
+            self.upload()
+
+    def _device_ran(self):
+        self._dev_dirty = True
+
+    @property
+    def w(self) -> np.ndarray:
+        """The padded primitive array (host mirror; modifications are uploaded
+        before the next device call)."""
+        if self._dev_dirty:
+            self.download()
+        self._host_dirty = True
+        return self._w
+
+    @property
+    def B(self) -> np.ndarray:
+        """Face-centred B, padded (n+1 per axis), 3 components (MHD 2D/3D)."""
+        if self._B is None:
+            raise AttributeError("grid has no face-centred B")
+        if self._dev_dirty:
+            self.download()
+        self._host_dirty = True
+        return self._B
+
+    def _B_(self):
+        return self.B
+
+    def interior(self) -> np.ndarray:
+        g = self.ghosts
+        sl = tuple(slice(g, g + x) for x in self.n)
+        return self.w[sl]
+
+    def _index(self, idx):
+        if not isinstance(idx, tuple):
+            idx = (idx,)
+        if len(idx) != self.dim:
+            raise IndexError(f"{self.dim}D grid needs {self.dim} indices")
+        g = self.ghosts
+        out = []
+        for i, n in zip(idx, self.n):
+            if not (-g <= i < n + g):
+                raise IndexError(f"index {i} outside [-{g}, {n + g})")
+            out.append(i + g)
+        return tuple(out)
+
+    def __getitem__(self, idx):
+        return self.w[self._index(idx)]
+
+    def __setitem__(self, idx, value):
+        self.w[self._index(idx)] = np.asarray(value, dtype=np.float64)[: self.nfields]
+
+    # -- boundary ------------------------------------------------------------
+    @property
+    def boundary(self) -> BoundaryList:
+        return self._boundary
+
+    @boundary.setter
+    def boundary(self, b):
+        self._boundary = as_list(b)
+        self._push_boundary()
+
+    def _push_boundary(self):
+        els = list(self._boundary)
+        arr = (_lib.BCDesc * max(1, len(els)))()
+        for k, e in enumerate(els):
+            arr[k].type = e.kind
+            arr[k].faces = e.get_faces()
+            arr[k].corners = int(e.corners)
+            st = list(e.state()) + [0.0] * 8
+            for q in range(8):
+                arr[k].state[q] = st[q]
+        _lib.check(self._lib.dragon_gpu_set_boundary(self._h, arr, len(els)))
+
+    def apply_boundary(self):
+        self._push_boundary()
+        self._to_device()
+        _lib.check(self._lib.dragon_gpu_apply_boundary(self._h))
+        self._device_ran()
+
+    # -- stepping --------------------------------------------------------------
+    def cfl_time(self) -> float:
+        """CFL::cfl_time on the current ghosts (CFL.cpp:88-137)."""
+        self._to_device()
+        out = ctypes.c_double()
+        _lib.check(self._lib.dragon_gpu_cfl_time(self._h, ctypes.byref(out)))
+        return out.value
+
+    def unsplit_step(self, dt: float):
+        """Grid::unsplit_step (Unsplit.cpp:28-206): raises StepFailed, committing
+        nothing, when the reference would throw."""
+        self._to_device()
+        st = _lib.StepStatus()
+        rc = self._lib.dragon_gpu_unsplit_step(self._h, float(dt), ctypes.byref(st))
+        if rc == 3:
+            raise StepFailed(self._lib.dragon_gpu_last_error().decode(), st)
+        _lib.check(rc)
+        self._device_ran()
+
+    def split_step(self, dt: float):
+        raise NotImplementedError("the Strang-split path is outside the unsplit update")
+
+    def advance(self, dt: float, check_cfl: bool = True) -> AdvanceResult:
+        """Grid::advance (CFL.cpp:151-213), run entirely on the device."""
+        self._to_device()
+        st = _lib.AdvanceStats()
+        rc = self._lib.dragon_gpu_advance(self._h, float(dt), int(bool(check_cfl)), ctypes.byref(st))
+        self._device_ran()
+        _lib.check(rc)
+        return _result(st)
+
+    advance_unsplit = advance
+
+    def advance_steps(self, nsteps: int) -> AdvanceResult:
+        """nsteps CFL-limited steps (each the reference's advance(cfl_time()))."""
+        self._to_device()
+        st = _lib.AdvanceStats()
+        rc = self._lib.dragon_gpu_advance_steps(self._h, int(nsteps), ctypes.byref(st))
+        self._device_ran()
+        _lib.check(rc)
+        return _result(st)
+
+    def initialize_B_fields(self):
+        """Grid::initialize_B_fields (B_fields.cpp:117-149)."""
+        self._push_boundary()
+        self._to_device()
+        _lib.check(self._lib.dragon_gpu_initialize_B_fields(self._h))
+        self._device_ran()
+
+    def launch_count(self) -> int:
+        return int(self._lib.dragon_gpu_launch_count(self._h))
+
+    def getGhosts(self) -> int:
+        return self.ghosts
+
+
+class Grid1D(_GridBase):
+    """Grid1D(size, dx, ghosts=1) (Grid.hpp:40-59)."""
+
+    dim = 1
+
+    def __init__(self, size: int, dx: float, ghosts: int = 1, config: Config | None = None):
+        super().__init__((size,), (dx,), ghosts, config)
+        self.dx = dx
+
+    def getSize(self):
+        return self.n[0]
+
+
+class Grid2D(_GridBase):
+    """Grid2D(nx, ny, dx, dy, ghosts=1) (Grid.hpp:61-101)."""
+
+    dim = 2
+
+    def __init__(self, nx: int, ny: int, dx: float, dy: float, ghosts: int = 1, config: Config | None = None):
+        super().__init__((nx, ny), (dx, dy), ghosts, config)
+        self.dx, self.dy = dx, dy
+
+    def getSizeX(self):
+        return self.n[0]
+
+    def getSizeY(self):
+        return self.n[1]
+
+
+class Grid3D(_GridBase):
+    """Grid3D(nx, ny, nz, dx, dy, dz, ghosts=2) (Grid.hpp:103-144)."""
+
+    dim = 3
+
+    def __init__(self, nx, ny, nz, dx, dy, dz, ghosts: int = 2, config: Config | None = None):
+        super().__init__((nx, ny, nz), (dx, dy, dz), ghosts, config)
+        self.dx, self.dy, self.dz = dx, dy, dz
+
+    def getSizeX(self):
+        return self.n[0]
+
+    def getSizeY(self):
+        return self.n[1]
+
+    def getSizeZ(self):
+        return self.n[2]

@@ -1,0 +1,113 @@
+"""Initial conditions of the standard test problems, as padded numpy arrays in
+the reference's memory order (cells i slowest, ghosts included, NF primitive
+fields rho, p, vx, vy, vz[, Bx, By, Bz]).
+
+These restate the workloads the path is measured on: the 1D Sod tube, the 2D
+Kelvin-Helmholtz shear layer, the 2D Orszag-Tang vortex and the 3D blast. Cell
+centres sit at (i + 1/2) * dx from the domain origin; ghosts are left zero
+(the boundary fill sets them).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+
+def _centres(n, lo, hi):
+    d = (hi - lo) / n
+    return lo + (np.arange(n) + 0.5) * d, d
+
+
+def sod_1d(n=512, ghosts=2, x0=0.5, left=(1.0, 0.0, 1.0), right=(0.125, 0.0, 0.1)):
+    """1D two-state Riemann problem on [0,1]: (rho, u, p) left / right of x0."""
+    x, dx = _centres(n, 0.0, 1.0)
+    w = np.zeros((n + 2 * ghosts, 5))
+    L = x < x0
+    w[ghosts:ghosts + n, 0] = np.where(L, left[0], right[0])
+    w[ghosts:ghosts + n, 2] = np.where(L, left[1], right[1])
+    w[ghosts:ghosts + n, 1] = np.where(L, left[2], right[2])
+    return w, dx
+
+
+def kelvin_helmholtz_2d(n=1024, ghosts=2, seed=1234, amp=0.01, ny=None):
+    """Periodic unit-square shear layer: rho=2, vx=+0.5 for |y-0.5|<0.25, else
+    rho=1, vx=-0.5; p=2.5; vy uniform noise of amplitude amp per cell from a
+    seeded generator (numpy PCG64, seed)."""
+    ny = ny or n
+    x, dx = _centres(n, 0.0, 1.0)
+    y, dy = _centres(ny, 0.0, 1.0)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    vy = rng.uniform(-amp, amp, size=(n, ny))
+    inner = np.abs(y - 0.5) < 0.25
+    w = np.zeros((n + 2 * ghosts, ny + 2 * ghosts, 5))
+    sl = (slice(ghosts, ghosts + n), slice(ghosts, ghosts + ny))
+    w[sl + (0,)] = np.where(inner[None, :], 2.0, 1.0)
+    w[sl + (1,)] = 2.5
+    w[sl + (2,)] = np.where(inner[None, :], 0.5, -0.5)
+    w[sl + (3,)] = vy
+    return w, dx, dy
+
+
+def orszag_tang_2d(n=1024, ghosts=3, B0=1.0 / math.sqrt(4.0 * math.pi)):
+    """Periodic [0,1]^2 Orszag-Tang vortex in DRAGON's Gaussian units:
+    rho = 25/(36 pi), p = 5/(12 pi), v = (-sin 2 pi y, sin 2 pi x),
+    face B = B0 (-sin 2 pi y, sin 4 pi x). Bx lives on x-faces at
+    (i dx, (j+1/2) dy), By on y-faces at ((i+1/2) dx, j dy). Returns the cell
+    array (cell B left zero: initialize_B_fields fills it) and the face array."""
+    x, dx = _centres(n, 0.0, 1.0)
+    y, dy = _centres(n, 0.0, 1.0)
+    g = ghosts
+    w = np.zeros((n + 2 * g, n + 2 * g, 8))
+    sl = (slice(g, g + n), slice(g, g + n))
+    X, Y = np.meshgrid(x, y, indexing="ij")
+    w[sl + (0,)] = 25.0 / (36.0 * math.pi)
+    w[sl + (1,)] = 5.0 / (12.0 * math.pi)
+    w[sl + (2,)] = -np.sin(2 * math.pi * Y)
+    w[sl + (3,)] = np.sin(2 * math.pi * X)
+    B = np.zeros((n + 1 + 2 * g, n + 1 + 2 * g, 3))
+    xf = np.arange(n + 1) * dx
+    yf = np.arange(n + 1) * dy
+    Xf, Yc = np.meshgrid(xf, np.concatenate([y, [y[-1] + dy]]), indexing="ij")
+    B[g:g + n + 1, g:g + n + 1, 0] = -B0 * np.sin(2 * math.pi * Yc)
+    Xc, Yf = np.meshgrid(np.concatenate([x, [x[-1] + dx]]), yf, indexing="ij")
+    B[g:g + n + 1, g:g + n + 1, 1] = B0 * np.sin(4 * math.pi * Xc)
+    return w, B, dx, dy
+
+
+def blast_3d(n=256, ghosts=2, p_in=10.0, p_out=0.1, r0=0.1):
+    """Blast on [-0.5,0.5]^3: rho=1, v=0, p=p_in inside r<r0, else p_out."""
+    x, dx = _centres(n, -0.5, 0.5)
+    g = ghosts
+    w = np.zeros((n + 2 * g,) * 3 + (5,))
+    X, Y, Z = np.meshgrid(x, x, x, indexing="ij")
+    r = np.sqrt(X * X + Y * Y + Z * Z)
+    sl = (slice(g, g + n),) * 3
+    w[sl + (0,)] = 1.0
+    w[sl + (1,)] = np.where(r < r0, p_in, p_out)
+    return w, dx
+
+
+def blast_2d_mhd(n=128, ghosts=3, p_in=10.0, p_out=0.1, r0=0.1, B=(1.0 / math.sqrt(2.0), 1.0 / math.sqrt(2.0), 0.0)):
+    """2D MHD blast on [-0.5,0.5]^2 with uniform B (cell and face values)."""
+    x, dx = _centres(n, -0.5, 0.5)
+    g = ghosts
+    w = np.zeros((n + 2 * g, n + 2 * g, 8))
+    X, Y = np.meshgrid(x, x, indexing="ij")
+    r = np.sqrt(X * X + Y * Y)
+    sl = (slice(g, g + n),) * 2
+    w[sl + (0,)] = 1.0
+    w[sl + (1,)] = np.where(r < r0, p_in, p_out)
+    Bf = np.zeros((n + 1 + 2 * g, n + 1 + 2 * g, 3))
+    Bf[g:g + n + 1, g:g + n + 1, 0] = B[0]
+    Bf[g:g + n + 1, g:g + n + 1, 1] = B[1]
+    Bf[g:g + n + 1, g:g + n + 1, 2] = B[2]
+    return w, Bf, dx
+
+
+def rel_l1(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """Relative L1 difference per field over the last axis: sum|a-b| / sum|b|."""
+    ax = tuple(range(a.ndim - 1))
+    num = np.abs(a - b).sum(axis=ax)
+    den = np.abs(b).sum(axis=ax)
+    return num / np.where(den > 0, den, 1.0)

@@ -1,0 +1,162 @@
+/*
+ * dragon_gpu.h — C ABI of the B200 unsplit Godunov update for DRAGON grids.
+ *
+ * One handle is one grid (DRAGON's Grid1D / Grid2D / Grid3D) resident in GPU
+ * memory. The entry points replace, one for one, the calls DRAGON's pthread
+ * subgrid path makes on a grid; each declaration names the reference
+ * interface it stands in for (paths are relative to the DRAGON source tree).
+ *
+ * Conventions
+ *   - Every function returns 0 on success or a DRAGON_GPU_E* code; the message
+ *     of the last failure on the calling thread is dragon_gpu_last_error().
+ *   - Host arrays use the reference's own memory order: the ghost-padded array
+ *     of ExtendedArray{1,2,3}D (Hydro/ExtendedArray/ExtendedArray.hpp:75,125;
+ *     last index fastest, ghosts included), NF doubles per cell in the order
+ *     of PrimitiveState (FluidElement/FluidElement.hpp:34-43):
+ *     rho, p, vx, vy, vz, and for MHD Bx, By, Bz (NF = 5 or 8).
+ *   - Face-centred B (MHD, 2D/3D) uses the (n+1)-per-dimension padded face
+ *     arrays of Grid2D/Grid3D (Hydro/Grid.hpp:65,107) with 3 doubles per face.
+ *   - A handle is used by one host thread at a time; distinct handles may run
+ *     concurrently (each owns a CUDA stream).
+ */
+#ifndef DRAGON_GPU_H
+#define DRAGON_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define DRAGON_GPU_OK 0
+#define DRAGON_GPU_EINVAL 1       /* bad argument */
+#define DRAGON_GPU_ECUDA 2        /* CUDA runtime failure */
+#define DRAGON_GPU_ESTEP 3        /* step produced an unphysical / non-finite state or no physical flux */
+#define DRAGON_GPU_ECFL 4         /* CFL limit failed: max signal speed is zero */
+#define DRAGON_GPU_EDT 5          /* retried step fell below Timestep_Tolerance */
+#define DRAGON_GPU_EUNSUPPORTED 6 /* configuration not built */
+
+/* Runtime form of DRAGON/Config.h's switches (Config.h:26-90). Ids equal the
+ * reference's macro values: RIEMANN_EXACT 0, HLL 1, HLLC 2, HLLD 3, HLLE 4,
+ * HLLX 5, ROE 6; LIMITER_MINMOD 0, MC 1, VANLEER 2, SUPERBEE 3, VANALBADA 4;
+ * CFL_MAX 0, CFL_ADD 1, p > 1 for the p-norm; CT_CONSV_TOTAL_E 0, THERMAL 1,
+ * BETA_GATED 2. */
+typedef struct dragon_config {
+    int mhd;              /* 0 hydro, 1 MHD (the reference's #define MHD) */
+    int riemann;          /* RIEMANN_DEFAULT */
+    int limiter;          /* MUSCL_DEFAULT_LIMITER */
+    int cfl;              /* CFL_CALCULATION */
+    int ct_energy;        /* CT_ENERGY_CONSV */
+    int exact_max_iters;  /* ExactRiemann_MaxIters (6) */
+    double exact_tol;     /* ExactRiemann_Tolerance (1e-12) */
+    double cfl_coeff;     /* CFL_coeff (0.3) */
+    double timestep_tol;  /* Timestep_Tolerance (1e-14) */
+    int precision;        /* 0: FP64 throughout (bit-faithful), 1: mixed FP32/FP64 */
+    int reserved[7];
+} dragon_config;
+
+/* Fills the reference's shipped defaults for the given physics mode. */
+void dragon_gpu_default_config(dragon_config* cfg, int mhd);
+
+/* Boundary list entry (DRAGON/Boundary/Boundary.hpp:158-229). type: 0 Outflow,
+ * 1 Outflow::Gated, 2 Fixed, 3 Reflective, 4 Periodic, 5 Ignore. faces is the
+ * bit mask of Boundary::face_mask (X- 1, X+ 2, Y- 4, Y+ 8, Z- 16, Z+ 32);
+ * state is Fixed's primitive state (NF values). */
+typedef struct dragon_bc_desc {
+    int type;
+    int faces;
+    int corners;
+    int reserved;
+    double state[8];
+} dragon_bc_desc;
+
+typedef struct dragon_step_status {
+    int code;              /* DRAGON_GPU_OK or DRAGON_GPU_ESTEP / ECFL */
+    int stage;             /* 1 predictor flux, 2 final flux, 3 non-finite, 4 unphysical, 5 CFL */
+    long long cell;        /* linear padded index of the first failing cell/face */
+    double dt;             /* dt of the (last) attempt */
+} dragon_step_status;
+
+typedef struct dragon_advance_stats {
+    int steps;                      /* successful steps */
+    int retries;                    /* halvings after a failed step (CFL.cpp:198-208) */
+    double last_dt;
+    double time_advanced;
+    unsigned long long pivots_exact;      /* verify_and_fallback pivots to the exact solver */
+    unsigned long long hlld_to_hlle;      /* HLLD star states replaced by HLLE */
+    unsigned long long newton_iters;      /* exact solver Newton iterations */
+    unsigned long long exact_calls;       /* exact solver star-pressure solves */
+    unsigned long long trrs;              /* two-rarefaction closed forms */
+    unsigned long long muscl_first_order; /* MUSCL first-order fallbacks */
+    dragon_step_status failure;           /* last failure seen (code 0 if none) */
+} dragon_advance_stats;
+
+typedef struct dragon_grid dragon_grid;
+
+/* Grid1D(size, dx, ghosts) / Grid2D(nx, ny, dx, dy, ghosts) /
+ * Grid3D(nx, ny, nz, dx, dy, dz, ghosts) (Hydro/Grid.hpp:46,70,112;
+ * Hydro/Godunov/Splitting.cpp:23-61): ghosts are raised to the minimum the
+ * scheme needs (2 hydro, 3 MHD) exactly like validGhosts. Unused extents are
+ * ignored. Replaces DistGrid{1,2,3}D's constructors (Refinement/DistGrid.cpp:41-111). */
+int dragon_gpu_grid_create(int dim, int nx, int ny, int nz, double dx, double dy, double dz, int ghosts,
+                           const dragon_config* cfg, dragon_grid** out);
+int dragon_gpu_grid_destroy(dragon_grid* g);
+/* getGhosts() / getSize*() (Hydro/Grid.hpp:54,79,121) */
+int dragon_gpu_grid_info(const dragon_grid* g, int* dim, int* n3, int* ghosts, int* nfields);
+/* Number of doubles in the padded primitive array and in the padded face-B array. */
+size_t dragon_gpu_prim_count(const dragon_grid* g);
+size_t dragon_gpu_faceB_count(const dragon_grid* g);
+
+/* Bulk access standing in for operator[] over the whole padded array
+ * (Hydro/Grid.hpp:52-53,77-78,119-120) and _B() (Hydro/Grid.hpp:83,125);
+ * the transfers DistGrid::pushToChildren / loadFromChildren do
+ * (Refinement/DistGrid.cpp:115-289). Synchronous with respect to the host. */
+int dragon_gpu_upload_prim(dragon_grid* g, const double* host);
+int dragon_gpu_download_prim(dragon_grid* g, double* host);
+int dragon_gpu_upload_faceB(dragon_grid* g, const double* host);
+int dragon_gpu_download_faceB(dragon_grid* g, double* host);
+
+/* grid.boundary = ... (Hydro/Grid.hpp:35; Boundary/BoundaryList.hpp:22-105). */
+int dragon_gpu_set_boundary(dragon_grid* g, const dragon_bc_desc* list, int n);
+/* boundary.apply(grid) (Boundary/BoundaryList.hpp:79-93) */
+int dragon_gpu_apply_boundary(dragon_grid* g);
+/* Grid::initialize_B_fields (MHD/B_fields.cpp:117-149) */
+int dragon_gpu_initialize_B_fields(dragon_grid* g);
+
+/* CFL::cfl_time (Hydro/CFL/CFL.cpp:88-137) on the current ghosts. */
+int dragon_gpu_cfl_time(dragon_grid* g, double* dt_out);
+/* Grid::unsplit_step(dt) (Hydro/Godunov/Unsplit.cpp:28-206, Splitting.cpp:100-115):
+ * one step with the caller's dt on the current ghosts; on failure nothing is
+ * committed and st describes the failure (the reference throws). */
+int dragon_gpu_unsplit_step(dragon_grid* g, double dt, dragon_step_status* st);
+/* Grid::advance(dt, check_cfl) (Hydro/CFL/CFL.cpp:151-213): the whole
+ * sub-cycling loop — ghost fill, CFL dt, step, halve-and-retry on failure —
+ * runs on the device; DistGrid's thread fan-out and all-or-nothing commit
+ * (Refinement/DistGrid.cpp:292-304, DRAGONWING/Multithreading/pthread_parallel.cpp:84-152)
+ * become one kernel sequence with a device error word. */
+int dragon_gpu_advance(dragon_grid* g, double interval, int check_cfl, dragon_advance_stats* st);
+/* advance by a fixed number of CFL-limited steps (the interval is unbounded). */
+int dragon_gpu_advance_steps(dragon_grid* g, int nsteps, dragon_advance_stats* st);
+
+/* The CUDA stream the handle's kernels run on (cudaStream_t). */
+void* dragon_gpu_stream(dragon_grid* g);
+/* Device pointer to the current primitive planes (SoA, NF planes of
+ * dragon_gpu_plane_stride doubles; layout described in the design notes). */
+int dragon_gpu_device_state(dragon_grid* g, double** prim, long long* plane_stride, long long* pitch);
+/* Number of kernels this handle has launched since creation. */
+unsigned long long dragon_gpu_launch_count(const dragon_grid* g);
+/* Step-kernel timing: when enabled, CUDA events bracket every step-kernel
+ * launch on the handle's stream; read returns the summed milliseconds and the
+ * number of timed launches since the last reset (no reference counterpart:
+ * measurement hook for the roofline). */
+int dragon_gpu_profile_enable(dragon_grid* g, int on);
+int dragon_gpu_profile_read(dragon_grid* g, double* ms_total, long long* launches, int reset);
+
+const char* dragon_gpu_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DRAGON_GPU_H */
