@@ -34,7 +34,7 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-N = 1024
+N = 1024  # grid extent per axis (--grid overrides it, e.g. for profiling captures)
 CELL_BYTES = 80  # 5 FP64 primitive fields read + written per cell update
 METRIC = "cell-updates/s (2D unsplit CTU hydro, FP64)"
 WORKLOAD = "kelvin_helmholtz_2d_1024sq_hllc_vanleer_cfl0.3_periodic"
@@ -303,7 +303,12 @@ def main():
     ap.add_argument("--mixed", action="store_true", help="mixed FP32/FP64 path")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--grid", type=int, default=1024, help="cells per axis (default: the 1024^2 workload)")
     args = ap.parse_args()
+    global N, WORKLOAD
+    if args.grid != N:
+        N = args.grid
+        WORKLOAD = WORKLOAD.replace("1024sq", f"{N}sq")
     if args.impl == "reference":
         run_reference(args)
     else:
