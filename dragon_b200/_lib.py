@@ -113,6 +113,11 @@ SIGNATURES = {
     "dragon_gpu_profile_read": (
         ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong),
                        ctypes.c_int]),
+    "dragon_gpu_cfl_time_noalloc": (
+        ctypes.c_int,
+        [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, c_double_p,
+         ctypes.c_longlong, ctypes.c_longlong, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+         ctypes.c_double, ctypes.c_void_p, c_double_p]),
     "dragon_gpu_last_error": (ctypes.c_char_p, []),
 }
 

@@ -114,6 +114,10 @@ int solver_id(const dragon_config& c) {
 
 }  // namespace
 
+// Lets the library's other translation units report a failure through
+// dragon_gpu_last_error().
+void dragon_gpu_set_error_message(const char* msg) { g_last_error = msg; }
+
 struct dragon_grid {
     int dim = 0;
     int n[3] = {1, 1, 1};

@@ -153,6 +153,28 @@ unsigned long long dragon_gpu_launch_count(const dragon_grid* g);
 int dragon_gpu_profile_enable(dragon_grid* g, int on);
 int dragon_gpu_profile_read(dragon_grid* g, double* ms_total, long long* launches, int reset);
 
+/* CFL time step of a state the caller already holds on the device, without
+ * allocating anything (no counterpart in the reference: it serves callers
+ * that may not allocate device memory after start-up, such as applications
+ * that hand all GPU memory to their own pool, or loops that cannot afford the
+ * device-wide synchronisation of cudaMalloc/cudaFree). The state uses this
+ * library's layout: NF planes of plane_stride doubles, each a ghost-padded
+ * array with rows of `pitch` doubles (the last index contiguous), as
+ * dragon_gpu_device_state reports it. The result equals dragon_gpu_cfl_time's
+ * for the same state and configuration (cfl = CFL_CALCULATION, cfl_coeff =
+ * CFL_coeff). stream is a cudaStream_t (NULL for the default stream); the
+ * call returns once dt_out is written.
+ * Limits: working memory is one fixed ~128 KB array inside the library, kept
+ * on every GPU that loads it until the process exits; grids may have at most
+ * 16382 cells along x (2D/3D) or 16777214 cells (1D), larger ones are
+ * rejected with DRAGON_GPU_EINVAL. The first call on each device looks up the
+ * array's device address, so make it before any CUDA stream capture. All
+ * calls share the array: calls that overlap on the GPU race, so serialise
+ * them. */
+int dragon_gpu_cfl_time_noalloc(int dim, int nx, int ny, int nz, int ghosts, int mhd, const double* d_prim,
+                                long long plane_stride, long long pitch, double dx, double dy, double dz, int cfl,
+                                double cfl_coeff, void* stream, double* dt_out);
+
 const char* dragon_gpu_last_error(void);
 
 #ifdef __cplusplus
