@@ -26,11 +26,21 @@ def _need_gpu():
         pytest.fail("CUDA device required for -m gpu tests")
 
 
+class _PortModule:
+    """The C restatement with the reference handle's module interface."""
+
+    def __init__(self):
+        from oracle import port, refgrid
+        self.RefGrid = port.PortGrid
+        self.bc_entries_from = refgrid.bc_entries_from
+
+
 def ref_mod():
+    """The reference library when it was built, else the C restatement pinned to it."""
     from oracle import refgrid
-    if not refgrid.available("hydro"):
-        pytest.skip("reference oracle library not present")
-    return refgrid
+    if refgrid.available("hydro"):
+        return refgrid
+    return _PortModule()
 
 
 def make_pair(dim, n, d, w0, boundary, riemann=dg.RIEMANN_HLLX, limiter=dg.LIMITER_MC, cfl=dg.CFL_ADD, ghosts=2):
