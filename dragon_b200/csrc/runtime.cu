@@ -141,6 +141,9 @@ struct dragon_grid {
     cudaStream_t stream = nullptr;
     bool imax_valid = false;
     unsigned long long launches = 0;
+    // intermediates of the 2D MHD step
+    MhdScratch mhd_s{};
+    double* mhd_buf = nullptr;
     // step-kernel timing (dragon_gpu_profile_*)
     bool prof = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -205,7 +208,13 @@ int launch_step_t(dragon_grid* h, int c) {
     if (h->dim == 1) {
         const int np = h->n[0] + 2 * h->g;
         k_step1d<MHD, S, k1dTS><<<(np + k1dTS - 1) / k1dTS, k1dTS, 0, h->stream>>>(h->cg, h->w[c], h->w[c ^ 1], h->ctl, sa);
-    } else if (h->dim == 2 && !MHD) {
+    } else if constexpr (MHD) {
+        if (h->dim != 2) return fail(DRAGON_GPU_EUNSUPPORTED, "3D MHD step is not built in this version");
+        int rc = launch_step2d_mhd<S>(h->cg, h->fg, h->w[c], h->w[c ^ 1], h->B[c], h->B[c ^ 1], h->mhd_s, h->ctl, sa,
+                                      h->stream);
+        if (rc) return fail(DRAGON_GPU_ECUDA, "MHD step launch failed");
+        h->launches += kMhd2DKernels - 1;
+    } else if (h->dim == 2) {
         auto kern = k_step2d_hydro<S, k2dTI, k2dTJ, k2dNT>;
         const size_t smem = sizeof(Smem2DH<k2dTI, k2dTJ>);
         static bool attr_set = false;
@@ -215,10 +224,6 @@ int launch_step_t(dragon_grid* h, int c) {
         }
         dim3 grid((h->n[1] + k2dTJ - 1) / k2dTJ, (h->n[0] + k2dTI - 1) / k2dTI);
         kern<<<grid, k2dNT, smem, h->stream>>>(h->cg, h->w[c], h->w[c ^ 1], h->ctl, sa);
-    } else if (h->dim == 2 && MHD) {
-        int rc = launch_step2d_mhd<S>(h->cg, h->fg, h->w[c], h->w[c ^ 1], h->B[c], h->B[c ^ 1], h->ctl, sa, h->stream);
-        if (rc == -1) return fail(DRAGON_GPU_EUNSUPPORTED, "2D MHD step is not built in this version");
-        if (rc) return fail(DRAGON_GPU_ECUDA, "MHD step launch failed");
     } else {
         return fail(DRAGON_GPU_EUNSUPPORTED, "3D unsplit step is not built in this version");
     }
@@ -477,6 +482,18 @@ int dragon_gpu_grid_create(int dim, int nx, int ny, int nz, double dx, double dy
             cudaMemsetAsync(h->B[b], 0, sizeof(double) * 3 * h->fg.plane, h->stream);
         }
     }
+    if (h->mhd && dim == 2) {
+        const long long P = h->fg.plane;
+        if (cudaMalloc(&h->mhd_buf, sizeof(double) * MhdScratch::kPlanes * P) != cudaSuccess)
+            return cleanup(fail(DRAGON_GPU_ECUDA, "cudaMalloc MHD intermediates failed"));
+        h->mhd_s.hs = h->mhd_buf;
+        h->mhd_s.fx = h->mhd_buf + 32 * P;
+        h->mhd_s.fy = h->mhd_buf + 40 * P;
+        h->mhd_s.er = h->mhd_buf + 48 * P;
+        h->mhd_s.e0 = h->mhd_buf + 51 * P;
+        h->mhd_s.eh = h->mhd_buf + 54 * P;
+        h->mhd_s.plane = P;
+    }
     if (cudaMalloc(&h->ctl, sizeof(StepCtl)) != cudaSuccess) return cleanup(fail(DRAGON_GPU_ECUDA, "cudaMalloc ctl failed"));
     cudaMemsetAsync(h->ctl, 0, sizeof(StepCtl), h->stream);
     if (cudaMallocHost(&h->hctl, sizeof(StepCtl)) != cudaSuccess) return cleanup(fail(DRAGON_GPU_ECUDA, "cudaMallocHost failed"));
@@ -502,6 +519,7 @@ int dragon_gpu_grid_destroy(dragon_grid* h) {
         if (h->B[b]) cudaFree(h->B[b]);
     }
     if (h->ctl) cudaFree(h->ctl);
+    if (h->mhd_buf) cudaFree(h->mhd_buf);
     if (h->hctl) cudaFreeHost(h->hctl);
     if (h->dbcs) cudaFree(h->dbcs);
     if (h->stage) cudaFree(h->stage);
