@@ -170,6 +170,14 @@ __device__ __forceinline__ void store_prim(double* __restrict__ w, long long pla
     }
 }
 
+// Warp-aggregated statistics: one atomic per warp and counter instead of one
+// per thread (threads that left early are simply not in the mask).
+__device__ __forceinline__ void warp_add_stat(unsigned long long* dst, unsigned v) {
+    const unsigned mask = __activemask();
+    const unsigned sum = __reduce_add_sync(mask, v);
+    if ((threadIdx.x & 31) == (unsigned)(__ffs(mask) - 1) && sum) atomicAdd(dst, (unsigned long long)sum);
+}
+
 // Parameters every step kernel receives by value.
 struct StepArgs {
     double dx, dy, dz;

@@ -20,6 +20,7 @@
 #include "../../include/dragon_gpu.h"
 #include "boundary.cuh"
 #include "step_hydro.cuh"
+#include "step3d.cuh"
 #include "step_mhd.cuh"
 
 using namespace dgpu;
@@ -144,6 +145,9 @@ struct dragon_grid {
     // intermediates of the 2D MHD step
     MhdScratch mhd_s{};
     double* mhd_buf = nullptr;
+    // intermediates of the 3D hydro step
+    Hydro3DScratch h3_s{};
+    double* h3_buf = nullptr;
     // step-kernel timing (dragon_gpu_profile_*)
     bool prof = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -225,7 +229,9 @@ int launch_step_t(dragon_grid* h, int c) {
         dim3 grid((h->n[1] + k2dTJ - 1) / k2dTJ, (h->n[0] + k2dTI - 1) / k2dTI);
         kern<<<grid, k2dNT, smem, h->stream>>>(h->cg, h->w[c], h->w[c ^ 1], h->ctl, sa);
     } else {
-        return fail(DRAGON_GPU_EUNSUPPORTED, "3D unsplit step is not built in this version");
+        int rc = launch_step3d_hydro<S>(h->cg, h->w[c], h->w[c ^ 1], h->h3_s, h->ctl, sa, h->stream);
+        if (rc) return fail(DRAGON_GPU_ECUDA, "3D step launch failed");
+        h->launches += kHydro3DKernels - 1;
     }
     CK(cudaGetLastError());
     if (h->prof) {
@@ -494,6 +500,15 @@ int dragon_gpu_grid_create(int dim, int nx, int ny, int nz, double dx, double dy
         h->mhd_s.eh = h->mhd_buf + 54 * P;
         h->mhd_s.plane = P;
     }
+    if (!h->mhd && dim == 3) {
+        const long long P = h->cg.plane;
+        if (cudaMalloc(&h->h3_buf, sizeof(double) * Hydro3DScratch::kPlanes * P) != cudaSuccess)
+            return cleanup(fail(DRAGON_GPU_ECUDA, "cudaMalloc 3D intermediates failed"));
+        h->h3_s.hs = h->h3_buf;
+        h->h3_s.pf = h->h3_buf + 30 * P;
+        h->h3_s.cf = h->h3_buf + 45 * P;
+        h->h3_s.plane = P;
+    }
     if (cudaMalloc(&h->ctl, sizeof(StepCtl)) != cudaSuccess) return cleanup(fail(DRAGON_GPU_ECUDA, "cudaMalloc ctl failed"));
     cudaMemsetAsync(h->ctl, 0, sizeof(StepCtl), h->stream);
     if (cudaMallocHost(&h->hctl, sizeof(StepCtl)) != cudaSuccess) return cleanup(fail(DRAGON_GPU_ECUDA, "cudaMallocHost failed"));
@@ -520,6 +535,7 @@ int dragon_gpu_grid_destroy(dragon_grid* h) {
     }
     if (h->ctl) cudaFree(h->ctl);
     if (h->mhd_buf) cudaFree(h->mhd_buf);
+    if (h->h3_buf) cudaFree(h->h3_buf);
     if (h->hctl) cudaFreeHost(h->hctl);
     if (h->dbcs) cudaFree(h->dbcs);
     if (h->stage) cudaFree(h->stage);

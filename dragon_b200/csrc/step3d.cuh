@@ -1,0 +1,303 @@
+// 3D unsplit CTU hydro step (Grid3D::unsplit_step hydro branch,
+// Unsplit.cpp:115-206; the 12-solve ctu_sweep_hydro, CTU.cpp:222-370) as six
+// kernels over global intermediates:
+//   K1 half states along x, y, z for cells [-1, n]^3
+//   K2 predictor fluxes (CTU.cpp:229-232)
+//   K3 the six corner-corrected fluxes F_Xz, F_Yz, F_Xy, F_Zy, F_Yx, F_Zx
+//      (computeCTUFlux_X/Y/Z, CTU.cpp:306-370; dt/3 transverse weights)
+//   K4 the two sequential transverse corrections of every half state
+//      (correctState, CTU.cpp:246-260,280-301)
+//   K5 final fluxes (Unsplit.cpp:102-105)
+//   K6 conservative update, physicality, CFL speed
+// Index ranges are the reference's, so every Riemann pivot that can fail does.
+#pragma once
+
+#include "grid.cuh"
+#include "recon.cuh"
+#include "riemann.cuh"
+
+namespace dgpu {
+
+struct Hydro3DScratch {
+    double* hs;    // 6 x 5 planes: xL, xR, yL, yR, zL, zR
+    double* pf;    // 3 x 5 planes: predictor F_X, F_Y, F_Z; then final fluxes
+    double* cf;    // 6 x 5 planes: F_Xz, F_Yz, F_Xy, F_Zy, F_Yx, F_Zx
+    long long plane;
+    static constexpr int kPlanes = 30 + 15 + 30;
+};
+
+struct Step3DArgs {
+    Geo G;
+    const double* w;
+    double* wout;
+    Hydro3DScratch S;
+    StepCtl* ctl;
+    StepArgs sa;
+};
+
+__device__ __forceinline__ bool h3_skip(const StepCtl* ctl, int* s) {
+    if (threadIdx.x == 0) *s = (*(const volatile int*)&ctl->err) | (*(const volatile int*)&ctl->done);
+    __syncthreads();
+    return *s != 0;
+}
+
+// cell of a flat launch over the box [lo, lo + ext) per axis, last index fastest
+__device__ __forceinline__ bool box_cell(long long t, const int* lo, const int* ext, int& i, int& j, int& k) {
+    const long long ek = ext[2], ej = ext[1];
+    if (t >= (long long)ext[0] * ej * ek) return false;
+    k = lo[2] + (int)(t % ek);
+    j = lo[1] + (int)((t / ek) % ej);
+    i = lo[0] + (int)(t / (ek * ej));
+    return true;
+}
+
+__device__ __forceinline__ Prim<double> ld5(const double* a, long long P, long long m) { return load_prim<false>(a, P, m); }
+__device__ __forceinline__ void st5(double* a, long long P, long long m, const Prim<double>& w) { store_prim<false>(a, P, m, w); }
+__device__ __forceinline__ Cons<double> ldc5(const double* a, long long P, long long m) {
+    return Cons<double>{a[m], a[P + m], a[2 * P + m], a[3 * P + m], a[4 * P + m], 0, 0, 0};
+}
+__device__ __forceinline__ void stc5(double* a, long long P, long long m, const Cons<double>& u) {
+    a[m] = u.rho; a[P + m] = u.E; a[2 * P + m] = u.mx; a[3 * P + m] = u.my; a[4 * P + m] = u.mz;
+}
+
+// K1: MUSCL half states along all three axes (computeHalfStates_X/Y/Z, Unsplit.cpp:344-436).
+__global__ void k_h3_halfstates(Step3DArgs A) {
+    __shared__ int s;
+    if (h3_skip(A.ctl, &s)) return;
+    const Geo& G = A.G;
+    const int lo[3] = {-1, -1, -1}, ext[3] = {G.n[0] + 2, G.n[1] + 2, G.n[2] + 2};
+    int i, j, k;
+    if (!box_cell(blockIdx.x * (long long)blockDim.x + threadIdx.x, lo, ext, i, j, k)) return;
+    const double dt = *(const volatile double*)&A.ctl->t1;
+    const double dts[3] = {dt / A.sa.dx, dt / A.sa.dy, dt / A.sa.dz};
+    const long long P = G.plane, m = gidx3(G, i, j, k);
+    const Prim<double> wc = ld5(A.w, P, m);
+    int fo = 0;
+#pragma unroll
+    for (int ax = 0; ax < 3; ax++) {
+        const int di = ax == 0, dj = ax == 1, dk = ax == 2;
+        Prim<double> wl = ld5(A.w, P, gidx3(G, i - di, j - dj, k - dk));
+        Prim<double> wr = ld5(A.w, P, gidx3(G, i + di, j + dj, k + dk));
+        Prim<double> c = wc, L, R;
+        if (ax == 1) { swap_xy(wl); swap_xy(c); swap_xy(wr); }
+        if (ax == 2) { swap_xz(wl); swap_xz(c); swap_xz(wr); }
+        fo += !muscl<false>(A.sa.limiter, wl, L, c, R, wr, dts[ax], 0.0, 0.0, 0.0);
+        if (ax == 1) { swap_xy(L); swap_xy(R); }
+        if (ax == 2) { swap_xz(L); swap_xz(R); }
+        st5(A.S.hs + (10 * ax) * A.S.plane, A.S.plane, m, L);
+        st5(A.S.hs + (10 * ax + 5) * A.S.plane, A.S.plane, m, R);
+    }
+    warp_add_stat(&A.ctl->muscl_first_order, fo);
+}
+
+template <int SOLVER, int AX>
+__device__ __forceinline__ void h3_flux(const Step3DArgs& A, double* out, int i, int j, int k, double dtn,
+                                        int stage, FaceStats* st) {
+    const Geo& G = A.G;
+    const long long SP = A.S.plane;
+    const int di = AX == 0, dj = AX == 1, dk = AX == 2;
+    const long long m = gidx3(G, i, j, k);
+    Prim<double> L = ld5(A.S.hs + (10 * AX + 5) * SP, SP, gidx3(G, i - di, j - dj, k - dk));
+    Prim<double> R = ld5(A.S.hs + (10 * AX) * SP, SP, m);
+    Cons<double> F;
+    const ExactOpts eo{A.sa.exact_max_iters, A.sa.exact_tol};
+    if (!face_flux<false, SOLVER, AX>(L, R, dtn, eo, F, st)) record_error(A.ctl, stage, m);
+    stc5(out, SP, m, F);
+}
+
+__device__ __forceinline__ void h3_stats(StepCtl* ctl, const FaceStats& st) {
+    warp_add_stat(&ctl->pivots_exact, st.pivot_exact);
+    warp_add_stat(&ctl->newton_iters, st.newton_iters);
+    warp_add_stat(&ctl->exact_calls, st.exact_calls);
+    warp_add_stat(&ctl->trrs, st.trrs);
+}
+
+// K2: predictor fluxes F_X on [0,nx]x[-1,ny]x[-1,nz], F_Y on [-1,nx]x[0,ny]x[-1,nz],
+// F_Z on [-1,nx]x[-1,ny]x[0,nz] (CTU.cpp:230-232).
+template <int SOLVER>
+__global__ void k_h3_prelim(Step3DArgs A) {
+    __shared__ int s;
+    if (h3_skip(A.ctl, &s)) return;
+    const Geo& G = A.G;
+    const int lo[3] = {-1, -1, -1}, ext[3] = {G.n[0] + 2, G.n[1] + 2, G.n[2] + 2};
+    int i, j, k;
+    if (!box_cell(blockIdx.x * (long long)blockDim.x + threadIdx.x, lo, ext, i, j, k)) return;
+    const double dt = *(const volatile double*)&A.ctl->t1;
+    FaceStats st{0, 0, 0, 0, 0};
+    const long long SP = A.S.plane;
+    if (i >= 0) h3_flux<SOLVER, 0>(A, A.S.pf, i, j, k, dt / A.sa.dx, ST_PRELIM_FLUX, &st);
+    if (j >= 0) h3_flux<SOLVER, 1>(A, A.S.pf + 5 * SP, i, j, k, dt / A.sa.dy, ST_PRELIM_FLUX, &st);
+    if (k >= 0) h3_flux<SOLVER, 2>(A, A.S.pf + 10 * SP, i, j, k, dt / A.sa.dz, ST_PRELIM_FLUX, &st);
+    h3_stats(A.ctl, st);
+}
+
+// One corner-corrected flux (computeCTUFlux_*, CTU.cpp:306-370): the half
+// states on both sides of face q along AX are corrected by the transverse
+// predictor flux T along TD with weight dtT, then solved along AX.
+template <int SOLVER, int AX, int TD>
+__device__ __forceinline__ void h3_ctu_flux(const Step3DArgs& A, const double* T, double* out, int i, int j, int k,
+                                            double dtn, double dtT, FaceStats* st) {
+    const Geo& G = A.G;
+    const long long SP = A.S.plane;
+    const int di = AX == 0, dj = AX == 1, dk = AX == 2;
+    const int ti = TD == 0, tj = TD == 1, tk = TD == 2;
+    auto trans = [&](int a, int b, int c) {
+        const Cons<double> t1 = ldc5(T, SP, gidx3(G, a + ti, b + tj, c + tk)), t0 = ldc5(T, SP, gidx3(G, a, b, c));
+        return c_mul<false>(c_sub<false>(t1, t0), dtT);
+    };
+    const Prim<double> L = to_prim<false>(c_sub<false>(
+        to_cons<false>(ld5(A.S.hs + (10 * AX + 5) * SP, SP, gidx3(G, i - di, j - dj, k - dk))), trans(i - di, j - dj, k - dk)));
+    const long long m = gidx3(G, i, j, k);
+    const Prim<double> R = to_prim<false>(c_sub<false>(to_cons<false>(ld5(A.S.hs + (10 * AX) * SP, SP, m)), trans(i, j, k)));
+    Cons<double> F;
+    const ExactOpts eo{A.sa.exact_max_iters, A.sa.exact_tol};
+    if (!face_flux<false, SOLVER, AX>(L, R, dtn, eo, F, st)) record_error(A.ctl, ST_PRELIM_FLUX, m);
+    stc5(out, SP, m, F);
+}
+
+// K3: the six corner-corrected fluxes over the reference's ranges: on the
+// normal axis faces [0, n]; on the transverse-flux axis cells [0, n); on the
+// third axis cells [-1, n].
+template <int SOLVER>
+__global__ void k_h3_ctu(Step3DArgs A) {
+    __shared__ int s;
+    if (h3_skip(A.ctl, &s)) return;
+    const Geo& G = A.G;
+    const int lo[3] = {-1, -1, -1}, ext[3] = {G.n[0] + 2, G.n[1] + 2, G.n[2] + 2};
+    int i, j, k;
+    if (!box_cell(blockIdx.x * (long long)blockDim.x + threadIdx.x, lo, ext, i, j, k)) return;
+    const int nx = G.n[0], ny = G.n[1], nz = G.n[2];
+    const double dt = *(const volatile double*)&A.ctl->t1;
+    const double dt_dx = dt / A.sa.dx, dt_dy = dt / A.sa.dy, dt_dz = dt / A.sa.dz;
+    const long long SP = A.S.plane;
+    const double* FX = A.S.pf;
+    const double* FY = A.S.pf + 5 * SP;
+    const double* FZ = A.S.pf + 10 * SP;
+    FaceStats st{0, 0, 0, 0, 0};
+    // F_Xz: i in [0,nx], j in [-1,ny], k in [0,nz)
+    if (i >= 0 && k >= 0 && k < nz) h3_ctu_flux<SOLVER, 0, 2>(A, FZ, A.S.cf, i, j, k, dt_dx, dt_dz / 3.0, &st);
+    // F_Yz: i in [-1,nx], j in [0,ny], k in [0,nz)
+    if (j >= 0 && k >= 0 && k < nz) h3_ctu_flux<SOLVER, 1, 2>(A, FZ, A.S.cf + 5 * SP, i, j, k, dt_dy, dt_dz / 3.0, &st);
+    // F_Xy: i in [0,nx], j in [0,ny), k in [-1,nz]
+    if (i >= 0 && j >= 0 && j < ny) h3_ctu_flux<SOLVER, 0, 1>(A, FY, A.S.cf + 10 * SP, i, j, k, dt_dx, dt_dy / 3.0, &st);
+    // F_Zy: i in [-1,nx], j in [0,ny), k in [0,nz]
+    if (j >= 0 && j < ny && k >= 0) h3_ctu_flux<SOLVER, 2, 1>(A, FY, A.S.cf + 15 * SP, i, j, k, dt_dz, dt_dy / 3.0, &st);
+    // F_Yx: i in [0,nx), j in [0,ny], k in [-1,nz]
+    if (i >= 0 && i < nx && j >= 0) h3_ctu_flux<SOLVER, 1, 0>(A, FX, A.S.cf + 20 * SP, i, j, k, dt_dy, dt_dx / 3.0, &st);
+    // F_Zx: i in [0,nx), j in [-1,ny], k in [0,nz]
+    if (i >= 0 && i < nx && k >= 0) h3_ctu_flux<SOLVER, 2, 0>(A, FX, A.S.cf + 25 * SP, i, j, k, dt_dz, dt_dx / 3.0, &st);
+    h3_stats(A.ctl, st);
+}
+
+// in-place correction of one half-state pair by a flux difference along D
+__device__ __forceinline__ void h3_correct(const Step3DArgs& A, int state_ax, const double* F, int D, double w,
+                                           int i, int j, int k) {
+    const Geo& G = A.G;
+    const long long SP = A.S.plane, m = gidx3(G, i, j, k);
+    const Cons<double> tr = c_mul<false>(
+        c_sub<false>(ldc5(F, SP, gidx3(G, i + (D == 0), j + (D == 1), k + (D == 2))), ldc5(F, SP, m)), w);
+    double* L = A.S.hs + (10 * state_ax) * SP;
+    double* R = A.S.hs + (10 * state_ax + 5) * SP;
+    st5(L, SP, m, to_prim<false>(c_sub<false>(to_cons<false>(ld5(L, SP, m)), tr)));
+    st5(R, SP, m, to_prim<false>(c_sub<false>(to_cons<false>(ld5(R, SP, m)), tr)));
+}
+
+// K4: x states (cells [-1,nx]x[0,ny)x[0,nz)) by F_Yz then F_Zy; y states
+// ([0,nx)x[-1,ny]x[0,nz)) by F_Xz then F_Zx; z states ([0,nx)x[0,ny)x[-1,nz])
+// by F_Xy then F_Yx (CTU.cpp:246-260).
+__global__ void k_h3_correct(Step3DArgs A) {
+    __shared__ int s;
+    if (h3_skip(A.ctl, &s)) return;
+    const Geo& G = A.G;
+    const int lo[3] = {-1, -1, -1}, ext[3] = {G.n[0] + 2, G.n[1] + 2, G.n[2] + 2};
+    int i, j, k;
+    if (!box_cell(blockIdx.x * (long long)blockDim.x + threadIdx.x, lo, ext, i, j, k)) return;
+    const int nx = G.n[0], ny = G.n[1], nz = G.n[2];
+    const double dt = *(const volatile double*)&A.ctl->t1;
+    const double hx = 0.5 * (dt / A.sa.dx), hy = 0.5 * (dt / A.sa.dy), hz = 0.5 * (dt / A.sa.dz);
+    const long long SP = A.S.plane;
+    const double* cf = A.S.cf;
+    if (j >= 0 && j < ny && k >= 0 && k < nz) {
+        h3_correct(A, 0, cf + 5 * SP, 1, hy, i, j, k);    // F_Yz
+        h3_correct(A, 0, cf + 15 * SP, 2, hz, i, j, k);   // F_Zy
+    }
+    if (i >= 0 && i < nx && k >= 0 && k < nz) {
+        h3_correct(A, 1, cf, 0, hx, i, j, k);             // F_Xz
+        h3_correct(A, 1, cf + 25 * SP, 2, hz, i, j, k);   // F_Zx
+    }
+    if (i >= 0 && i < nx && j >= 0 && j < ny) {
+        h3_correct(A, 2, cf + 10 * SP, 0, hx, i, j, k);   // F_Xy
+        h3_correct(A, 2, cf + 20 * SP, 1, hy, i, j, k);   // F_Yx
+    }
+}
+
+// K5: final fluxes on [0,n] along the normal axis, [0,n) on the others.
+template <int SOLVER>
+__global__ void k_h3_final(Step3DArgs A) {
+    __shared__ int s;
+    if (h3_skip(A.ctl, &s)) return;
+    const Geo& G = A.G;
+    const int lo[3] = {0, 0, 0}, ext[3] = {G.n[0] + 1, G.n[1] + 1, G.n[2] + 1};
+    int i, j, k;
+    if (!box_cell(blockIdx.x * (long long)blockDim.x + threadIdx.x, lo, ext, i, j, k)) return;
+    const int nx = G.n[0], ny = G.n[1], nz = G.n[2];
+    const double dt = *(const volatile double*)&A.ctl->t1;
+    FaceStats st{0, 0, 0, 0, 0};
+    const long long SP = A.S.plane;
+    if (j < ny && k < nz) h3_flux<SOLVER, 0>(A, A.S.pf, i, j, k, dt / A.sa.dx, ST_FINAL_FLUX, &st);
+    if (i < nx && k < nz) h3_flux<SOLVER, 1>(A, A.S.pf + 5 * SP, i, j, k, dt / A.sa.dy, ST_FINAL_FLUX, &st);
+    if (i < nx && j < ny) h3_flux<SOLVER, 2>(A, A.S.pf + 10 * SP, i, j, k, dt / A.sa.dz, ST_FINAL_FLUX, &st);
+    h3_stats(A.ctl, st);
+}
+
+// K6: conservative update of the interior (applyFluxes 3D, Unsplit.cpp:272-288),
+// physicality, CFL speed of the committed state.
+__global__ void k_h3_update(Step3DArgs A) {
+    __shared__ int s;
+    __shared__ double red[32];
+    if (h3_skip(A.ctl, &s)) return;
+    const Geo& G = A.G;
+    const int lo[3] = {0, 0, 0}, ext[3] = {G.n[0], G.n[1], G.n[2]};
+    int i, j, k;
+    double vmax = 0.0;
+    if (box_cell(blockIdx.x * (long long)blockDim.x + threadIdx.x, lo, ext, i, j, k)) {
+        const double dt = *(const volatile double*)&A.ctl->t1;
+        const double dt_dx = dt / A.sa.dx, dt_dy = dt / A.sa.dy, dt_dz = dt / A.sa.dz;
+        const long long P = G.plane, SP = A.S.plane, m = gidx3(G, i, j, k);
+        const double* FX = A.S.pf;
+        const double* FY = A.S.pf + 5 * SP;
+        const double* FZ = A.S.pf + 10 * SP;
+        Cons<double> U = to_cons<false>(ld5(A.w, P, m));
+        U = c_add<false>(U, c_mul<false>(c_sub<false>(ldc5(FX, SP, m), ldc5(FX, SP, gidx3(G, i + 1, j, k))), dt_dx));
+        U = c_add<false>(U, c_mul<false>(c_sub<false>(ldc5(FY, SP, m), ldc5(FY, SP, gidx3(G, i, j + 1, k))), dt_dy));
+        U = c_add<false>(U, c_mul<false>(c_sub<false>(ldc5(FZ, SP, m), ldc5(FZ, SP, gidx3(G, i, j, k + 1))), dt_dz));
+        const Prim<double> nw = to_prim<false>(U);
+        if (!is_finite<false>(U)) record_error(A.ctl, ST_NAN, m);
+        else if (!is_physical<false>(nw)) record_error(A.ctl, ST_UNPHYSICAL, m);
+        st5(A.wout, P, m, nw);
+        vmax = cfl_speed<false>(nw, A.sa.cfl, A.sa.dx, A.sa.dy, A.sa.dz);
+    }
+    vmax = block_max(vmax, red);
+    if (threadIdx.x == 0) atomic_max_speed(&A.ctl->vmax[A.sa.slot_out], vmax);
+}
+
+template <int SOLVER>
+inline int launch_step3d_hydro(const Geo& G, const double* w, double* wout, const Hydro3DScratch& S, StepCtl* ctl,
+                               const StepArgs& sa, cudaStream_t st) {
+    Step3DArgs A{G, w, wout, S, ctl, sa};
+    auto blocks = [](long long n) { return (int)((n + 255) / 256); };
+    const long long box = (long long)(G.n[0] + 2) * (G.n[1] + 2) * (G.n[2] + 2);
+    const long long fbox = (long long)(G.n[0] + 1) * (G.n[1] + 1) * (G.n[2] + 1);
+    const long long cells = (long long)G.n[0] * G.n[1] * G.n[2];
+    if (cudaMemcpyAsync(wout, w, sizeof(double) * 5 * G.plane, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return 1;
+    k_h3_halfstates<<<blocks(box), 256, 0, st>>>(A);
+    k_h3_prelim<SOLVER><<<blocks(box), 256, 0, st>>>(A);
+    k_h3_ctu<SOLVER><<<blocks(box), 256, 0, st>>>(A);
+    k_h3_correct<<<blocks(box), 256, 0, st>>>(A);
+    k_h3_final<SOLVER><<<blocks(fbox), 256, 0, st>>>(A);
+    k_h3_update<<<blocks(cells), 256, 0, st>>>(A);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+constexpr int kHydro3DKernels = 6;
+
+}  // namespace dgpu

@@ -182,7 +182,7 @@ __global__ void k_mhd2d_halfstates(Mhd2DArgs A) {
     store_prim<true>(A.S.hs + 16 * SP, SP, m, L);
     store_prim<true>(A.S.hs + 24 * SP, SP, m, R);
     store_v3(A.S.er, SP, m, body_e(wc));
-    if (fo) atomicAdd(&A.ctl->muscl_first_order, (unsigned long long)fo);
+    warp_add_stat(&A.ctl->muscl_first_order, fo);
 }
 
 // K2: predictor fluxes: x faces [-1, nx+1] x rows [-2, ny+1], y faces cols
@@ -212,7 +212,7 @@ __global__ void k_mhd2d_prelim(Mhd2DArgs A) {
         face_flux<true, SOLVER, 1>(L, R, dt_dy, eo, Fl, &st);
         store_cons8(A.S.fy, SP, gidx2(F, i, j), Fl);
     }
-    if (st.hlld_to_hlle) atomicAdd(&A.ctl->hlld_to_hlle, (unsigned long long)st.hlld_to_hlle);
+    warp_add_stat(&A.ctl->hlld_to_hlle, st.hlld_to_hlle);
 }
 
 // Corner E from face fluxes plus Gardiner-Stone upwinding against a body E
@@ -342,7 +342,7 @@ __global__ void k_mhd2d_final_flux(Mhd2DArgs A) {
         face_flux<true, SOLVER, 1>(L, R, dt_dy, eo, Fl, &st);
         store_cons8(A.S.fy, SP, gidx2(F, i, j), Fl);
     }
-    if (st.hlld_to_hlle) atomicAdd(&A.ctl->hlld_to_hlle, (unsigned long long)st.hlld_to_hlle);
+    warp_add_stat(&A.ctl->hlld_to_hlle, st.hlld_to_hlle);
 }
 
 // K6: final corner E on edges [0, nx]^2 against the half-step body E.
