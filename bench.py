@@ -245,6 +245,53 @@ def run_gpu(args):
         kmax = kms.value
     ms_per_step = ms / args.steps
     value = ws * N * N * args.steps / (ms / 1e3)
+    fp64_state = G.w.copy()  # after warm-up + K steps, for the mixed path's L1
+
+    # ---- mixed FP32/FP64 path: same input, same steps, same timing procedure
+    mixed = None
+    if not args.no_mixed:
+        cfg_m = dg.Config(riemann=dg.RIEMANN_HLLC, limiter=dg.LIMITER_VANLEER, cfl=dg.CFL_ADD, precision=dg.PREC_MIXED)
+        Gm = dg.Grid2D(N, N, dx, dy, ghosts=2, config=cfg_m)
+        Gm.w[...] = w0
+        Gm.boundary = dg.Periodic()
+        Lm, hm = Gm._lib, Gm._h
+        stream_m = torch.cuda.ExternalStream(Lm.dragon_gpu_stream(hm), device=dev)
+        Gm.advance_steps(max(args.warmup, 1))
+        Lm.dragon_gpu_profile_enable(hm, 1)
+        Lm.dragon_gpu_profile_read(hm, None, None, 1)
+        ev = []
+        barrier()
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream_m):
+                flush.fill_(1.0)
+                a_ = torch.cuda.Event(enable_timing=True)
+                b_ = torch.cuda.Event(enable_timing=True)
+                a_.record(stream_m)
+            _lib.check(Lm.dragon_gpu_advance_steps(hm, 1, None))
+            b_.record(stream_m)
+            ev.append((a_, b_))
+        torch.cuda.synchronize()
+        barrier()
+        ms_m = sum(a.elapsed_time(b) for a, b in ev)
+        kms_m = __import__("ctypes").c_double()
+        kn_m = __import__("ctypes").c_longlong()
+        Lm.dragon_gpu_profile_read(hm, __import__("ctypes").byref(kms_m), __import__("ctypes").byref(kn_m), 1)
+        if ws > 1:
+            t = torch.tensor([ms_m], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms_m = t.item()
+        g = 2
+        l1 = problems.rel_l1(Gm.w[g:-g, g:-g], fp64_state[g:-g, g:-g])
+        km = kms_m.value / max(1, kn_m.value)
+        mixed = {"value": ws * N * N * args.steps / (ms_m / 1e3), "unit": "cell-updates/s",
+                 "ms_per_step": ms_m / args.steps, "speedup_vs_fp64": ms / ms_m,
+                 "rel_l1_vs_fp64_per_field": [float(x) for x in l1],
+                 "rel_l1_fields": ["rho", "p", "vx", "vy", "vz"],
+                 "steps_compared": args.steps + max(args.warmup, 1),
+                 "kernel": "k_step2d_hydro_mixed", "kernel_ms_avg": km,
+                 "roofline_hbm_frac": (N * N * CELL_BYTES / (km / 1e3) / 1e9) / measured_peaks()[0] if km > 0 else None}
+        Gm.close()
 
     # ---- e2e: through the C ABI from pinned host memory, every step
     host_in = torch.from_numpy(G.w.copy()).pin_memory()
@@ -296,6 +343,8 @@ def run_gpu(args):
             "clocks": clocks,
             "wall_s_timed": t_wall,
         }
+        if mixed is not None:
+            line["mixed"] = mixed
         if not args.no_cpu_baseline:
             cb, why = reference_baseline(1000, 0, budget_s=args.cpu_budget)
             line["cpu_baseline"] = cb if cb else {"unavailable": why}
@@ -313,6 +362,7 @@ def main():
     ap.add_argument("--impl", default="dragon_b200", choices=["dragon_b200", "reference"])
     ap.add_argument("--mixed", action="store_true", help="mixed FP32/FP64 path")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurement")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--grid", type=int, default=1024, help="cells per axis (default: the 1024^2 workload)")
     args = ap.parse_args()

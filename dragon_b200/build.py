@@ -1,36 +1,40 @@
 """In-tree build of the CUDA library (sm_100a) behind include/dragon_gpu.h.
 
-The FP64 kernels are compiled with --fmad=false so that no a*b+c is fused:
-together with IEEE division and square root this keeps the FP64 path's
-arithmetic identical to the reference's (compiled without contraction).
+Each translation unit is compiled on its own, then linked into
+dragon_b200/libdragon_gpu.so:
+  * the FP64 kernels with --fmad=false, so no a*b+c is fused: together with
+    IEEE division and square root this keeps the FP64 path's arithmetic
+    identical to the reference's (compiled without contraction);
+  * the mixed-precision kernels (step_mixed.cu) with FMA contraction and fast
+    single-precision division / square root; these flags leave FP64 alone.
 """
 from __future__ import annotations
 
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
+OBJ = os.path.join(ROOT, "_build", "obj")
 LIB = os.path.join(HERE, "libdragon_gpu.so")
 
-NVCC_FLAGS = [
-    "-std=c++17", "-O3", "-lineinfo",
-    "-gencode", "arch=compute_100a,code=sm_100a",
-    "--fmad=false",
-    "-Xcompiler", "-fPIC", "-shared",
-    "-I" + os.path.join(ROOT, "include"),
-]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+BASE = ["-std=c++17", "-O3", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC", "-I" + os.path.join(ROOT, "include")]
+EXACT = ["--fmad=false"]
+FAST32 = ["--fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
+PER_FILE = {"step_mixed.cu": FAST32}
 
 
 def _sources():
-    return [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith(".cu")]
+    return [f for f in sorted(os.listdir(CSRC)) if f.endswith(".cu")]
 
 
 def _deps():
     return [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh", ".h"))] + [
-        os.path.join(ROOT, "include", "dragon_gpu.h")]
+        os.path.join(ROOT, "include", "dragon_gpu.h"), os.path.abspath(__file__)]
 
 
 def needs_build() -> bool:
@@ -45,10 +49,19 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not needs_build():
         return LIB
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc, *NVCC_FLAGS, "-o", LIB + ".tmp", *_sources()]
-    if verbose:
-        print(" ".join(cmd), file=sys.stderr)
-    subprocess.run(cmd, check=True, cwd=CSRC)
+    os.makedirs(OBJ, exist_ok=True)
+
+    def compile_one(src):
+        obj = os.path.join(OBJ, src.replace(".cu", ".o"))
+        cmd = [nvcc, *BASE, *PER_FILE.get(src, EXACT), "-c", os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True, cwd=CSRC)
+        return obj
+
+    with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
+        objs = list(ex.map(compile_one, _sources()))
+    subprocess.run([nvcc, *ARCH, "-shared", "-o", LIB + ".tmp", *objs], check=True)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

@@ -19,9 +19,10 @@
 
 #include "../../include/dragon_gpu.h"
 #include "boundary.cuh"
-#include "step_hydro.cuh"
-#include "step3d.cuh"
-#include "step_mhd.cuh"
+#include "launchers.h"
+#include "recon.cuh"
+#include "riemann.cuh"
+#include "scratch.h"
 
 using namespace dgpu;
 
@@ -42,8 +43,6 @@ int fail(int code, const std::string& msg) {
     } while (0)
 
 constexpr int kBatch = 64;
-constexpr int k2dTI = 8, k2dTJ = 32, k2dNT = 256;
-constexpr int k1dTS = 128;
 
 long long round_up(long long a, long long b) { return (a + b - 1) / b * b; }
 
@@ -200,8 +199,7 @@ void collect_profile(dragon_grid* h) {
     h->ev_pending.clear();
 }
 
-template <bool MHD, int S>
-int launch_step_t(dragon_grid* h, int c) {
+int launch_step(dragon_grid* h, int c) {
     const StepArgs sa = step_args(h, c ^ 1);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (h->prof) {
@@ -209,54 +207,29 @@ int launch_step_t(dragon_grid* h, int c) {
         e1 = take_event(h);
         cudaEventRecord(e0, h->stream);
     }
+    int rc = 0, nk = 1;
     if (h->dim == 1) {
-        const int np = h->n[0] + 2 * h->g;
-        k_step1d<MHD, S, k1dTS><<<(np + k1dTS - 1) / k1dTS, k1dTS, 0, h->stream>>>(h->cg, h->w[c], h->w[c ^ 1], h->ctl, sa);
-    } else if constexpr (MHD) {
+        rc = launch_step1d(h->mhd, h->solver, h->cg, h->w[c], h->w[c ^ 1], h->ctl, sa, h->stream);
+    } else if (h->mhd) {
         if (h->dim != 2) return fail(DRAGON_GPU_EUNSUPPORTED, "3D MHD step is not built in this version");
-        int rc = launch_step2d_mhd<S>(h->cg, h->fg, h->w[c], h->w[c ^ 1], h->B[c], h->B[c ^ 1], h->mhd_s, h->ctl, sa,
-                                      h->stream);
-        if (rc) return fail(DRAGON_GPU_ECUDA, "MHD step launch failed");
-        h->launches += kMhd2DKernels - 1;
+        rc = launch_step2d_mhd(h->solver, h->cg, h->fg, h->w[c], h->w[c ^ 1], h->B[c], h->B[c ^ 1], h->mhd_s, h->ctl,
+                               sa, h->stream);
+        nk = kMhd2DKernels;
     } else if (h->dim == 2) {
-        auto kern = k_step2d_hydro<S, k2dTI, k2dTJ, k2dNT>;
-        const size_t smem = sizeof(Smem2DH<k2dTI, k2dTJ>);
-        static bool attr_set = false;
-        if (!attr_set) {
-            CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            attr_set = true;
-        }
-        dim3 grid((h->n[1] + k2dTJ - 1) / k2dTJ, (h->n[0] + k2dTI - 1) / k2dTI);
-        kern<<<grid, k2dNT, smem, h->stream>>>(h->cg, h->w[c], h->w[c ^ 1], h->ctl, sa);
+        rc = (h->cfg.precision == 1)
+                 ? launch_step2d_hydro_mixed(h->solver, h->cg, h->w[c], h->w[c ^ 1], h->ctl, sa, h->stream)
+                 : launch_step2d_hydro(h->solver, h->cg, h->w[c], h->w[c ^ 1], h->ctl, sa, h->stream);
     } else {
-        int rc = launch_step3d_hydro<S>(h->cg, h->w[c], h->w[c ^ 1], h->h3_s, h->ctl, sa, h->stream);
-        if (rc) return fail(DRAGON_GPU_ECUDA, "3D step launch failed");
-        h->launches += kHydro3DKernels - 1;
+        rc = launch_step3d_hydro(h->solver, h->cg, h->w[c], h->w[c ^ 1], h->h3_s, h->ctl, sa, h->stream);
+        nk = kHydro3DKernels;
     }
-    CK(cudaGetLastError());
+    if (rc) return fail(DRAGON_GPU_ECUDA, std::string("step launch failed: ") + cudaGetErrorString(cudaGetLastError()));
     if (h->prof) {
         cudaEventRecord(e1, h->stream);
         h->ev_pending.push_back({e0, e1});
     }
-    h->launches++;
+    h->launches += nk;
     return 0;
-}
-
-int launch_step(dragon_grid* h, int c) {
-    if (h->mhd) {
-        switch (h->solver) {
-            case RS_HLL: return launch_step_t<true, RS_HLL>(h, c);
-            case RS_HLLE: return launch_step_t<true, RS_HLLE>(h, c);
-            default: return launch_step_t<true, RS_HLLD>(h, c);
-        }
-    }
-    switch (h->solver) {
-        case RS_HLLC: return launch_step_t<false, RS_HLLC>(h, c);
-        case RS_HLL: return launch_step_t<false, RS_HLL>(h, c);
-        case RS_HLLE: return launch_step_t<false, RS_HLLE>(h, c);
-        case RS_ROE: return launch_step_t<false, RS_ROE>(h, c);
-        default: return launch_step_t<false, RS_EXACT>(h, c);
-    }
 }
 
 int launch_prologue(dragon_grid* h, int c, int bookkeeping, int apply_bc, int compute_dt, int slot_in, int slot_out) {
@@ -469,6 +442,10 @@ int dragon_gpu_grid_create(int dim, int nx, int ny, int nz, double dx, double dy
     h->g = ghosts > gmin ? ghosts : gmin;
     if (h->mhd && dim == 1) h->g = ghosts > 3 ? ghosts : 3;
     h->solver = solver_id(h->cfg);
+    if (h->cfg.precision != 0 && !(dim == 2 && !h->mhd)) {
+        delete h;
+        return fail(DRAGON_GPU_EUNSUPPORTED, "the mixed-precision path is built for 2D hydro grids");
+    }
     h->cg = make_geo(dim, h->n, h->g);
     int nfc[3] = {h->n[0] + 1, h->n[1] + 1, h->n[2] + 1};
     h->fg = make_geo(dim, nfc, h->g);

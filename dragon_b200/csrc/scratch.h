@@ -1,0 +1,30 @@
+// Device intermediates of the multi-kernel steps (allocated per grid handle).
+#pragma once
+
+namespace dgpu {
+
+// 2D MHD step, all on the face geometry (n+1 per axis, same ghosts), which
+// covers every cell, face and edge index the step uses.
+struct MhdScratch {
+    double* hs;   // 4 x 8 planes: xL, xR, yL, yR half states (primitive)
+    double* fx;   // 8 planes: predictor, then final x-face fluxes
+    double* fy;   // 8 planes: predictor, then final y-face fluxes
+    double* er;   // 3 planes: body E of w
+    double* e0;   // 3 planes: predictor corner E, then final corner E
+    double* eh;   // 3 planes: body E of the half-step cells
+    long long plane;
+    static constexpr int kPlanes = 32 + 8 + 8 + 3 + 3 + 3;
+};
+constexpr int kMhd2DKernels = 7;
+
+// 3D hydro step, on the cell geometry.
+struct Hydro3DScratch {
+    double* hs;    // 6 x 5 planes: xL, xR, yL, yR, zL, zR
+    double* pf;    // 3 x 5 planes: predictor F_X, F_Y, F_Z; then final fluxes
+    double* cf;    // 6 x 5 planes: F_Xz, F_Yz, F_Xy, F_Zy, F_Yx, F_Zx
+    long long plane;
+    static constexpr int kPlanes = 30 + 15 + 30;
+};
+constexpr int kHydro3DKernels = 6;
+
+}  // namespace dgpu

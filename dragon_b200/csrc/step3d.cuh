@@ -15,16 +15,9 @@
 #include "grid.cuh"
 #include "recon.cuh"
 #include "riemann.cuh"
+#include "scratch.h"
 
 namespace dgpu {
-
-struct Hydro3DScratch {
-    double* hs;    // 6 x 5 planes: xL, xR, yL, yR, zL, zR
-    double* pf;    // 3 x 5 planes: predictor F_X, F_Y, F_Z; then final fluxes
-    double* cf;    // 6 x 5 planes: F_Xz, F_Yz, F_Xy, F_Zy, F_Yx, F_Zx
-    long long plane;
-    static constexpr int kPlanes = 30 + 15 + 30;
-};
 
 struct Step3DArgs {
     Geo G;
@@ -282,7 +275,7 @@ __global__ void k_h3_update(Step3DArgs A) {
 }
 
 template <int SOLVER>
-inline int launch_step3d_hydro(const Geo& G, const double* w, double* wout, const Hydro3DScratch& S, StepCtl* ctl,
+inline int launch_step3d_hydro_t(const Geo& G, const double* w, double* wout, const Hydro3DScratch& S, StepCtl* ctl,
                                const StepArgs& sa, cudaStream_t st) {
     Step3DArgs A{G, w, wout, S, ctl, sa};
     auto blocks = [](long long n) { return (int)((n + 255) / 256); };
@@ -298,6 +291,5 @@ inline int launch_step3d_hydro(const Geo& G, const double* w, double* wout, cons
     k_h3_update<<<blocks(cells), 256, 0, st>>>(A);
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
-constexpr int kHydro3DKernels = 6;
 
 }  // namespace dgpu

@@ -19,13 +19,14 @@
 #include "grid.cuh"
 #include "recon.cuh"
 #include "riemann.cuh"
+#include "scratch.h"
 
 namespace dgpu {
 
 // Grid2D/3D::initialize_B_fields after the boundary fill (B_fields.cpp:117-149):
 // every cell, ghosts included, takes the average of its two face values per
 // component (2D keeps the cell's z face value), pressure untouched.
-__global__ void k_init_body_fields(Geo G, Geo FG, double* __restrict__ w, const double* __restrict__ B) {
+static __global__ void k_init_body_fields(Geo G, Geo FG, double* __restrict__ w, const double* __restrict__ B) {
     const int ng = G.g;
     const long long ex = G.ext[0], ey = G.ext[1], ez = G.ext[2];
     const long long total = ex * ey * ez;
@@ -55,26 +56,13 @@ __global__ void k_init_body_fields(Geo G, Geo FG, double* __restrict__ w, const 
     }
 }
 
-inline int launch_init_body_fields(const Geo& G, const Geo& FG, double* w, const double* B, cudaStream_t s) {
+inline int launch_init_body_fields_t(const Geo& G, const Geo& FG, double* w, const double* B, cudaStream_t s) {
     const long long total = (long long)G.ext[0] * G.ext[1] * G.ext[2];
     int blocks = (int)((total + 255) / 256);
     if (blocks > 148 * 16) blocks = 148 * 16;
     k_init_body_fields<<<blocks, 256, 0, s>>>(G, FG, w, B);
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
-
-// Intermediates of the 2D MHD step, all on the face geometry (n+1 per axis,
-// same ghosts), which covers every cell, face and edge index the step uses.
-struct MhdScratch {
-    double* hs;   // 4 x 8 planes: xL, xR, yL, yR half states (primitive)
-    double* fx;   // 8 planes: predictor, then final x-face fluxes
-    double* fy;   // 8 planes: predictor, then final y-face fluxes
-    double* er;   // 3 planes: body E of w
-    double* e0;   // 3 planes: predictor corner E, then final corner E
-    double* eh;   // 3 planes: body E of the half-step cells
-    long long plane;
-    static constexpr int kPlanes = 32 + 8 + 8 + 3 + 3 + 3;
-};
 
 __device__ __forceinline__ void store_cons8(double* __restrict__ a, long long P, long long m, const Cons<double>& u) {
     a[m] = u.rho; a[P + m] = u.E; a[2 * P + m] = u.mx; a[3 * P + m] = u.my; a[4 * P + m] = u.mz;
@@ -410,7 +398,7 @@ __global__ void k_mhd2d_update(Mhd2DArgs A) {
 // the output buffers are first copied from the inputs (the reference commits
 // the interior only, Unsplit.cpp:104-107).
 template <int SOLVER>
-inline int launch_step2d_mhd(const Geo& G, const Geo& FG, const double* w, double* wout, const double* B, double* Bout,
+inline int launch_step2d_mhd_t(const Geo& G, const Geo& FG, const double* w, double* wout, const double* B, double* Bout,
                              const MhdScratch& S, StepCtl* ctl, const StepArgs& sa, cudaStream_t st) {
     Mhd2DArgs A{G, FG, w, wout, B, Bout, S, ctl, sa};
     const dim3 blk(32, 8);
@@ -427,6 +415,5 @@ inline int launch_step2d_mhd(const Geo& G, const Geo& FG, const double* w, doubl
     k_mhd2d_update<<<grid_for(nx, ny), blk, 0, st>>>(A);
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
-constexpr int kMhd2DKernels = 7;
 
 }  // namespace dgpu
