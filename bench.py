@@ -176,6 +176,59 @@ def run_reference(args):
     print(json.dumps(base))
 
 
+def learned_guess_report(train_runs=4, train_n=96, train_steps=15, n=128, p_in=1000.0, steps=10):
+    """The learned star-pressure guess on a 3D blast: a network trained on the
+    GPU from seeded blast runs (inner pressure log-uniform in [10, 1e4]), then
+    an unseen blast run with the reference's mean guess, the analytic guess
+    and the learned guess, cap lifted so every solve reaches the tolerance,
+    plus the reference's own setting (mean guess, cap 6)."""
+    import torch
+
+    import dragon_b200 as dg
+    from dragon_b200 import learned, problems
+
+    t0 = time.perf_counter()
+    net = learned.Network(seed=2024)
+    info = learned.collect_blast_samples(net, runs=train_runs, n=train_n, steps=train_steps, seed=2024, stride=8)
+    fit = learned.fit(net, steps=6000, batch=16384, lr=3e-3)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    out = {"train": {"runs": train_runs, "grid": train_n, "steps": train_steps, "samples": info["samples"],
+                     "rmse_ln_pstar": fit["rmse_log"], "gate": fit["gate"], "seconds": train_s},
+           "workload": f"3D blast {n}^3, p_in {p_in:g}, MC, exact solver, {steps} steps"}
+    ref = None
+    for name, guess, cap in (("mean_cap64", dg.GUESS_MEAN, 64), ("reference_mean_cap6", dg.GUESS_MEAN, 6),
+                             ("analytic_cap64", dg.GUESS_ANALYTIC, 64), ("learned_cap64", dg.GUESS_LEARNED, 64)):
+        w, d = problems.blast_3d(n, ghosts=2, p_in=p_in)
+        G = dg.Grid3D(n, n, n, d, d, d, ghosts=2, config=dg.Config(
+            riemann=dg.RIEMANN_EXACT, limiter=dg.LIMITER_MC, exact_max_iters=cap, exact_guess=guess))
+        G.w[...] = w
+        if guess == dg.GUESS_LEARNED:
+            G.set_network(net)
+        G.advance_steps(1)
+        G.newton_stats(reset=True)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        G.advance_steps(steps)
+        ms = (time.perf_counter() - t) / steps * 1e3
+        st = G.newton_stats()
+        e = {"newton_iters_per_solve": st["newton_iters"] / max(1, st["exact_calls"]),
+             "solves": st["exact_calls"], "two_rarefaction_faces": st["trrs"], "cap_hits": st["cap_hits"],
+             "fallback_rate": (st["guess_rejects"] + st["judge_reruns"]) / max(1, st["exact_calls"]),
+             "ms_per_step_wall": ms}
+        if ref is None:
+            ref = G.w.copy()
+        else:
+            e["rel_l1_vs_mean_cap64"] = [float(x) for x in problems.rel_l1(G.w[2:-2, 2:-2, 2:-2], ref[2:-2, 2:-2, 2:-2])]
+        out[name] = e
+        G.close()
+    m, l_ = out["mean_cap64"]["newton_iters_per_solve"], out["learned_cap64"]["newton_iters_per_solve"]
+    out["iteration_reduction_vs_mean"] = m / l_
+    out["iteration_reduction_vs_analytic"] = out["analytic_cap64"]["newton_iters_per_solve"] / l_
+    net.close()
+    return out
+
+
 def run_gpu(args):
     import torch
     import torch.distributed as dist
@@ -345,6 +398,8 @@ def run_gpu(args):
         }
         if mixed is not None:
             line["mixed"] = mixed
+        if not args.no_learned:
+            line["learned_guess"] = learned_guess_report()
         if not args.no_cpu_baseline:
             cb, why = reference_baseline(1000, 0, budget_s=args.cpu_budget)
             line["cpu_baseline"] = cb if cb else {"unavailable": why}
@@ -363,6 +418,7 @@ def main():
     ap.add_argument("--mixed", action="store_true", help="mixed FP32/FP64 path")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurement")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned star-pressure guess report")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--grid", type=int, default=1024, help="cells per axis (default: the 1024^2 workload)")
     args = ap.parse_args()

@@ -29,7 +29,8 @@ class DragonConfig(ctypes.Structure):
         ("cfl_coeff", ctypes.c_double),
         ("timestep_tol", ctypes.c_double),
         ("precision", ctypes.c_int),
-        ("reserved", ctypes.c_int * 7),
+        ("exact_guess", ctypes.c_int),
+        ("reserved", ctypes.c_int * 6),
     ]
 
 
@@ -74,7 +75,18 @@ class AdvanceStats(ctypes.Structure):
     ]
 
 
-# Every symbol include/dragon_gpu.h declares, with its ctypes signature.
+class NewtonStats(ctypes.Structure):
+    """dragon_newton_stats (include/dragon_learned.h)."""
+
+    _fields_ = [(n, ctypes.c_ulonglong) for n in (
+        "exact_calls", "newton_iters", "trrs", "cap_hits", "guess_rejects", "judge_reruns", "pivots_exact",
+        "log_seen", "log_stored")]
+
+
+c_float_p = ctypes.POINTER(ctypes.c_float)
+
+# Every symbol include/dragon_gpu.h and include/dragon_learned.h declare, with
+# its ctypes signature.
 SIGNATURES = {
     "dragon_gpu_default_config": (None, [ctypes.POINTER(DragonConfig), ctypes.c_int]),
     "dragon_gpu_grid_create": (
@@ -119,6 +131,31 @@ SIGNATURES = {
          ctypes.c_longlong, ctypes.c_longlong, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
          ctypes.c_double, ctypes.c_void_p, c_double_p]),
     "dragon_gpu_last_error": (ctypes.c_char_p, []),
+    # dragon_learned.h
+    "dragon_gpu_newton_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(NewtonStats), ctypes.c_int]),
+    "dragon_gpu_newton_log_enable": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_int]),
+    "dragon_gpu_newton_log_read": (
+        ctypes.c_int, [ctypes.c_void_p, c_double_p, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]),
+    "dragon_gpu_newton_log_device": (
+        ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_longlong)]),
+    "dragon_gpu_mlp_create": (ctypes.c_int, [ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_void_p)]),
+    "dragon_gpu_mlp_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "dragon_gpu_mlp_load": (ctypes.c_int, [ctypes.c_void_p, c_float_p, ctypes.c_int]),
+    "dragon_gpu_mlp_save": (ctypes.c_int, [ctypes.c_void_p, c_float_p, ctypes.c_int]),
+    "dragon_gpu_mlp_add_samples": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_longlong, ctypes.c_int]),
+    "dragon_gpu_mlp_sample_count": (ctypes.c_longlong, [ctypes.c_void_p]),
+    "dragon_gpu_mlp_clear_samples": (ctypes.c_int, [ctypes.c_void_p]),
+    "dragon_gpu_mlp_fit_normalisation": (ctypes.c_int, [ctypes.c_void_p]),
+    "dragon_gpu_mlp_features": (
+        ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_longlong, c_float_p, c_float_p]),
+    "dragon_gpu_mlp_gradient": (
+        ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_longlong, c_float_p, c_float_p]),
+    "dragon_gpu_mlp_train": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_float, c_float_p]),
+    "dragon_gpu_mlp_evaluate": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_longlong, c_float_p]),
+    "dragon_gpu_mlp_set_gate": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_float]),
+    "dragon_gpu_mlp_guess": (
+        ctypes.c_int, [ctypes.c_void_p, c_double_p, ctypes.c_longlong, c_double_p, c_double_p, c_float_p]),
+    "dragon_gpu_grid_set_mlp": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
 }
 
 _lib = None

@@ -32,9 +32,21 @@ def _sources():
     return [f for f in sorted(os.listdir(CSRC)) if f.endswith(".cu")]
 
 
+def _headers():
+    return [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))] + [
+        os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include")) if f.endswith(".h")] + [
+        os.path.abspath(__file__)]
+
+
 def _deps():
-    return [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh", ".h"))] + [
-        os.path.join(ROOT, "include", "dragon_gpu.h"), os.path.abspath(__file__)]
+    return [os.path.join(CSRC, f) for f in _sources()] + _headers()
+
+
+def _stale(src: str, obj: str, newest_header: float) -> bool:
+    if not os.path.exists(obj):
+        return True
+    t = os.path.getmtime(obj)
+    return os.path.getmtime(src) > t or newest_header > t
 
 
 def needs_build() -> bool:
@@ -51,8 +63,12 @@ def build(force: bool = False, verbose: bool = False) -> str:
     nvcc = os.environ.get("NVCC", "nvcc")
     os.makedirs(OBJ, exist_ok=True)
 
+    newest_header = max(os.path.getmtime(h) for h in _headers())
+
     def compile_one(src):
         obj = os.path.join(OBJ, src.replace(".cu", ".o"))
+        if not force and not _stale(os.path.join(CSRC, src), obj, newest_header):
+            return obj
         cmd = [nvcc, *BASE, *PER_FILE.get(src, EXACT), "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)

@@ -11,8 +11,11 @@
 #include <stdint.h>
 
 #include "fluid.cuh"
+#include "riemann.cuh"
 
 namespace dgpu {
+
+struct MlpNet;
 
 // Geometry of one padded array (cells or faces).
 struct Geo {
@@ -50,6 +53,7 @@ struct StepCtl {
     int pad0, pad1;
     // statistics (summed over all face solves of committed and failed steps)
     unsigned long long pivots_exact, hlld_to_hlle, newton_iters, exact_calls, trrs, muscl_first_order;
+    unsigned long long cap_hits, guess_rejects, judge_reruns;
     // interior max CFL speed (bits of a non-negative double): slots 0/1 ping-pong
     // with the state buffers, slot 2 is scratch for cfl_time. Kept last: the
     // host rewrites everything before it when a new advance starts.
@@ -188,6 +192,13 @@ struct StepArgs {
     int ct_energy;
     int slot_out;        // vmax slot the epilogue accumulates into
     int forced;          // retry: use ctl->t1 even if err was set earlier in this batch
+    int exact_guess;     // GuessMode of the exact solver
+    NewtonLog nlog;      // converged-solve sample log (rows null: off)
+    const MlpNet* mlp;   // learned guess network (GUESS_LEARNED)
 };
+
+__host__ __device__ __forceinline__ ExactOpts exact_opts(const StepArgs& sa) {
+    return ExactOpts{sa.exact_max_iters, sa.exact_tol, sa.exact_guess, sa.nlog};
+}
 
 }  // namespace dgpu

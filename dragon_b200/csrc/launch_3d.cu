@@ -11,7 +11,8 @@ int launch_step3d_hydro(int solver, const Geo& G, const double* w, double* wout,
         case RS_HLL: return launch_step3d_hydro_t<RS_HLL>(G, w, wout, S, ctl, sa, st);
         case RS_HLLE: return launch_step3d_hydro_t<RS_HLLE>(G, w, wout, S, ctl, sa, st);
         case RS_ROE: return launch_step3d_hydro_t<RS_ROE>(G, w, wout, S, ctl, sa, st);
-        default: return launch_step3d_hydro_t<RS_EXACT>(G, w, wout, S, ctl, sa, st);
+        default: return launch_step3d_hydro_t<RS_EXACT>(G, w, wout, S, ctl, sa, st,
+                                                         sa.exact_guess == GUESS_LEARNED && sa.mlp != nullptr);
     }
 }
 

@@ -6,6 +6,10 @@
 
 #include "fluid.cuh"
 
+#ifdef __CUDACC__
+#include <cooperative_groups.h>
+#endif
+
 namespace dgpu {
 
 // Solver ids match DRAGON/Config.h:39-50 (RIEMANN_*).
@@ -18,11 +22,33 @@ struct FaceStats {
     int newton_iters;  // exact solver Newton iterations
     int exact_calls;   // exact solver star-pressure solves
     int trrs;          // two-rarefaction closed forms
+    int cap_hits;      // Newton stopped by the iteration cap before the tolerance
+    int guess_rejects; // Newton solves whose learned guess was unusable: analytic guess used
+    int judge_reruns;  // learned guess hit the cap: solve rerun from the analytic guess
+};
+
+// Starting point of the star-pressure Newton iteration. GUESS_MEAN is the
+// reference's (pL + pR) / 2 (Exact.cpp:47); GUESS_ANALYTIC is the adaptive
+// PVRS / two-rarefaction / two-shock choice; GUESS_LEARNED takes the network's
+// value, with the analytic guess as fallback when that value is unusable and
+// as judge when the iteration from it hits the cap.
+enum GuessMode : int { GUESS_MEAN = 0, GUESS_ANALYTIC = 1, GUESS_LEARNED = 2 };
+
+// Converged Newton solves recorded as training samples for the learned guess:
+// kNewtonLogCols doubles per row (face-normal frame).
+constexpr int kNewtonLogCols = 8;  // rhoL, vxL, pL, rhoR, vxR, pR, p*, iterations
+struct NewtonLog {
+    double* rows;                  // null: logging off
+    unsigned long long* count;     // converged solves seen
+    long long cap;                 // rows available
+    int stride;                    // keep every stride-th solve (>= 1)
 };
 
 struct ExactOpts {
     int max_iters;     // ExactRiemann_MaxIters (Config.h:44); <= 0 means no cap
     double tol;        // ExactRiemann_Tolerance (Config.h:43)
+    int guess;         // GuessMode
+    NewtonLog log;
 };
 
 // HLL::roeAvg (HLL.cpp:21-37)
@@ -200,10 +226,30 @@ struct ExactSolution {
     Prim<R> wL, wR, sL, sR;
 };
 
+#ifdef __CUDACC__
+// Appends one converged solve to the sample log. The lanes of a warp that
+// reach this together reserve their slots with one atomic.
+__device__ __forceinline__ void newton_log_push(const NewtonLog& lg, double rl, double ul, double pl, double rr,
+                                                double ur, double pr, double ps, int n) {
+    namespace cg = cooperative_groups;
+    cg::coalesced_group grp = cg::coalesced_threads();
+    unsigned long long base = 0;
+    if (grp.thread_rank() == 0) base = atomicAdd(lg.count, (unsigned long long)grp.size());
+    base = grp.shfl(base, 0);
+    const unsigned long long idx = base + grp.thread_rank();
+    if (idx % (unsigned long long)lg.stride != 0) return;
+    const unsigned long long row = idx / (unsigned long long)lg.stride;
+    if (row >= (unsigned long long)lg.cap) return;
+    double* r = lg.rows + row * kNewtonLogCols;
+    r[0] = rl; r[1] = ul; r[2] = pl; r[3] = rr; r[4] = ur; r[5] = pr; r[6] = ps; r[7] = n;
+}
+#endif
+
 // Riemann::exact_StarP (Exact.cpp:71-84): Newton from pGuess, step clamp
 // 0.8 p, stop on relative change <= tol or after max_iters iterations.
+// *converged tells whether the tolerance (not the cap) ended the iteration.
 template <class R>
-DHD R exact_star_p(const Prim<R>& L, const Prim<R>& Rt, R pGuess, ExactOpts o, FaceStats* st) {
+DHD R exact_star_p(const Prim<R>& L, const Prim<R>& Rt, R pGuess, ExactOpts o, FaceStats* st, bool* converged) {
     R pStar = pGuess, CHA = R(1);
     int iters = o.max_iters;
     int n = 0;
@@ -215,14 +261,71 @@ DHD R exact_star_p(const Prim<R>& L, const Prim<R>& Rt, R pGuess, ExactOpts o, F
         CHA = sabs(delta / (pStar + delta / R(2)));
         n++;
     } while (CHA > R(o.tol) && --iters != 0);
-    if (st) { st->newton_iters += n; st->exact_calls += 1; }
+    const bool conv = !(CHA > R(o.tol));
+    if (st) { st->newton_iters += n; st->exact_calls += 1; st->cap_hits += !conv; }
+#ifdef __CUDA_ARCH__
+    // only well-posed solves become samples: the reference also runs the
+    // solver on unphysical corrected states of a step that is then retried
+    if (conv && o.log.rows && pStar > R(0) && sfinite(pStar) && L.rho > R(0) && L.p > R(0) && Rt.rho > R(0) &&
+        Rt.p > R(0) && sfinite(L.rho + L.p + L.vx + Rt.rho + Rt.p + Rt.vx))
+        newton_log_push(o.log, L.rho, L.vx, L.p, Rt.rho, Rt.vx, Rt.p, pStar, n);
+#endif
+    *converged = conv;
     return pStar;
 }
 
-// Riemann::exact(pGuess) including the two-rarefaction early-out (Exact.cpp:47-69)
-// and Riemann::TRRS (Exact.cpp:96-113).
+// Adaptive analytic star-pressure guess (Toro, Riemann Solvers and Numerical
+// Methods for Fluid Dynamics, 3rd ed., sec. 9.5.1, with Q = 2): the
+// primitive-variable (PVRS) estimate when the pressure ratio is small and the
+// estimate lies between the data pressures, the two-rarefaction estimate when
+// it falls below both, the two-shock estimate linearised at PVRS otherwise.
+// An unusable value (vacuum-generating data) gives the reference's mean.
 template <class R>
-DHD ExactSolution<R> exact_solve(const Prim<R>& L, const Prim<R>& Rt, R pGuess, ExactOpts o, FaceStats* st) {
+DHD R analytic_guess(const Prim<R>& L, const Prim<R>& Rt) {
+    const R aL = sound_speed(L), aR = sound_speed(Rt);
+    const R du = Rt.vx - L.vx;
+    const R mean = (L.p + Rt.p) / R(2);
+    const R ppv = smax(R(0), mean - R(0.125) * du * (L.rho + Rt.rho) * (aL + aR));
+    const R pmin = smin(L.p, Rt.p), pmax = smax(L.p, Rt.p);
+    R g;
+    if (pmax / pmin <= R(2) && pmin <= ppv && ppv <= pmax) {
+        g = ppv;
+    } else if (ppv < pmin) {
+        const R z = R(kGm1_2G);
+        g = pow((aL + aR - R(kGm1_2) * du) / (aL / pow(L.p, z) + aR / pow(Rt.p, z)), R(k2G_Gm1));
+    } else {
+        const R gL = sqrt(R(k2_Gp1) / L.rho / (ppv + R(kGm1_Gp1) * L.p));
+        const R gR = sqrt(R(k2_Gp1) / Rt.rho / (ppv + R(kGm1_Gp1) * Rt.p));
+        g = (gL * L.p + gR * Rt.p - du) / (gL + gR);
+    }
+    return (g > R(0) && sfinite(g)) ? g : mean;
+}
+
+// The network's guess for one face, evaluated by the caller (GUESS_LEARNED):
+// guess, the analytic guess, and the two-rarefaction decision when the caller
+// already made it (-1: not made).
+template <class R>
+struct LearnedGuess {
+    R guess;
+    R analytic;
+    int trrs;
+};
+
+// The two-rarefaction early-out test of Riemann::exact (Exact.cpp:52-53).
+template <class R>
+DHD bool exact_is_trrs(const Prim<R>& L, const Prim<R>& Rt) {
+    R p_min = smin(L.p, Rt.p);
+    return exact_f(p_min, L) + exact_f(p_min, Rt) + Rt.vx - L.vx >= R(0);
+}
+
+// Riemann::exact(pGuess) including the two-rarefaction early-out (Exact.cpp:47-69)
+// and Riemann::TRRS (Exact.cpp:96-113). The Newton start follows o.guess and
+// is formed only when Newton runs: the reference's mean, the analytic guess,
+// or the learned one (with the analytic guess as fallback when it is
+// unusable and as judge, rerunning the solve, when it hits the cap).
+template <class R>
+DHD ExactSolution<R> exact_solve(const Prim<R>& L, const Prim<R>& Rt, ExactOpts o, FaceStats* st,
+                                 const LearnedGuess<R>* learned = nullptr) {
     ExactSolution<R> s;
     s.wL = L;
     s.wR = Rt;
@@ -230,8 +333,8 @@ DHD ExactSolution<R> exact_solve(const Prim<R>& L, const Prim<R>& Rt, R pGuess, 
     s.sR = zero_prim<R>();
     s.sL.vx = L.vx; s.sL.vy = L.vy; s.sL.vz = L.vz;
     s.sR.vx = Rt.vx; s.sR.vy = Rt.vy; s.sR.vz = Rt.vz;
-    R p_min = smin(L.p, Rt.p);
-    if (exact_f(p_min, L) + exact_f(p_min, Rt) + Rt.vx - L.vx >= R(0)) {
+    const bool trrs = (learned && learned->trrs >= 0) ? learned->trrs != 0 : exact_is_trrs(L, Rt);
+    if (trrs) {
         if (st) st->trrs += 1;
         R aL = sound_speed(L), aR = sound_speed(Rt);
         R _LR = pow(L.p / Rt.p, R(kGm1_2G)) * aR / aL;
@@ -243,7 +346,24 @@ DHD ExactSolution<R> exact_solve(const Prim<R>& L, const Prim<R>& Rt, R pGuess, 
         s.sR.rho = Rt.rho * pow(s.sR.p / Rt.p, R(kGinv));
         return s;
     }
-    R p = exact_star_p(L, Rt, pGuess, o, st);
+    R pGuess, judge = R(0);
+    if (o.guess == GUESS_MEAN) {
+        pGuess = (L.p + Rt.p) / R(2);
+    } else if (o.guess != GUESS_LEARNED || !learned) {
+        pGuess = analytic_guess(L, Rt);
+    } else if (learned->guess > R(0) && sfinite(learned->guess)) {
+        pGuess = learned->guess;
+        judge = learned->analytic;
+    } else {
+        pGuess = learned->analytic;
+        if (st) st->guess_rejects++;
+    }
+    bool conv;
+    R p = exact_star_p(L, Rt, pGuess, o, st, &conv);
+    if (!conv && judge > R(0)) {
+        if (st) st->judge_reruns++;
+        p = exact_star_p(L, Rt, judge, o, st, &conv);
+    }
     s.sL.p = p;
     s.sR.p = p;
     // Riemann::exact_StarV (Exact.cpp:85-86)
@@ -297,16 +417,13 @@ DHD Prim<R> exact_sample(ExactSolution<R> s, R x_t) {
     return state;
 }
 
-// Riemann::exact().flux() (Exact.cpp:115-120)
+// Riemann::exact().flux() (Exact.cpp:115-120) with the configured guess.
 template <class R>
-DHD Cons<R> exact_flux(const Prim<R>& L, const Prim<R>& Rt, R pGuess, ExactOpts o, FaceStats* st) {
-    ExactSolution<R> s = exact_solve(L, Rt, pGuess, o, st);
+DHD Cons<R> exact_flux_default(const Prim<R>& L, const Prim<R>& Rt, ExactOpts o, FaceStats* st,
+                               const LearnedGuess<R>* learned = nullptr) {
+    ExactSolution<R> s = exact_solve(L, Rt, o, st, learned);
     Prim<R> w = exact_sample(s, R(0));
     return prim_flux<false>(w);
-}
-template <class R>
-DHD Cons<R> exact_flux_default(const Prim<R>& L, const Prim<R>& Rt, ExactOpts o, FaceStats* st) {
-    return exact_flux(L, Rt, (L.p + Rt.p) / R(2), o, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -489,7 +606,8 @@ DHD Cons<R> hlld(Prim<R>& L, Prim<R>& Rt, FaceStats* st) {
 // along x. dt_dx > 0 enables the hydro physicality check. Returns false when
 // the reference would throw (no physical flux found).
 template <bool MHD, int SOLVER, class R>
-DHD bool face_flux_x(Prim<R> L, Prim<R> Rt, R dt_dx, ExactOpts eo, Cons<R>& F, FaceStats* st) {
+DHD bool face_flux_x(Prim<R> L, Prim<R> Rt, R dt_dx, ExactOpts eo, Cons<R>& F, FaceStats* st,
+                     const LearnedGuess<R>* learned = nullptr) {
     if constexpr (MHD) {
         if constexpr (SOLVER == RS_HLL) F = hll<true>(L, Rt);
         else if constexpr (SOLVER == RS_HLLE) F = hlle<true>(L, Rt);
@@ -499,7 +617,7 @@ DHD bool face_flux_x(Prim<R> L, Prim<R> Rt, R dt_dx, ExactOpts eo, Cons<R>& F, F
         if constexpr (SOLVER == RS_HLL) F = hll<false>(L, Rt);
         else if constexpr (SOLVER == RS_HLLE) F = hlle<false>(L, Rt);
         else if constexpr (SOLVER == RS_ROE) F = roe(L, Rt);
-        else if constexpr (SOLVER == RS_EXACT) F = exact_flux_default(L, Rt, eo, st);
+        else if constexpr (SOLVER == RS_EXACT) F = exact_flux_default(L, Rt, eo, st, learned);
         else F = hllc(L, Rt);
         if (!(dt_dx > R(0))) return true;
         // verify_and_fallback (Flux.cpp:77-97); Riemann_ExactFallback_Parameter = 1
@@ -519,10 +637,11 @@ DHD bool face_flux_x(Prim<R> L, Prim<R> Rt, R dt_dx, ExactOpts eo, Cons<R>& F, F
 // Riemann::flux_X/Y/Z (Flux.cpp:101-115): swap the normal axis into x, solve,
 // swap the flux back. AX: 0 = x, 1 = y, 2 = z.
 template <bool MHD, int SOLVER, int AX, class R>
-DHD bool face_flux(Prim<R> L, Prim<R> Rt, R dt_dL, ExactOpts eo, Cons<R>& F, FaceStats* st) {
+DHD bool face_flux(Prim<R> L, Prim<R> Rt, R dt_dL, ExactOpts eo, Cons<R>& F, FaceStats* st,
+                   const LearnedGuess<R>* learned = nullptr) {
     swap_axis<AX>(L);
     swap_axis<AX>(Rt);
-    bool ok = face_flux_x<MHD, SOLVER>(L, Rt, dt_dL, eo, F, st);
+    bool ok = face_flux_x<MHD, SOLVER>(L, Rt, dt_dL, eo, F, st, learned);
     swap_axis<AX>(F);
     return ok;
 }

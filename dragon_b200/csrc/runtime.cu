@@ -18,8 +18,10 @@
 #include <vector>
 
 #include "../../include/dragon_gpu.h"
+#include "../../include/dragon_learned.h"
 #include "boundary.cuh"
 #include "launchers.h"
+#include "mlp.cuh"
 #include "recon.cuh"
 #include "riemann.cuh"
 #include "scratch.h"
@@ -118,6 +120,9 @@ int solver_id(const dragon_config& c) {
 // dragon_gpu_last_error().
 void dragon_gpu_set_error_message(const char* msg) { g_last_error = msg; }
 
+// Packed network of a trainer (learned.cu).
+const MlpNet* dragon_mlp_packed_net(dragon_mlp* m);
+
 struct dragon_grid {
     int dim = 0;
     int n[3] = {1, 1, 1};
@@ -153,6 +158,13 @@ struct dragon_grid {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending;
     double prof_ms = 0;
     long long prof_n = 0;
+    // exact solver: converged-solve log, learned-guess network, counters
+    double* nlog_rows = nullptr;
+    unsigned long long* nlog_count = nullptr;
+    long long nlog_cap = 0;
+    int nlog_stride = 1;
+    MlpNet* mlp_dev = nullptr;
+    dragon_newton_stats ntot{};
 };
 
 namespace {
@@ -171,6 +183,9 @@ StepArgs step_args(const dragon_grid* h, int slot_out) {
     a.ct_energy = h->cfg.ct_energy;
     a.slot_out = slot_out;
     a.forced = 0;
+    a.exact_guess = h->cfg.exact_guess;
+    a.nlog = NewtonLog{h->nlog_rows, h->nlog_count, h->nlog_cap, h->nlog_stride};
+    a.mlp = h->mlp_dev;
     return a;
 }
 
@@ -201,6 +216,8 @@ void collect_profile(dragon_grid* h) {
 
 int launch_step(dragon_grid* h, int c) {
     const StepArgs sa = step_args(h, c ^ 1);
+    if (sa.exact_guess == GUESS_LEARNED && h->solver == RS_EXACT && !sa.mlp)
+        return fail(DRAGON_GPU_EINVAL, "exact_guess = learned needs a network (dragon_gpu_grid_set_mlp)");
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (h->prof) {
         e0 = take_event(h);
@@ -298,7 +315,19 @@ void fill_failure(const StepCtl& c, dragon_step_status* st, int code) {
     st->dt = c.t1;
 }
 
-void fill_stats(const StepCtl& c, dragon_advance_stats* st) {
+// Adds a control block's exact-solver counters to the grid's running totals.
+void add_newton(dragon_grid* h, const StepCtl& c) {
+    h->ntot.exact_calls += c.exact_calls;
+    h->ntot.newton_iters += c.newton_iters;
+    h->ntot.trrs += c.trrs;
+    h->ntot.cap_hits += c.cap_hits;
+    h->ntot.guess_rejects += c.guess_rejects;
+    h->ntot.judge_reruns += c.judge_reruns;
+    h->ntot.pivots_exact += c.pivots_exact;
+}
+
+void fill_stats(dragon_grid* h, const StepCtl& c, dragon_advance_stats* st) {
+    add_newton(h, c);
     if (!st) return;
     st->pivots_exact += c.pivots_exact;
     st->hlld_to_hlle += c.hlld_to_hlle;
@@ -352,7 +381,7 @@ int advance_impl(dragon_grid* h, double remaining, int max_steps, int check_cfl,
             h->cur = c;
             h->imax_valid = true;
             const int stage = (int)(C.err_key >> 56);
-            fill_stats(C, st);
+            fill_stats(h, C, st);
             if (st) { st->steps = (int)ks; fill_failure(C, &st->failure, DRAGON_GPU_ESTEP); }
             if (stage == ST_CFL_ZERO) {
                 if (st) st->failure.code = DRAGON_GPU_ECFL;
@@ -371,12 +400,13 @@ int advance_impl(dragon_grid* h, double remaining, int max_steps, int check_cfl,
                 C.err = 0;
                 C.err_key = ~0ull;
                 C.pivots_exact = C.hlld_to_hlle = C.newton_iters = C.exact_calls = C.trrs = C.muscl_first_order = 0;
+                C.cap_hits = C.guess_rejects = C.judge_reruns = 0;
                 if ((rc = push_ctl(h))) return rc;
                 if ((rc = zero_slot(h, c ^ 1))) return rc;
                 if ((rc = launch_step(h, c))) return rc;
                 if ((rc = pull_ctl(h))) return rc;
                 if (!C.err) break;
-                fill_stats(C, st);
+                fill_stats(h, C, st);
             }
             // success: the next prologue accounts the retried step
             k = ks + 1;
@@ -386,7 +416,7 @@ int advance_impl(dragon_grid* h, double remaining, int max_steps, int check_cfl,
         if (C.done) {
             h->cur = cur0 ^ (int)(C.steps_done & 1);
             h->imax_valid = true;
-            fill_stats(C, st);
+            fill_stats(h, C, st);
             if (st) {
                 st->steps = C.steps_done;
                 st->retries = retries;
@@ -442,6 +472,14 @@ int dragon_gpu_grid_create(int dim, int nx, int ny, int nz, double dx, double dy
     h->g = ghosts > gmin ? ghosts : gmin;
     if (h->mhd && dim == 1) h->g = ghosts > 3 ? ghosts : 3;
     h->solver = solver_id(h->cfg);
+    if (h->cfg.exact_guess < GUESS_MEAN || h->cfg.exact_guess > GUESS_LEARNED) {
+        delete h;
+        return fail(DRAGON_GPU_EINVAL, "exact_guess must be 0 (mean), 1 (analytic) or 2 (learned)");
+    }
+    if (h->cfg.exact_guess == GUESS_LEARNED && !(dim == 3 && !h->mhd)) {
+        delete h;
+        return fail(DRAGON_GPU_EUNSUPPORTED, "the learned star-pressure guess is built for 3D hydro grids");
+    }
     if (h->cfg.precision != 0 && !(dim == 2 && !h->mhd)) {
         delete h;
         return fail(DRAGON_GPU_EUNSUPPORTED, "the mixed-precision path is built for 2D hydro grids");
@@ -516,6 +554,9 @@ int dragon_gpu_grid_destroy(dragon_grid* h) {
     if (h->hctl) cudaFreeHost(h->hctl);
     if (h->dbcs) cudaFree(h->dbcs);
     if (h->stage) cudaFree(h->stage);
+    if (h->nlog_rows) cudaFree(h->nlog_rows);
+    if (h->nlog_count) cudaFree(h->nlog_count);
+    if (h->mlp_dev) cudaFree(h->mlp_dev);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return 0;
@@ -642,6 +683,7 @@ int dragon_gpu_unsplit_step(dragon_grid* h, double dt, dragon_step_status* st) {
     if ((rc = zero_slot(h, c ^ 1))) return rc;
     if ((rc = launch_step(h, c))) return rc;
     if ((rc = pull_ctl(h))) return rc;
+    add_newton(h, *h->hctl);
     if (h->hctl->err) {
         fill_failure(*h->hctl, st, DRAGON_GPU_ESTEP);
         return fail(DRAGON_GPU_ESTEP, stage_name((int)(h->hctl->err_key >> 56)));
@@ -700,6 +742,89 @@ int dragon_gpu_initialize_B_fields(dragon_grid* h) {
     if (rc) return fail(DRAGON_GPU_ECUDA, "initialize_B_fields launch failed");
     h->launches++;
     h->imax_valid = false;
+    CK(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int dragon_gpu_newton_stats(dragon_grid* h, dragon_newton_stats* out, int reset) {
+    if (!h) return fail(DRAGON_GPU_EINVAL, "null handle");
+    if (out) {
+        *out = h->ntot;
+        if (h->nlog_count) {
+            unsigned long long seen = 0;
+            CK(cudaMemcpyAsync(&seen, h->nlog_count, sizeof(seen), cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            out->log_seen = seen;
+            const unsigned long long kept = (seen + h->nlog_stride - 1) / h->nlog_stride;
+            out->log_stored = kept < (unsigned long long)h->nlog_cap ? kept : (unsigned long long)h->nlog_cap;
+        }
+    }
+    if (reset) h->ntot = dragon_newton_stats{};
+    return 0;
+}
+
+int dragon_gpu_newton_log_enable(dragon_grid* h, long long capacity, int stride) {
+    if (!h || capacity < 0 || stride < 1) return fail(DRAGON_GPU_EINVAL, "invalid log arguments");
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->nlog_rows) cudaFree(h->nlog_rows);
+    if (h->nlog_count) cudaFree(h->nlog_count);
+    h->nlog_rows = nullptr;
+    h->nlog_count = nullptr;
+    h->nlog_cap = 0;
+    h->nlog_stride = 1;
+    if (capacity == 0) return 0;
+    CK(cudaMalloc(&h->nlog_rows, sizeof(double) * kNewtonLogCols * capacity));
+    CK(cudaMalloc(&h->nlog_count, sizeof(unsigned long long)));
+    CK(cudaMemsetAsync(h->nlog_count, 0, sizeof(unsigned long long), h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->nlog_cap = capacity;
+    h->nlog_stride = stride;
+    return 0;
+}
+
+static long long nlog_stored(dragon_grid* h, int* rc) {
+    *rc = 0;
+    if (!h->nlog_count) return 0;
+    unsigned long long seen = 0;
+    if (cudaMemcpyAsync(&seen, h->nlog_count, sizeof(seen), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+        cudaStreamSynchronize(h->stream) != cudaSuccess) {
+        *rc = fail(DRAGON_GPU_ECUDA, "reading the log counter failed");
+        return 0;
+    }
+    const unsigned long long kept = (seen + h->nlog_stride - 1) / h->nlog_stride;
+    return kept < (unsigned long long)h->nlog_cap ? (long long)kept : h->nlog_cap;
+}
+
+int dragon_gpu_newton_log_read(dragon_grid* h, double* host_rows, long long max_rows, long long* n_out) {
+    if (!h || max_rows < 0 || (max_rows > 0 && !host_rows)) return fail(DRAGON_GPU_EINVAL, "invalid arguments");
+    int rc;
+    long long n = nlog_stored(h, &rc);
+    if (rc) return rc;
+    if (n > max_rows) n = max_rows;
+    if (n > 0) {
+        CK(cudaMemcpyAsync(host_rows, h->nlog_rows, sizeof(double) * kNewtonLogCols * n, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    if (n_out) *n_out = n;
+    return 0;
+}
+
+int dragon_gpu_newton_log_device(dragon_grid* h, const double** rows, long long* n_stored) {
+    if (!h) return fail(DRAGON_GPU_EINVAL, "null handle");
+    int rc;
+    const long long n = nlog_stored(h, &rc);
+    if (rc) return rc;
+    if (rows) *rows = h->nlog_rows;
+    if (n_stored) *n_stored = n;
+    return 0;
+}
+
+int dragon_gpu_grid_set_mlp(dragon_grid* h, const dragon_mlp* m) {
+    if (!h || !m) return fail(DRAGON_GPU_EINVAL, "null argument");
+    const MlpNet* net = dragon_mlp_packed_net(const_cast<dragon_mlp*>(m));
+    if (!net) return fail(DRAGON_GPU_ECUDA, "packing the network failed");
+    if (!h->mlp_dev) CK(cudaMalloc(&h->mlp_dev, sizeof(MlpNet)));
+    CK(cudaMemcpyAsync(h->mlp_dev, net, sizeof(MlpNet), cudaMemcpyDeviceToDevice, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     return 0;
 }

@@ -13,6 +13,7 @@
 #pragma once
 
 #include "grid.cuh"
+#include "mlp.cuh"
 #include "recon.cuh"
 #include "riemann.cuh"
 #include "scratch.h"
@@ -93,7 +94,7 @@ __device__ __forceinline__ void h3_flux(const Step3DArgs& A, double* out, int i,
     Prim<double> L = ld5(A.S.hs + (10 * AX + 5) * SP, SP, gidx3(G, i - di, j - dj, k - dk));
     Prim<double> R = ld5(A.S.hs + (10 * AX) * SP, SP, m);
     Cons<double> F;
-    const ExactOpts eo{A.sa.exact_max_iters, A.sa.exact_tol};
+    const ExactOpts eo = exact_opts(A.sa);
     if (!face_flux<false, SOLVER, AX>(L, R, dtn, eo, F, st)) record_error(A.ctl, stage, m);
     stc5(out, SP, m, F);
 }
@@ -103,6 +104,136 @@ __device__ __forceinline__ void h3_stats(StepCtl* ctl, const FaceStats& st) {
     warp_add_stat(&ctl->newton_iters, st.newton_iters);
     warp_add_stat(&ctl->exact_calls, st.exact_calls);
     warp_add_stat(&ctl->trrs, st.trrs);
+    warp_add_stat(&ctl->cap_hits, st.cap_hits);
+    warp_add_stat(&ctl->guess_rejects, st.guess_rejects);
+    warp_add_stat(&ctl->judge_reruns, st.judge_reruns);
+}
+
+// ---------------------------------------------------------------------------
+// Learned-guess variants of the three flux kernels (exact solver only). The
+// network runs as a warp collective on the tensor cores, so these kernels
+// keep every lane of a warp converged up to the inference: lanes without a
+// face carry a neutral state instead of returning early, and the solve that
+// follows is predicated on the face being real.
+
+__device__ __forceinline__ Prim<double> neutral_state() {
+    Prim<double> w = zero_prim<double>();
+    w.rho = 1.0;
+    w.p = 1.0;
+    return w;
+}
+
+template <int AX>
+__device__ __forceinline__ LearnedGuess<double> learned_guess_face(const Step3DArgs& A, const Prim<double>& L,
+                                                                   const Prim<double>& R, bool valid) {
+    Prim<double> Ln = L, Rn = R;
+    swap_axis<AX>(Ln);
+    swap_axis<AX>(Rn);
+    return mlp_guess_warp(A.sa.mlp, Ln, Rn, valid);
+}
+
+template <int AX>
+__device__ __forceinline__ void h3_flux_learned(const Step3DArgs& A, double* out, bool valid, int i, int j, int k,
+                                                double dtn, int stage, FaceStats* st) {
+    const Geo& G = A.G;
+    const long long SP = A.S.plane;
+    const int di = AX == 0, dj = AX == 1, dk = AX == 2;
+    Prim<double> L = neutral_state(), R = neutral_state();
+    long long m = 0;
+    if (valid) {
+        m = gidx3(G, i, j, k);
+        L = ld5(A.S.hs + (10 * AX + 5) * SP, SP, gidx3(G, i - di, j - dj, k - dk));
+        R = ld5(A.S.hs + (10 * AX) * SP, SP, m);
+    }
+    const LearnedGuess<double> g = learned_guess_face<AX>(A, L, R, valid);
+    if (!valid) return;
+    Cons<double> F;
+    if (!face_flux<false, RS_EXACT, AX>(L, R, dtn, exact_opts(A.sa), F, st, &g)) record_error(A.ctl, stage, m);
+    stc5(out, SP, m, F);
+}
+
+template <int AX, int TD>
+__device__ __forceinline__ void h3_ctu_flux_learned(const Step3DArgs& A, const double* T, double* out, bool valid,
+                                                    int i, int j, int k, double dtn, double dtT, FaceStats* st) {
+    const Geo& G = A.G;
+    const long long SP = A.S.plane;
+    const int di = AX == 0, dj = AX == 1, dk = AX == 2;
+    const int ti = TD == 0, tj = TD == 1, tk = TD == 2;
+    Prim<double> L = neutral_state(), R = neutral_state();
+    long long m = 0;
+    if (valid) {
+        auto trans = [&](int a, int b, int c) {
+            const Cons<double> t1 = ldc5(T, SP, gidx3(G, a + ti, b + tj, c + tk)), t0 = ldc5(T, SP, gidx3(G, a, b, c));
+            return c_mul<false>(c_sub<false>(t1, t0), dtT);
+        };
+        m = gidx3(G, i, j, k);
+        L = to_prim<false>(c_sub<false>(to_cons<false>(ld5(A.S.hs + (10 * AX + 5) * SP, SP, gidx3(G, i - di, j - dj, k - dk))),
+                                        trans(i - di, j - dj, k - dk)));
+        R = to_prim<false>(c_sub<false>(to_cons<false>(ld5(A.S.hs + (10 * AX) * SP, SP, m)), trans(i, j, k)));
+    }
+    const LearnedGuess<double> g = learned_guess_face<AX>(A, L, R, valid);
+    if (!valid) return;
+    Cons<double> F;
+    if (!face_flux<false, RS_EXACT, AX>(L, R, dtn, exact_opts(A.sa), F, st, &g))
+        record_error(A.ctl, ST_PRELIM_FLUX, m);
+    stc5(out, SP, m, F);
+}
+
+__global__ void k_h3_prelim_learned(Step3DArgs A) {
+    __shared__ int s;
+    if (h3_skip(A.ctl, &s)) return;
+    const Geo& G = A.G;
+    const int lo[3] = {-1, -1, -1}, ext[3] = {G.n[0] + 2, G.n[1] + 2, G.n[2] + 2};
+    int i = 0, j = 0, k = 0;
+    const bool in = box_cell(blockIdx.x * (long long)blockDim.x + threadIdx.x, lo, ext, i, j, k);
+    const double dt = *(const volatile double*)&A.ctl->t1;
+    FaceStats st{};
+    const long long SP = A.S.plane;
+    h3_flux_learned<0>(A, A.S.pf, in && i >= 0, i, j, k, dt / A.sa.dx, ST_PRELIM_FLUX, &st);
+    h3_flux_learned<1>(A, A.S.pf + 5 * SP, in && j >= 0, i, j, k, dt / A.sa.dy, ST_PRELIM_FLUX, &st);
+    h3_flux_learned<2>(A, A.S.pf + 10 * SP, in && k >= 0, i, j, k, dt / A.sa.dz, ST_PRELIM_FLUX, &st);
+    h3_stats(A.ctl, st);
+}
+
+__global__ void k_h3_ctu_learned(Step3DArgs A) {
+    __shared__ int s;
+    if (h3_skip(A.ctl, &s)) return;
+    const Geo& G = A.G;
+    const int lo[3] = {-1, -1, -1}, ext[3] = {G.n[0] + 2, G.n[1] + 2, G.n[2] + 2};
+    int i = 0, j = 0, k = 0;
+    const bool in = box_cell(blockIdx.x * (long long)blockDim.x + threadIdx.x, lo, ext, i, j, k);
+    const int nx = G.n[0], ny = G.n[1], nz = G.n[2];
+    const double dt = *(const volatile double*)&A.ctl->t1;
+    const double dt_dx = dt / A.sa.dx, dt_dy = dt / A.sa.dy, dt_dz = dt / A.sa.dz;
+    const long long SP = A.S.plane;
+    const double* FX = A.S.pf;
+    const double* FY = A.S.pf + 5 * SP;
+    const double* FZ = A.S.pf + 10 * SP;
+    FaceStats st{};
+    h3_ctu_flux_learned<0, 2>(A, FZ, A.S.cf, in && i >= 0 && k >= 0 && k < nz, i, j, k, dt_dx, dt_dz / 3.0, &st);
+    h3_ctu_flux_learned<1, 2>(A, FZ, A.S.cf + 5 * SP, in && j >= 0 && k >= 0 && k < nz, i, j, k, dt_dy, dt_dz / 3.0, &st);
+    h3_ctu_flux_learned<0, 1>(A, FY, A.S.cf + 10 * SP, in && i >= 0 && j >= 0 && j < ny, i, j, k, dt_dx, dt_dy / 3.0, &st);
+    h3_ctu_flux_learned<2, 1>(A, FY, A.S.cf + 15 * SP, in && j >= 0 && j < ny && k >= 0, i, j, k, dt_dz, dt_dy / 3.0, &st);
+    h3_ctu_flux_learned<1, 0>(A, FX, A.S.cf + 20 * SP, in && i >= 0 && i < nx && j >= 0, i, j, k, dt_dy, dt_dx / 3.0, &st);
+    h3_ctu_flux_learned<2, 0>(A, FX, A.S.cf + 25 * SP, in && i >= 0 && i < nx && k >= 0, i, j, k, dt_dz, dt_dx / 3.0, &st);
+    h3_stats(A.ctl, st);
+}
+
+__global__ void k_h3_final_learned(Step3DArgs A) {
+    __shared__ int s;
+    if (h3_skip(A.ctl, &s)) return;
+    const Geo& G = A.G;
+    const int lo[3] = {0, 0, 0}, ext[3] = {G.n[0] + 1, G.n[1] + 1, G.n[2] + 1};
+    int i = 0, j = 0, k = 0;
+    const bool in = box_cell(blockIdx.x * (long long)blockDim.x + threadIdx.x, lo, ext, i, j, k);
+    const int nx = G.n[0], ny = G.n[1], nz = G.n[2];
+    const double dt = *(const volatile double*)&A.ctl->t1;
+    FaceStats st{};
+    const long long SP = A.S.plane;
+    h3_flux_learned<0>(A, A.S.pf, in && j < ny && k < nz, i, j, k, dt / A.sa.dx, ST_FINAL_FLUX, &st);
+    h3_flux_learned<1>(A, A.S.pf + 5 * SP, in && i < nx && k < nz, i, j, k, dt / A.sa.dy, ST_FINAL_FLUX, &st);
+    h3_flux_learned<2>(A, A.S.pf + 10 * SP, in && i < nx && j < ny, i, j, k, dt / A.sa.dz, ST_FINAL_FLUX, &st);
+    h3_stats(A.ctl, st);
 }
 
 // K2: predictor fluxes F_X on [0,nx]x[-1,ny]x[-1,nz], F_Y on [-1,nx]x[0,ny]x[-1,nz],
@@ -143,7 +274,7 @@ __device__ __forceinline__ void h3_ctu_flux(const Step3DArgs& A, const double* T
     const long long m = gidx3(G, i, j, k);
     const Prim<double> R = to_prim<false>(c_sub<false>(to_cons<false>(ld5(A.S.hs + (10 * AX) * SP, SP, m)), trans(i, j, k)));
     Cons<double> F;
-    const ExactOpts eo{A.sa.exact_max_iters, A.sa.exact_tol};
+    const ExactOpts eo = exact_opts(A.sa);
     if (!face_flux<false, SOLVER, AX>(L, R, dtn, eo, F, st)) record_error(A.ctl, ST_PRELIM_FLUX, m);
     stc5(out, SP, m, F);
 }
@@ -274,9 +405,10 @@ __global__ void k_h3_update(Step3DArgs A) {
     if (threadIdx.x == 0) atomic_max_speed(&A.ctl->vmax[A.sa.slot_out], vmax);
 }
 
+// learned: the exact solver takes its Newton start from the network (sa.mlp).
 template <int SOLVER>
 inline int launch_step3d_hydro_t(const Geo& G, const double* w, double* wout, const Hydro3DScratch& S, StepCtl* ctl,
-                               const StepArgs& sa, cudaStream_t st) {
+                               const StepArgs& sa, cudaStream_t st, bool learned = false) {
     Step3DArgs A{G, w, wout, S, ctl, sa};
     auto blocks = [](long long n) { return (int)((n + 255) / 256); };
     const long long box = (long long)(G.n[0] + 2) * (G.n[1] + 2) * (G.n[2] + 2);
@@ -284,6 +416,16 @@ inline int launch_step3d_hydro_t(const Geo& G, const double* w, double* wout, co
     const long long cells = (long long)G.n[0] * G.n[1] * G.n[2];
     if (cudaMemcpyAsync(wout, w, sizeof(double) * 5 * G.plane, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return 1;
     k_h3_halfstates<<<blocks(box), 256, 0, st>>>(A);
+    if constexpr (SOLVER == RS_EXACT) {
+        if (learned) {
+            k_h3_prelim_learned<<<blocks(box), 256, 0, st>>>(A);
+            k_h3_ctu_learned<<<blocks(box), 256, 0, st>>>(A);
+            k_h3_correct<<<blocks(box), 256, 0, st>>>(A);
+            k_h3_final_learned<<<blocks(fbox), 256, 0, st>>>(A);
+            k_h3_update<<<blocks(cells), 256, 0, st>>>(A);
+            return cudaGetLastError() == cudaSuccess ? 0 : 1;
+        }
+    }
     k_h3_prelim<SOLVER><<<blocks(box), 256, 0, st>>>(A);
     k_h3_ctu<SOLVER><<<blocks(box), 256, 0, st>>>(A);
     k_h3_correct<<<blocks(box), 256, 0, st>>>(A);

@@ -27,7 +27,7 @@ struct Smem2DH {
         } f;
     } u;
     double red[32];
-    unsigned long long stat[6];
+    unsigned long long stat[7];
 };
 
 enum { HS_XL = 0, HS_XR = 1, HS_YL = 2, HS_YR = 3 };
@@ -99,10 +99,10 @@ k_step2d_hydro(Geo G, const double* __restrict__ win, double* __restrict__ wout,
     const double dt = *(volatile double*)&ctl->t1;
     const double dt_dx = dt / sa.dx, dt_dy = dt / sa.dy;
     const double hdx = 0.5 * dt_dx, hdy = 0.5 * dt_dy;
-    const ExactOpts eo{sa.exact_max_iters, sa.exact_tol};
+    const ExactOpts eo = exact_opts(sa);
     FaceStats st{0, 0, 0, 0, 0};
     int first_order = 0;
-    if (threadIdx.x < 6) S.stat[threadIdx.x] = 0;
+    if (threadIdx.x < 7) S.stat[threadIdx.x] = 0;
 
     // P0: tile + two-cell halo of the primitive state
     constexpr int WI = TI + 4, WJ = TJ + 4;
@@ -267,6 +267,7 @@ k_step2d_hydro(Geo G, const double* __restrict__ win, double* __restrict__ wout,
     if (st.exact_calls) atomicAdd(&S.stat[3], (unsigned long long)st.exact_calls);
     if (st.trrs) atomicAdd(&S.stat[4], (unsigned long long)st.trrs);
     if (first_order) atomicAdd(&S.stat[5], (unsigned long long)first_order);
+    if (st.cap_hits) atomicAdd(&S.stat[6], (unsigned long long)st.cap_hits);
     __syncthreads();
     if (threadIdx.x == 0) {
         if (S.stat[0]) atomicAdd(&ctl->pivots_exact, S.stat[0]);
@@ -274,6 +275,7 @@ k_step2d_hydro(Geo G, const double* __restrict__ win, double* __restrict__ wout,
         if (S.stat[3]) atomicAdd(&ctl->exact_calls, S.stat[3]);
         if (S.stat[4]) atomicAdd(&ctl->trrs, S.stat[4]);
         if (S.stat[5]) atomicAdd(&ctl->muscl_first_order, S.stat[5]);
+        if (S.stat[6]) atomicAdd(&ctl->cap_hits, S.stat[6]);
     }
 }
 
@@ -299,7 +301,7 @@ k_step1d(Geo G, const double* __restrict__ win, double* __restrict__ wout, StepC
     const long long PL = G.plane;
     const double dt = *(volatile double*)&ctl->t1;
     const double dt_dx = dt / sa.dx;
-    const ExactOpts eo{sa.exact_max_iters, sa.exact_tol};
+    const ExactOpts eo = exact_opts(sa);
     FaceStats st{0, 0, 0, 0, 0};
     int first_order = 0;
 
@@ -387,6 +389,7 @@ k_step1d(Geo G, const double* __restrict__ win, double* __restrict__ wout, StepC
     if (st.newton_iters) atomicAdd(&ctl->newton_iters, (unsigned long long)st.newton_iters);
     if (st.exact_calls) atomicAdd(&ctl->exact_calls, (unsigned long long)st.exact_calls);
     if (st.trrs) atomicAdd(&ctl->trrs, (unsigned long long)st.trrs);
+    if (st.cap_hits) atomicAdd(&ctl->cap_hits, (unsigned long long)st.cap_hits);
     if (first_order) atomicAdd(&ctl->muscl_first_order, (unsigned long long)first_order);
 }
 

@@ -184,7 +184,7 @@ __global__ void k_mhd2d_prelim(Mhd2DArgs A) {
     const double dt = mhd_dt(A.ctl), dt_dx = dt / A.sa.dx, dt_dy = dt / A.sa.dy;
     const Geo& F = A.FG;
     const long long SP = A.S.plane;
-    const ExactOpts eo{A.sa.exact_max_iters, A.sa.exact_tol};
+    const ExactOpts eo = exact_opts(A.sa);
     FaceStats st{0, 0, 0, 0, 0};
     const int nx = A.G.n[0], ny = A.G.n[1];
     Cons<double> Fl;
@@ -315,7 +315,7 @@ __global__ void k_mhd2d_final_flux(Mhd2DArgs A) {
     const double dt = mhd_dt(A.ctl), dt_dx = dt / A.sa.dx, dt_dy = dt / A.sa.dy;
     const Geo& F = A.FG;
     const long long SP = A.S.plane;
-    const ExactOpts eo{A.sa.exact_max_iters, A.sa.exact_tol};
+    const ExactOpts eo = exact_opts(A.sa);
     FaceStats st{0, 0, 0, 0, 0};
     Cons<double> Fl;
     if (i >= 0) {

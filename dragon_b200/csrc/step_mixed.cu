@@ -60,7 +60,7 @@ k_step2d_hydro_mixed(Geo G, const double* __restrict__ win, double* __restrict__
     const double dt = *(volatile double*)&ctl->t1;
     const double dt_dx = dt / sa.dx, dt_dy = dt / sa.dy;
     const float fdx = (float)dt_dx, fdy = (float)dt_dy, hdx = (float)(0.5 * dt_dx), hdy = (float)(0.5 * dt_dy);
-    const ExactOpts eo{sa.exact_max_iters, sa.exact_tol};
+    const ExactOpts eo = exact_opts(sa);
     FaceStats st{0, 0, 0, 0, 0};
     int first_order = 0;
     if (threadIdx.x < 6) S.stat[threadIdx.x] = 0;

@@ -28,6 +28,7 @@ LIMITER_MINMOD, LIMITER_MC, LIMITER_VANLEER, LIMITER_SUPERBEE, LIMITER_VANALBADA
 CFL_MAX, CFL_ADD = 0, 1
 CT_CONSV_TOTAL_E, CT_CONSV_THERMAL, CT_CONSV_BETA_GATED = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
+GUESS_MEAN, GUESS_ANALYTIC, GUESS_LEARNED = 0, 1, 2
 
 
 @dataclass
@@ -44,6 +45,7 @@ class Config:
     cfl_coeff: float = 0.3
     timestep_tol: float = 1e-14
     precision: int = PREC_FP64
+    exact_guess: int = GUESS_MEAN
 
     def to_c(self) -> _lib.DragonConfig:
         c = _lib.DragonConfig()
@@ -57,6 +59,7 @@ class Config:
         c.cfl_coeff = self.cfl_coeff
         c.timestep_tol = self.timestep_tol
         c.precision = self.precision
+        c.exact_guess = self.exact_guess
         return c
 
 
@@ -279,6 +282,33 @@ class _GridBase:
 
     def launch_count(self) -> int:
         return int(self._lib.dragon_gpu_launch_count(self._h))
+
+    # -- exact solver: Newton statistics, sample log, learned guess ----------
+    def newton_stats(self, reset: bool = False) -> dict:
+        """Exact-solver counters summed over every step since creation / reset."""
+        st = _lib.NewtonStats()
+        _lib.check(self._lib.dragon_gpu_newton_stats(self._h, ctypes.byref(st), int(bool(reset))))
+        return {name: int(getattr(st, name)) for name, _ in st._fields_}
+
+    def newton_log(self, capacity: int, stride: int = 1):
+        """Starts logging converged Newton solves (every stride-th, up to capacity rows); 0 stops."""
+        _lib.check(self._lib.dragon_gpu_newton_log_enable(self._h, int(capacity), int(stride)))
+
+    def newton_log_rows(self, max_rows: int | None = None) -> np.ndarray:
+        """Stored log rows: rhoL, vxL, pL, rhoR, vxR, pR, p*, iterations (face-normal frame)."""
+        rows_p = ctypes.c_void_p()
+        n = ctypes.c_longlong()
+        _lib.check(self._lib.dragon_gpu_newton_log_device(self._h, ctypes.byref(rows_p), ctypes.byref(n)))
+        m = n.value if max_rows is None else min(n.value, int(max_rows))
+        out = np.zeros((m, 8))
+        got = ctypes.c_longlong()
+        if m:
+            _lib.check(self._lib.dragon_gpu_newton_log_read(self._h, self._ptr(out), m, ctypes.byref(got)))
+        return out[:got.value] if m else out
+
+    def set_network(self, net) -> None:
+        """Copies a learned-guess network (dragon_b200.learned.Network) into the grid."""
+        _lib.check(self._lib.dragon_gpu_grid_set_mlp(self._h, net._h))
 
     def getGhosts(self) -> int:
         return self.ghosts

@@ -53,7 +53,10 @@ typedef struct dragon_config {
     double cfl_coeff;     /* CFL_coeff (0.3) */
     double timestep_tol;  /* Timestep_Tolerance (1e-14) */
     int precision;        /* 0: FP64 throughout (bit-faithful), 1: mixed FP32/FP64 */
-    int reserved[7];
+    int exact_guess;      /* start of the exact solver's Newton iteration: 0 the reference's
+                             (pL + pR) / 2 (Exact.cpp:47), 1 adaptive PVRS / two-rarefaction /
+                             two-shock, 2 learned (dragon_learned.h; 3D grids) */
+    int reserved[6];
 } dragon_config;
 
 /* Fills the reference's shipped defaults for the given physics mode. */

@@ -466,6 +466,11 @@ static double ex_rho(prim_t w, double p) {
 }
 typedef struct { prim_t wL, wR, sL, sR; } sol_t;
 static int g_newton_iters;
+/* Optional record of every Newton-branch solve: (rhoL, vxL, pL, rhoR, vxR, pR,
+ * p*, iterations; negative when the cap, not the tolerance, ended it) per row. Test infrastructure for the learned-guess sample
+ * log; off unless ora_exact_log_start was called. */
+static double* g_log_buf;
+static long g_log_cap, g_log_n;
 
 static sol_t exact_solve(prim_t L, prim_t R, double pGuess) {
     sol_t s;
@@ -496,6 +501,15 @@ static sol_t exact_solve(prim_t L, prim_t R, double pGuess) {
         CHA = fabs(delta / (p + delta / 2));
         g_newton_iters++;
     } while (CHA > O.exact_tol && --iters != 0);
+    if (g_log_buf) {
+        if (g_log_n < g_log_cap) {
+            double* row = g_log_buf + 8 * g_log_n;
+            row[0] = L.rho; row[1] = L.v.x; row[2] = L.p;
+            row[3] = R.rho; row[4] = R.v.x; row[5] = R.p;
+            row[6] = p; row[7] = (CHA > O.exact_tol) ? -g_newton_iters : g_newton_iters;
+        }
+        g_log_n++;
+    }
     s.sL.p = p;
     s.sR.p = p;
     s.sL.v.x = (L.v.x + R.v.x + ex_f(p, R) - ex_f(p, L)) / 2.0;
@@ -1810,6 +1824,23 @@ int ora_riemann_flux(int solver, const double* l, const double* r, double dt_dx,
     O.riemann = keep;
     put_cons(F, out);
     return g_fail;
+}
+void ora_exact_log_start(double* buf, long cap) {
+#if !MHD
+    g_log_buf = buf;
+    g_log_cap = cap;
+    g_log_n = 0;
+#else
+    (void)buf; (void)cap;
+#endif
+}
+long ora_exact_log_stop(void) {
+#if !MHD
+    g_log_buf = 0;
+    return g_log_n;
+#else
+    return 0;
+#endif
 }
 void ora_exact_star(const double* l, const double* r, double pGuess, double* sl, double* sr, int* iters) {
 #if !MHD

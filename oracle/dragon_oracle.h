@@ -54,6 +54,12 @@ void ora_muscl(const double* wl, const double* wc, const double* wr, double dt_d
                double* R);
 int ora_riemann_flux(int solver, const double* l, const double* r, double dt_dx, int axis, double* out);
 void ora_exact_star(const double* l, const double* r, double pGuess, double* sl, double* sr, int* iters);
+/* Records every Newton-branch exact solve into buf (8 doubles per row:
+ * rhoL, vxL, pL, rhoR, vxR, pR, p*, iterations, negated when the iteration
+ * cap rather than the tolerance ended the solve; x-normal frame) until cap rows;
+ * stop returns the number of solves seen (may exceed cap). Hydro build only. */
+void ora_exact_log_start(double* buf, long cap);
+long ora_exact_log_stop(void);
 
 #ifdef __cplusplus
 }

@@ -48,6 +48,8 @@ def load(mhd: bool) -> ctypes.CDLL:
     L.ora_muscl.argtypes = [_dp, _dp, _dp, ctypes.c_double, _dp, _dp, _dp]
     L.ora_riemann_flux.argtypes = [ctypes.c_int, _dp, _dp, ctypes.c_double, ctypes.c_int, _dp]
     L.ora_exact_star.argtypes = [_dp, _dp, ctypes.c_double, _dp, _dp, ctypes.POINTER(ctypes.c_int)]
+    L.ora_exact_log_start.argtypes = [_dp, ctypes.c_long]
+    L.ora_exact_log_stop.restype = ctypes.c_long
     _libs[mhd] = L
     return L
 
@@ -168,3 +170,25 @@ def run_steps_2d(w0, dx, dy, steps, riemann=5, limiter=1, boundary=(), ghosts=2)
     for _ in range(steps):
         P.step_cfl()
     return P.get_prim()
+
+
+class ExactLog:
+    """Context manager recording the hydro oracle's Newton-branch exact solves:
+    rows (rhoL, vxL, pL, rhoR, vxR, pR, p*, iterations) in the face-normal frame; the
+    iteration count is negated when the cap ended the solve."""
+
+    def __init__(self, cap=1 << 20):
+        self.buf = np.zeros((cap, 8))
+        self.n = 0
+
+    def __enter__(self):
+        load(False).ora_exact_log_start(_p(self.buf), self.buf.shape[0])
+        return self
+
+    def __exit__(self, *exc):
+        self.n = load(False).ora_exact_log_stop()
+        return False
+
+    @property
+    def rows(self):
+        return self.buf[:min(self.n, self.buf.shape[0])]

@@ -54,6 +54,21 @@ static int flux_ax(int ax, const double* l, const double* r, double dt, double* 
 }
 
 extern "C" {
+#ifndef HC_MHD
+double hc_analytic_guess(const double* l, const double* r) { return analytic_guess(P(l), P(r)); }
+// Exact flux along x with a star-pressure guess policy (learned: null or
+// {learned guess, analytic guess}); stats receives
+// newton_iters, exact_calls, trrs, cap_hits, guess_rejects, judge_reruns.
+void hc_exact_flux_guess(const double* l, const double* r, int mode, int max_iters, const double* learned,
+                         double* out, int* stats) {
+    FaceStats st{};
+    ExactOpts eo{max_iters, 1e-12, mode, NewtonLog{}};
+    const LearnedGuess<double> lg{learned ? learned[0] : 0.0, learned ? learned[1] : 0.0, -1};
+    Cout(exact_flux_default(P(l), P(r), eo, &st, learned ? &lg : nullptr), out);
+    const int v[6] = {st.newton_iters, st.exact_calls, st.trrs, st.cap_hits, st.guess_rejects, st.judge_reruns};
+    for (int i = 0; i < 6; i++) stats[i] = v[i];
+}
+#endif
 int hc_nfields(void) { return NF; }
 void hc_prim_to_cons(const double* w, double* u) { Cout(to_cons<M>(P(w)), u); }
 void hc_cons_to_prim(const double* u, double* w) { Pout(to_prim<M>(C(u)), w); }

@@ -1,16 +1,16 @@
-"""The C-ABI library loads and exports every symbol include/dragon_gpu.h
-declares (no compute calls: this runs without a GPU)."""
+"""The C-ABI library loads and exports every symbol include/dragon_gpu.h and
+include/dragon_learned.h declare (no compute calls: this runs without a GPU)."""
 import ctypes
 import os
 import re
 
 from conftest import ROOT
 
-HEADER = os.path.join(ROOT, "include", "dragon_gpu.h")
+HEADERS = [os.path.join(ROOT, "include", h) for h in ("dragon_gpu.h", "dragon_learned.h")]
 
 
 def declared_symbols():
-    txt = open(HEADER).read()
+    txt = "".join(open(h).read() for h in HEADERS)
     txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
     return sorted(set(re.findall(r"\b(dragon_gpu_\w+)\s*\(", txt)))
 
@@ -18,7 +18,8 @@ def declared_symbols():
 def test_header_declares_api():
     syms = declared_symbols()
     for must in ("dragon_gpu_grid_create", "dragon_gpu_advance", "dragon_gpu_unsplit_step", "dragon_gpu_cfl_time",
-                 "dragon_gpu_set_boundary", "dragon_gpu_upload_prim", "dragon_gpu_download_prim"):
+                 "dragon_gpu_set_boundary", "dragon_gpu_upload_prim", "dragon_gpu_download_prim",
+                 "dragon_gpu_mlp_train", "dragon_gpu_mlp_gradient", "dragon_gpu_newton_log_enable"):
         assert must in syms
 
 
