@@ -85,8 +85,22 @@ class NewtonStats(ctypes.Structure):
 
 c_float_p = ctypes.POINTER(ctypes.c_float)
 
-# Every symbol include/dragon_gpu.h and include/dragon_learned.h declare, with
-# its ctypes signature.
+
+class BatchTuning(ctypes.Structure):
+    """dragon_batch_tuning (include/dragon_batch.h)."""
+
+    _fields_ = [("tile_1d", ctypes.c_int), ("ctas_per_sm", ctypes.c_int), ("order", ctypes.c_int),
+                ("graph_steps", ctypes.c_int)]
+
+
+class BatchStats(ctypes.Structure):
+    """dragon_batch_stats (include/dragon_batch.h)."""
+
+    _fields_ = [("steps", ctypes.c_int), ("retries", ctypes.c_int), ("graph_replays", ctypes.c_int),
+                ("work_items", ctypes.c_longlong), ("spin_timeouts", ctypes.c_ulonglong), ("replay_ms", ctypes.c_double)]
+
+# Every symbol include/dragon_gpu.h, include/dragon_learned.h and
+# include/dragon_batch.h declare, with its ctypes signature.
 SIGNATURES = {
     "dragon_gpu_default_config": (None, [ctypes.POINTER(DragonConfig), ctypes.c_int]),
     "dragon_gpu_grid_create": (
@@ -156,6 +170,16 @@ SIGNATURES = {
     "dragon_gpu_mlp_guess": (
         ctypes.c_int, [ctypes.c_void_p, c_double_p, ctypes.c_longlong, c_double_p, c_double_p, c_float_p]),
     "dragon_gpu_grid_set_mlp": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    # dragon_batch.h
+    "dragon_gpu_batch_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p)]),
+    "dragon_gpu_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "dragon_gpu_batch_add_instance": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
+    "dragon_gpu_batch_size": (ctypes.c_int, [ctypes.c_void_p]),
+    "dragon_gpu_batch_set_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(BatchTuning)]),
+    "dragon_gpu_batch_get_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(BatchTuning)]),
+    "dragon_gpu_batch_autotune": (
+        ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(BatchTuning), ctypes.POINTER(ctypes.c_double)]),
+    "dragon_gpu_batch_advance_steps": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(BatchStats)]),
 }
 
 _lib = None

@@ -218,9 +218,12 @@ __device__ inline void bc_faces_axis(const Geo& FG, const int* ncell, double* __
 // Per-step prologue, one CTA: step bookkeeping of the previous step, ghost
 // fill, CFL over the ghost ring combined with the interior max the previous
 // step's epilogue produced, and this step's dt (CFL.cpp:188-213).
+// The body runs on one CTA of any size (a multiple of 32 threads); k_prologue
+// launches it alone, the batched step runs it as one work item.
 template <bool MHD>
-__global__ void __launch_bounds__(1024) k_prologue(Geo G, Geo FG, double* __restrict__ w, double* __restrict__ B,
-                                                   const BCEntry* __restrict__ bcs, StepCtl* ctl, PrologueArgs pa) {
+__device__ __forceinline__ void prologue_body(const Geo& G, const Geo& FG, double* __restrict__ w,
+                                              double* __restrict__ B, const BCEntry* __restrict__ bcs, StepCtl* ctl,
+                                              const PrologueArgs& pa) {
     __shared__ int s_skip;
     __shared__ double s_red[32];
     if (threadIdx.x == 0) {
@@ -333,6 +336,12 @@ __global__ void __launch_bounds__(1024) k_prologue(Geo G, Geo FG, double* __rest
             ctl->t1 = ctl->remaining;
         }
     }
+}
+
+template <bool MHD>
+__global__ void __launch_bounds__(1024) k_prologue(Geo G, Geo FG, double* __restrict__ w, double* __restrict__ B,
+                                                   const BCEntry* __restrict__ bcs, StepCtl* ctl, PrologueArgs pa) {
+    prologue_body<MHD>(G, FG, w, B, bcs, ctl, pa);
 }
 
 // Interior CFL maximum over all interior cells (multi-CTA), accumulated into

@@ -50,7 +50,8 @@ struct StepCtl {
     int steps_done;                // successful steps in this advance
     int max_steps;                 // step budget (<= 0: unlimited)
     int check_cfl;                 // advance(dt, check_cfl)
-    int pad0, pad1;
+    int cur;                       // batched step: buffer holding the current state
+    int pad0;
     // statistics (summed over all face solves of committed and failed steps)
     unsigned long long pivots_exact, hlld_to_hlle, newton_iters, exact_calls, trrs, muscl_first_order;
     unsigned long long cap_hits, guess_rejects, judge_reruns;

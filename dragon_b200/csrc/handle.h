@@ -1,0 +1,79 @@
+// Internal: the grid handle behind dragon_grid* and the runtime helpers the
+// batched step (batch.cu) shares with the single-grid runtime (runtime.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <utility>
+#include <vector>
+
+#include "../../include/dragon_gpu.h"
+#include "../../include/dragon_learned.h"
+#include "boundary.cuh"
+#include "scratch.h"
+
+namespace dgpu {
+struct MlpNet;
+}
+
+struct dragon_grid {
+    int dim = 0;
+    int n[3] = {1, 1, 1};
+    int g = 0;
+    double d[3] = {0, 0, 0};
+    int nf = 5;
+    bool mhd = false;
+    dragon_config cfg{};
+    int solver = dgpu::RS_HLLC;
+    dgpu::Geo cg{}, fg{};
+    double* w[2] = {nullptr, nullptr};
+    double* B[2] = {nullptr, nullptr};
+    int cur = 0;
+    dgpu::StepCtl* ctl = nullptr;
+    dgpu::StepCtl* hctl = nullptr;
+    dgpu::BCEntry* dbcs = nullptr;
+    int nbc = 0;
+    std::vector<dgpu::BCEntry> hbcs;
+    double* stage = nullptr;
+    size_t stage_elems = 0;
+    cudaStream_t stream = nullptr;
+    bool imax_valid = false;
+    unsigned long long launches = 0;
+    // intermediates of the 2D MHD step
+    dgpu::MhdScratch mhd_s{};
+    double* mhd_buf = nullptr;
+    // intermediates of the 3D hydro step
+    dgpu::Hydro3DScratch h3_s{};
+    double* h3_buf = nullptr;
+    // step-kernel timing (dragon_gpu_profile_*)
+    bool prof = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending;
+    double prof_ms = 0;
+    long long prof_n = 0;
+    // exact solver: converged-solve log, learned-guess network, counters
+    double* nlog_rows = nullptr;
+    unsigned long long* nlog_count = nullptr;
+    long long nlog_cap = 0;
+    int nlog_stride = 1;
+    dgpu::MlpNet* mlp_dev = nullptr;
+    dragon_newton_stats ntot{};
+};
+
+namespace dgpu_rt {
+
+// Step arguments for a step that reads buffer c and accumulates its CFL max into slot_out.
+dgpu::StepArgs step_args(const dragon_grid* h, int slot_out);
+// Enqueues the step kernels reading buffer c, writing c ^ 1.
+int launch_step(dragon_grid* h, int c);
+// Enqueues the interior CFL maximum of buffer c into vmax[slot].
+int launch_interior_cfl(dragon_grid* h, int c, int slot);
+// Host mirror of the control block <-> device (header only / all, synchronising).
+int push_ctl(dragon_grid* h);
+int pull_ctl(dragon_grid* h);
+int zero_slot(dragon_grid* h, int slot);
+void reset_ctl(dragon_grid* h, double remaining, int max_steps, int check_cfl);
+void add_newton(dragon_grid* h, const dgpu::StepCtl& c);
+const char* stage_name(int s);
+
+}  // namespace dgpu_rt

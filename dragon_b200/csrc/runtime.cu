@@ -20,6 +20,7 @@
 #include "../../include/dragon_gpu.h"
 #include "../../include/dragon_learned.h"
 #include "boundary.cuh"
+#include "handle.h"
 #include "launchers.h"
 #include "mlp.cuh"
 #include "recon.cuh"
@@ -123,51 +124,8 @@ void dragon_gpu_set_error_message(const char* msg) { g_last_error = msg; }
 // Packed network of a trainer (learned.cu).
 const MlpNet* dragon_mlp_packed_net(dragon_mlp* m);
 
-struct dragon_grid {
-    int dim = 0;
-    int n[3] = {1, 1, 1};
-    int g = 0;
-    double d[3] = {0, 0, 0};
-    int nf = 5;
-    bool mhd = false;
-    dragon_config cfg{};
-    int solver = RS_HLLC;
-    Geo cg{}, fg{};
-    double* w[2] = {nullptr, nullptr};
-    double* B[2] = {nullptr, nullptr};
-    int cur = 0;
-    StepCtl* ctl = nullptr;
-    StepCtl* hctl = nullptr;
-    BCEntry* dbcs = nullptr;
-    int nbc = 0;
-    std::vector<BCEntry> hbcs;
-    double* stage = nullptr;
-    size_t stage_elems = 0;
-    cudaStream_t stream = nullptr;
-    bool imax_valid = false;
-    unsigned long long launches = 0;
-    // intermediates of the 2D MHD step
-    MhdScratch mhd_s{};
-    double* mhd_buf = nullptr;
-    // intermediates of the 3D hydro step
-    Hydro3DScratch h3_s{};
-    double* h3_buf = nullptr;
-    // step-kernel timing (dragon_gpu_profile_*)
-    bool prof = false;
-    std::vector<cudaEvent_t> ev_pool;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending;
-    double prof_ms = 0;
-    long long prof_n = 0;
-    // exact solver: converged-solve log, learned-guess network, counters
-    double* nlog_rows = nullptr;
-    unsigned long long* nlog_count = nullptr;
-    long long nlog_cap = 0;
-    int nlog_stride = 1;
-    MlpNet* mlp_dev = nullptr;
-    dragon_newton_stats ntot{};
-};
 
-namespace {
+namespace dgpu_rt {
 
 size_t dense_count(const Geo& G) { return (size_t)G.ext[0] * G.ext[1] * G.ext[2]; }
 
@@ -428,7 +386,9 @@ int advance_impl(dragon_grid* h, double remaining, int max_steps, int check_cfl,
     }
 }
 
-}  // namespace
+}  // namespace dgpu_rt
+
+using namespace dgpu_rt;
 
 extern "C" {
 

@@ -286,9 +286,11 @@ k_step2d_hydro(Geo G, const double* __restrict__ win, double* __restrict__ wout,
 // state and the last face the raw rightmost ghost as its right state; every
 // cell but the two outermost is updated, and cell n+2g-2 gets the reference's
 // second zero-flux round trip (Splitting.cpp:93-94). All cells are committed.
+// One tile of TS cells (cells tile*TS ...); TS threads. k_step1d runs one
+// tile per CTA, the batched step runs tiles as work items.
 template <bool MHD, int SOLVER, int TS>
-__global__ void __launch_bounds__(TS)
-k_step1d(Geo G, const double* __restrict__ win, double* __restrict__ wout, StepCtl* ctl, StepArgs sa) {
+__device__ __forceinline__ void step1d_tile(const Geo& G, const double* __restrict__ win, double* __restrict__ wout,
+                                            StepCtl* ctl, const StepArgs& sa, int tile) {
     constexpr int NF = MHD ? 8 : 5;
     __shared__ double sw[NF][TS + 4];
     __shared__ double sL[NF][TS + 2], sR[NF][TS + 2];
@@ -297,7 +299,7 @@ k_step1d(Geo G, const double* __restrict__ win, double* __restrict__ wout, StepC
     __shared__ int s_skip;
     if (cta_should_skip(ctl, &s_skip)) return;
     const int np = G.n[0] + 2 * G.g;   // padded cells
-    const int p0 = blockIdx.x * TS;
+    const int p0 = tile * TS;
     const long long PL = G.plane;
     const double dt = *(volatile double*)&ctl->t1;
     const double dt_dx = dt / sa.dx;
@@ -324,14 +326,14 @@ k_step1d(Geo G, const double* __restrict__ win, double* __restrict__ wout, StepC
         return r;
     };
 
-    for (int q = threadIdx.x; q < TS + 4; q += TS) {
+    for (int q = threadIdx.x; q < TS + 4; q += blockDim.x) {
         const int p = p0 - 2 + q;
         if (p >= 0 && p < np)
             for (int f = 0; f < NF; f++) sw[f][q] = win[f * PL + p];
     }
     __syncthreads();
     // half states for cells p in [p0-1, p0+TS]; local index q = p - p0 + 1
-    for (int q = threadIdx.x; q < TS + 2; q += TS) {
+    for (int q = threadIdx.x; q < TS + 2; q += blockDim.x) {
         const int p = p0 - 1 + q;
         if (p >= 1 && p <= np - 2) {
             Prim<double> oL, oR;
@@ -342,7 +344,7 @@ k_step1d(Geo G, const double* __restrict__ win, double* __restrict__ wout, StepC
     }
     __syncthreads();
     // faces p in [p0-1, p0+TS-1]; local index q = p - p0 + 1
-    for (int q = threadIdx.x; q < TS + 1; q += TS) {
+    for (int q = threadIdx.x; q < TS + 1; q += blockDim.x) {
         const int p = p0 - 1 + q;
         if (p < 0 || p > np - 2) continue;
         Prim<double> L = (p == 0) ? getw(q + 1) : get(sR, q);
@@ -355,8 +357,7 @@ k_step1d(Geo G, const double* __restrict__ win, double* __restrict__ wout, StepC
     }
     __syncthreads();
     double vmax = 0.0;
-    {
-        const int q = threadIdx.x;        // cell p = p0 + q
+    for (int q = threadIdx.x; q < TS; q += blockDim.x) {   // cell p = p0 + q
         const int p = p0 + q;
         if (p < np) {
             Prim<double> w0 = getw(q + 2);
@@ -377,7 +378,7 @@ k_step1d(Geo G, const double* __restrict__ win, double* __restrict__ wout, StepC
             const int c = p - G.g;
             if (c >= 0 && c < G.n[0]) {
                 if (!is_physical<MHD>(nw)) record_error(ctl, ST_UNPHYSICAL, p);
-                vmax = cfl_speed_1d<MHD>(nw);
+                vmax = speed_max(vmax, cfl_speed_1d<MHD>(nw));
             }
             store_prim<MHD>(wout, PL, p, nw);
         }
@@ -391,6 +392,12 @@ k_step1d(Geo G, const double* __restrict__ win, double* __restrict__ wout, StepC
     if (st.trrs) atomicAdd(&ctl->trrs, (unsigned long long)st.trrs);
     if (st.cap_hits) atomicAdd(&ctl->cap_hits, (unsigned long long)st.cap_hits);
     if (first_order) atomicAdd(&ctl->muscl_first_order, (unsigned long long)first_order);
+}
+
+template <bool MHD, int SOLVER, int TS>
+__global__ void __launch_bounds__(TS)
+k_step1d(Geo G, const double* __restrict__ win, double* __restrict__ wout, StepCtl* ctl, StepArgs sa) {
+    step1d_tile<MHD, SOLVER, TS>(G, win, wout, ctl, sa, blockIdx.x);
 }
 
 }  // namespace dgpu

@@ -129,20 +129,31 @@ __device__ __forceinline__ bool mhd_skip(const StepCtl* ctl, int* s) {
 }
 __device__ __forceinline__ double mhd_dt(const StepCtl* ctl) { return *(const volatile double*)&ctl->t1; }
 
-// Thread (ti, tj) of a 2D launch covering [i0, i0 + ni) x [j0, j0 + nj).
-__device__ __forceinline__ bool cell_of(int i0, int ni, int j0, int nj, int& i, int& j) {
-    j = j0 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
-    i = i0 + (int)(blockIdx.y * blockDim.y + threadIdx.y);
+// A 32 x 8 tile of cells: block coordinates (bx along j, by along i) and the
+// thread's place in it. The phase kernels take it from their 2D launch; the
+// batched step takes it from a work item.
+struct Tile2 {
+    int bx, by, tx, ty;
+};
+constexpr int kTileJ = 32, kTileI = 8;
+__device__ __forceinline__ Tile2 launch_tile() {
+    return Tile2{(int)blockIdx.x, (int)blockIdx.y, (int)threadIdx.x, (int)threadIdx.y};
+}
+
+// Cell (i, j) of tile T in a sweep covering [i0, i0 + ni) x [j0, j0 + nj).
+__device__ __forceinline__ bool cell_of(const Tile2& T, int i0, int ni, int j0, int nj, int& i, int& j) {
+    j = j0 + T.bx * kTileJ + T.tx;
+    i = i0 + T.by * kTileI + T.ty;
     return i < i0 + ni && j < j0 + nj;
 }
 
 // K1: half states for cells [-2, nx+1]^2 (computeHalfStates_X/Y, Unsplit.cpp:292-342,
 // copyFaceFields_X/Y, B_fields.cpp:166-183) and the body E of w (bodyElectric g=1).
-__global__ void k_mhd2d_halfstates(Mhd2DArgs A) {
+__device__ __forceinline__ void mhd2d_halfstates(const Mhd2DArgs& A, const Tile2& T) {
     __shared__ int s;
     if (mhd_skip(A.ctl, &s)) return;
     int i, j;
-    if (!cell_of(-2, A.G.n[0] + 4, -2, A.G.n[1] + 4, i, j)) return;
+    if (!cell_of(T, -2, A.G.n[0] + 4, -2, A.G.n[1] + 4, i, j)) return;
     const double dt = mhd_dt(A.ctl), dt_dx = dt / A.sa.dx, dt_dy = dt / A.sa.dy;
     const Geo& G = A.G;
     const Geo& F = A.FG;
@@ -176,11 +187,11 @@ __global__ void k_mhd2d_halfstates(Mhd2DArgs A) {
 // K2: predictor fluxes: x faces [-1, nx+1] x rows [-2, ny+1], y faces cols
 // [-2, nx+1] x [-1, ny+1] (ctu_sweep_MHD, CTU.cpp:140-141).
 template <int SOLVER>
-__global__ void k_mhd2d_prelim(Mhd2DArgs A) {
+__device__ __forceinline__ void mhd2d_prelim(const Mhd2DArgs& A, const Tile2& T) {
     __shared__ int s;
     if (mhd_skip(A.ctl, &s)) return;
     int i, j;
-    if (!cell_of(-2, A.G.n[0] + 4, -2, A.G.n[1] + 4, i, j)) return;
+    if (!cell_of(T, -2, A.G.n[0] + 4, -2, A.G.n[1] + 4, i, j)) return;
     const double dt = mhd_dt(A.ctl), dt_dx = dt / A.sa.dx, dt_dy = dt / A.sa.dy;
     const Geo& F = A.FG;
     const long long SP = A.S.plane;
@@ -229,11 +240,11 @@ __device__ __forceinline__ V3 corner_e(const Mhd2DArgs& A, const double* __restr
 }
 
 // K3: predictor corner E on edges [-1, nx+1]^2 against the body E of w.
-__global__ void k_mhd2d_e0(Mhd2DArgs A) {
+__device__ __forceinline__ void mhd2d_e0(const Mhd2DArgs& A, const Tile2& T) {
     __shared__ int s;
     if (mhd_skip(A.ctl, &s)) return;
     int i, j;
-    if (!cell_of(-1, A.G.n[0] + 3, -1, A.G.n[1] + 3, i, j)) return;
+    if (!cell_of(T, -1, A.G.n[0] + 3, -1, A.G.n[1] + 3, i, j)) return;
     store_v3(A.S.e0, A.S.plane, gidx2(A.FG, i, j), corner_e(A, A.S.er, i, j));
 }
 
@@ -241,11 +252,11 @@ __global__ void k_mhd2d_e0(Mhd2DArgs A) {
 // B_fields.cpp:21-40), the half-step cell (applyFluxes g=1 with the predictor
 // fluxes) with face->cell B, its body E, and the CTU corrections of the four
 // half states with the MHD source terms (CTU.cpp:143-202).
-__global__ void k_mhd2d_half(Mhd2DArgs A) {
+__device__ __forceinline__ void mhd2d_half(const Mhd2DArgs& A, const Tile2& T) {
     __shared__ int s;
     if (mhd_skip(A.ctl, &s)) return;
     int i, j;
-    if (!cell_of(-1, A.G.n[0] + 2, -1, A.G.n[1] + 2, i, j)) return;
+    if (!cell_of(T, -1, A.G.n[0] + 2, -1, A.G.n[1] + 2, i, j)) return;
     const double dt = mhd_dt(A.ctl), dt_dx = dt / A.sa.dx, dt_dy = dt / A.sa.dy;
     const double hdx = 0.5 * dt_dx, hdy = 0.5 * dt_dy;
     const Geo& G = A.G;
@@ -307,11 +318,11 @@ __global__ void k_mhd2d_half(Mhd2DArgs A) {
 // K5: final fluxes, x faces [0, nx] x rows [-1, ny], y faces cols [-1, nx] x
 // [0, ny] (Unsplit.cpp:58-60).
 template <int SOLVER>
-__global__ void k_mhd2d_final_flux(Mhd2DArgs A) {
+__device__ __forceinline__ void mhd2d_final_flux(const Mhd2DArgs& A, const Tile2& T) {
     __shared__ int s;
     if (mhd_skip(A.ctl, &s)) return;
     int i, j;
-    if (!cell_of(-1, A.G.n[0] + 2, -1, A.G.n[1] + 2, i, j)) return;
+    if (!cell_of(T, -1, A.G.n[0] + 2, -1, A.G.n[1] + 2, i, j)) return;
     const double dt = mhd_dt(A.ctl), dt_dx = dt / A.sa.dx, dt_dy = dt / A.sa.dy;
     const Geo& F = A.FG;
     const long long SP = A.S.plane;
@@ -334,23 +345,23 @@ __global__ void k_mhd2d_final_flux(Mhd2DArgs A) {
 }
 
 // K6: final corner E on edges [0, nx]^2 against the half-step body E.
-__global__ void k_mhd2d_efinal(Mhd2DArgs A) {
+__device__ __forceinline__ void mhd2d_efinal(const Mhd2DArgs& A, const Tile2& T) {
     __shared__ int s;
     if (mhd_skip(A.ctl, &s)) return;
     int i, j;
-    if (!cell_of(0, A.G.n[0] + 1, 0, A.G.n[1] + 1, i, j)) return;
+    if (!cell_of(T, 0, A.G.n[0] + 1, 0, A.G.n[1] + 1, i, j)) return;
     store_v3(A.S.e0, A.S.plane, gidx2(A.FG, i, j), corner_e(A, A.S.eh, i, j));
 }
 
 // K7: interior cells: conservative update (applyFluxes), Faraday on the faces
 // the cell owns (B_fields.cpp:21-40), face->cell B with the energy gate,
 // physicality and the CFL speed of the committed state.
-__global__ void k_mhd2d_update(Mhd2DArgs A) {
+__device__ __forceinline__ void mhd2d_update(const Mhd2DArgs& A, const Tile2& T) {
     __shared__ int s;
     __shared__ double red[32];
     if (mhd_skip(A.ctl, &s)) return;
     int i, j;
-    const bool in = cell_of(0, A.G.n[0], 0, A.G.n[1], i, j);
+    const bool in = cell_of(T, 0, A.G.n[0], 0, A.G.n[1], i, j);
     const double dt = mhd_dt(A.ctl), dt_dx = dt / A.sa.dx, dt_dy = dt / A.sa.dy;
     const Geo& G = A.G;
     const Geo& F = A.FG;
@@ -394,6 +405,17 @@ __global__ void k_mhd2d_update(Mhd2DArgs A) {
     }
 }
 
+// Kernels of the single-grid step: one 32 x 8 tile per CTA.
+static __global__ void k_mhd2d_halfstates(Mhd2DArgs A) { mhd2d_halfstates(A, launch_tile()); }
+template <int SOLVER>
+__global__ void k_mhd2d_prelim(Mhd2DArgs A) { mhd2d_prelim<SOLVER>(A, launch_tile()); }
+static __global__ void k_mhd2d_e0(Mhd2DArgs A) { mhd2d_e0(A, launch_tile()); }
+static __global__ void k_mhd2d_half(Mhd2DArgs A) { mhd2d_half(A, launch_tile()); }
+template <int SOLVER>
+__global__ void k_mhd2d_final_flux(Mhd2DArgs A) { mhd2d_final_flux<SOLVER>(A, launch_tile()); }
+static __global__ void k_mhd2d_efinal(Mhd2DArgs A) { mhd2d_efinal(A, launch_tile()); }
+static __global__ void k_mhd2d_update(Mhd2DArgs A) { mhd2d_update(A, launch_tile()); }
+
 // 2D MHD CTU + CT step: the seven kernels in order. Ghost cells and faces of
 // the output buffers are first copied from the inputs (the reference commits
 // the interior only, Unsplit.cpp:104-107).
@@ -401,8 +423,8 @@ template <int SOLVER>
 inline int launch_step2d_mhd_t(const Geo& G, const Geo& FG, const double* w, double* wout, const double* B, double* Bout,
                              const MhdScratch& S, StepCtl* ctl, const StepArgs& sa, cudaStream_t st) {
     Mhd2DArgs A{G, FG, w, wout, B, Bout, S, ctl, sa};
-    const dim3 blk(32, 8);
-    auto grid_for = [&](int ni, int nj) { return dim3((nj + 31) / 32, (ni + 7) / 8); };
+    const dim3 blk(kTileJ, kTileI);
+    auto grid_for = [&](int ni, int nj) { return dim3((nj + kTileJ - 1) / kTileJ, (ni + kTileI - 1) / kTileI); };
     const int nx = G.n[0], ny = G.n[1];
     if (cudaMemcpyAsync(wout, w, sizeof(double) * 8 * G.plane, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return 1;
     if (cudaMemcpyAsync(Bout, B, sizeof(double) * 3 * FG.plane, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return 1;

@@ -105,6 +105,39 @@ def blast_2d_mhd(n=128, ghosts=3, p_in=10.0, p_out=0.1, r0=0.1, B=(1.0 / math.sq
     return w, Bf, dx
 
 
+def riemann_1d(n, left, right, ghosts=2, x0=0.5):
+    """1D two-state problem on [0,1] with (rho, u, p) per side."""
+    return sod_1d(n, ghosts=ghosts, x0=x0, left=left, right=right)
+
+
+def batch_instances(n1d=2048, n2d=256, seed=5, sizes_1d=(64, 4096), sizes_2d=(64, 128, 256)):
+    """The batched uneven-instance workload: n1d 1D hydro Riemann problems with
+    N log-uniform in sizes_1d and per-side rho log-uniform in [0.01, 10], p
+    log-uniform in [0.01, 100], u uniform in [-2, 2]; and n2d 2D MHD blasts
+    (rho = 1, p = 0.1, p = 10 inside r < 0.1, B = (1/sqrt2, 1/sqrt2, 0),
+    periodic) at sizes drawn uniformly from sizes_2d. Returns two lists of
+    dicts with the arrays each grid needs."""
+    rng = np.random.default_rng(seed)
+    one = []
+    for _ in range(n1d):
+        n = int(np.exp(rng.uniform(np.log(sizes_1d[0]), np.log(sizes_1d[1] + 1))))
+        n = min(max(n, sizes_1d[0]), sizes_1d[1])
+        st = []
+        for _side in range(2):
+            rho = float(np.exp(rng.uniform(np.log(0.01), np.log(10.0))))
+            p = float(np.exp(rng.uniform(np.log(0.01), np.log(100.0))))
+            u = float(rng.uniform(-2.0, 2.0))
+            st.append((rho, u, p))
+        w, dx = riemann_1d(n, st[0], st[1])
+        one.append({"n": n, "w": w, "dx": dx})
+    two = []
+    for _ in range(n2d):
+        n = int(sizes_2d[rng.integers(len(sizes_2d))])
+        w, Bf, dx = blast_2d_mhd(n, ghosts=3)
+        two.append({"n": n, "w": w, "B": Bf, "dx": dx})
+    return one, two
+
+
 def rel_l1(a: np.ndarray, b: np.ndarray) -> np.ndarray:
     """Relative L1 difference per field over the last axis: sum|a-b| / sum|b|."""
     ax = tuple(range(a.ndim - 1))

@@ -1,12 +1,13 @@
-"""The C-ABI library loads and exports every symbol include/dragon_gpu.h and
-include/dragon_learned.h declare (no compute calls: this runs without a GPU)."""
+"""The C-ABI library loads and exports every symbol include/dragon_gpu.h,
+include/dragon_learned.h and include/dragon_batch.h declare (no compute
+calls: this runs without a GPU)."""
 import ctypes
 import os
 import re
 
 from conftest import ROOT
 
-HEADERS = [os.path.join(ROOT, "include", h) for h in ("dragon_gpu.h", "dragon_learned.h")]
+HEADERS = [os.path.join(ROOT, "include", h) for h in ("dragon_gpu.h", "dragon_learned.h", "dragon_batch.h")]
 
 
 def declared_symbols():
@@ -19,7 +20,8 @@ def test_header_declares_api():
     syms = declared_symbols()
     for must in ("dragon_gpu_grid_create", "dragon_gpu_advance", "dragon_gpu_unsplit_step", "dragon_gpu_cfl_time",
                  "dragon_gpu_set_boundary", "dragon_gpu_upload_prim", "dragon_gpu_download_prim",
-                 "dragon_gpu_mlp_train", "dragon_gpu_mlp_gradient", "dragon_gpu_newton_log_enable"):
+                 "dragon_gpu_mlp_train", "dragon_gpu_mlp_gradient", "dragon_gpu_newton_log_enable",
+                 "dragon_gpu_batch_create", "dragon_gpu_batch_advance_steps", "dragon_gpu_batch_autotune"):
         assert must in syms
 
 
