@@ -14,7 +14,14 @@ fused update). Metric: cell-updates/s (interior cells x steps / time).
   roofline   the fused step kernel's algorithmic HBM bytes (80 B per cell
              update: 5 FP64 fields read + written) over its CUDA-event time;
   cpu_baseline  the DRAGON reference itself (oracle/_ref, DistGrid2D with
-             core_count = host threads) on a bounded number of full steps.
+             core_count = host threads) on a bounded number of full steps;
+  mixed      the mixed FP32/FP64 path on the same workload, with its relative
+             L1 difference per field from the FP64 state;
+  learned_guess  the exact solver's Newton iterations per solve on a 3D blast
+             with the reference's mean guess, the analytic guess and the
+             GPU-trained network's guess (training included);
+  batch      2048 1D hydro + 256 2D MHD grids of uneven sizes advanced by the
+             persistent work-queue kernel, against the same grids one by one.
 
 ``--impl reference`` times only the reference on the host cores and prints its
 own line. Multi-GPU (torchrun): every rank advances its own 1024^2 grid
@@ -229,6 +236,73 @@ def learned_guess_report(train_runs=4, train_n=96, train_steps=15, n=128, p_in=1
     return out
 
 
+def batch_report(steps=500, one_by_one_steps=50):
+    """Batched uneven instances: 2048 1D hydro Riemann problems (N log-uniform
+    in [64, 4096], seeded states) and 256 2D MHD blasts (64^2 / 128^2 / 256^2,
+    HLLD + CT, periodic), each with its own CFL dt, advanced together by the
+    persistent work-queue kernel (autotuned launch shape, CUDA-graph replays);
+    against the same grids advanced one after another."""
+    import torch
+
+    import dragon_b200 as dg
+    from dragon_b200 import batch, problems
+
+    one, two = problems.batch_instances()
+
+    def make():
+        grids = []
+        for spec in one:
+            G = dg.Grid1D(spec["n"], spec["dx"], ghosts=2, config=dg.Config(riemann=dg.RIEMANN_HLLX,
+                                                                              limiter=dg.LIMITER_MC))
+            G.w[...] = spec["w"]
+            grids.append(G)
+        for spec in two:
+            n = spec["n"]
+            G = dg.Grid2D(n, n, spec["dx"], spec["dx"], ghosts=3, config=dg.Config(mhd=True, riemann=dg.RIEMANN_HLLX))
+            G.w[...] = spec["w"]
+            G.B[...] = spec["B"]
+            G.boundary = dg.Periodic()
+            G.initialize_B_fields()
+            grids.append(G)
+        return grids
+
+    cells = sum(s["n"] for s in one) + sum(s["n"] ** 2 for s in two)
+    grids = make()
+    b = batch.Batch(grids)
+    t0 = time.perf_counter()
+    tune, _ = b.autotune(3)
+    tune_s = time.perf_counter() - t0
+    b.advance_steps(3)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    st = b.advance_steps(steps)
+    wall = time.perf_counter() - t0
+    for G in grids:
+        G.close()
+    ref = make()
+    for G in ref:
+        G.advance_steps(3)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for G in ref:
+        G.advance_steps(one_by_one_steps)
+    torch.cuda.synchronize()
+    wall1 = time.perf_counter() - t0
+    for G in ref:
+        G.close()
+    rate = cells * steps / wall
+    rate1 = cells * one_by_one_steps / wall1
+    return {"workload": "2048 1D hydro Riemann problems (N log-uniform [64,4096]) + 256 2D MHD blasts "
+                        "(64^2/128^2/256^2), HLLC / HLLD, MC, own CFL dt each, FP64",
+            "instances": len(one) + len(two), "cells_per_step": cells, "steps": steps,
+            "value": rate, "unit": "cell-updates/s", "device_value": cells * steps / (st["replay_ms"] / 1e3),
+            "one_by_one_value": rate1, "one_by_one_steps": one_by_one_steps, "speedup_vs_one_by_one": rate / rate1,
+            "work_items_per_step": st["work_items"], "graph_replays": st["graph_replays"],
+            "retries": st["retries"], "spin_timeouts": st["spin_timeouts"],
+            "tuning": {"tile_1d": tune.tile_1d, "ctas_per_sm": tune.ctas_per_sm, "order": tune.order,
+                       "graph_steps": tune.graph_steps}, "autotune_seconds": tune_s}
+
+
 def run_gpu(args):
     import torch
     import torch.distributed as dist
@@ -400,6 +474,8 @@ def run_gpu(args):
             line["mixed"] = mixed
         if not args.no_learned:
             line["learned_guess"] = learned_guess_report()
+        if not args.no_batch:
+            line["batch"] = batch_report()
         if not args.no_cpu_baseline:
             cb, why = reference_baseline(1000, 0, budget_s=args.cpu_budget)
             line["cpu_baseline"] = cb if cb else {"unavailable": why}
@@ -419,6 +495,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurement")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned star-pressure guess report")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched uneven-instance report")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--grid", type=int, default=1024, help="cells per axis (default: the 1024^2 workload)")
     args = ap.parse_args()
