@@ -21,7 +21,9 @@ fused update). Metric: cell-updates/s (interior cells x steps / time).
              with the reference's mean guess, the analytic guess and the
              GPU-trained network's guess (training included);
   batch      2048 1D hydro + 256 2D MHD grids of uneven sizes advanced by the
-             persistent work-queue kernel, against the same grids one by one.
+             persistent work-queue kernel, against the same grids one by one;
+  mhd        2D MHD Orszag-Tang 1024^2, FP64 and mixed, with the mixed path's
+             L1 per field and max |div B| of both.
 
 ``--impl reference`` times only the reference on the host cores and prints its
 own line. Multi-GPU (torchrun): every rank advances its own 1024^2 grid
@@ -37,6 +39,8 @@ import subprocess
 import sys
 import threading
 import time
+
+import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
@@ -233,6 +237,58 @@ def learned_guess_report(train_runs=4, train_n=96, train_steps=15, n=128, p_in=1
     out["iteration_reduction_vs_mean"] = m / l_
     out["iteration_reduction_vs_analytic"] = out["analytic_cap64"]["newton_iters_per_solve"] / l_
     net.close()
+    return out
+
+
+def mhd_report(n=1024, steps=20, warmup=3):
+    """2D MHD Orszag-Tang n^2 (HLLD, MC, CTU + CT, BETA_GATED, periodic): the
+    FP64 path and the mixed path on the same state, device time per step with
+    L2 flushed, the mixed path's relative L1 per field against the FP64 state
+    and max |div B| (in units of 1/dx) of both."""
+    import torch
+
+    import dragon_b200 as dg
+    from dragon_b200 import problems
+
+    w0, B0, dx, dy = problems.orszag_tang_2d(n, ghosts=3)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    out = {"workload": f"2D MHD Orszag-Tang {n}^2, HLLD, MC, CTU+CT, BETA_GATED, periodic", "steps": steps + warmup}
+    states = {}
+    for name, prec in (("fp64", dg.PREC_FP64), ("mixed", dg.PREC_MIXED)):
+        G = dg.Grid2D(n, n, dx, dy, ghosts=3, config=dg.Config(mhd=True, riemann=dg.RIEMANN_HLLX, precision=prec))
+        G.w[...] = w0
+        G.B[...] = B0
+        G.boundary = dg.Periodic()
+        G.initialize_B_fields()
+        G.advance_steps(warmup)
+        stream = torch.cuda.ExternalStream(G._lib.dragon_gpu_stream(G._h))
+        ev = []
+        torch.cuda.synchronize()
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+            G.advance_steps(1)
+            b.record(stream)
+            ev.append((a, b))
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in ev) / steps
+        Bf = G.B.copy()
+        g = 3
+        d = (Bf[g + 1:g + n + 1, g:g + n, 0] - Bf[g:g + n, g:g + n, 0]) + (Bf[g:g + n, g + 1:g + n + 1, 1] - Bf[g:g + n, g:g + n, 1])
+        states[name] = (G.w.copy(), Bf)
+        out[name] = {"ms_per_step": ms, "value": n * n / (ms / 1e3), "unit": "cell-updates/s",
+                     "max_abs_divB_dx": float(np.abs(d).max())}
+        G.close()
+    g = 3
+    l1 = problems.rel_l1(states["mixed"][0][g:-g, g:-g], states["fp64"][0][g:-g, g:-g])
+    lb = problems.rel_l1(states["mixed"][1][g:-g, g:-g, :2], states["fp64"][1][g:-g, g:-g, :2])
+    out["mixed"]["speedup_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    out["mixed"]["rel_l1_vs_fp64_per_field"] = [float(x) for x in l1]
+    out["mixed"]["rel_l1_fields"] = ["rho", "p", "vx", "vy", "vz", "Bx", "By", "Bz"]
+    out["mixed"]["rel_l1_face_B_vs_fp64"] = [float(x) for x in lb]
     return out
 
 
@@ -476,6 +532,8 @@ def run_gpu(args):
             line["learned_guess"] = learned_guess_report()
         if not args.no_batch:
             line["batch"] = batch_report()
+        if not args.no_mhd:
+            line["mhd"] = mhd_report()
         if not args.no_cpu_baseline:
             cb, why = reference_baseline(1000, 0, budget_s=args.cpu_budget)
             line["cpu_baseline"] = cb if cb else {"unavailable": why}
@@ -496,6 +554,7 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurement")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned star-pressure guess report")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched uneven-instance report")
+    ap.add_argument("--no-mhd", action="store_true", help="skip the 2D MHD (Orszag-Tang) report")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--grid", type=int, default=1024, help="cells per axis (default: the 1024^2 workload)")
     args = ap.parse_args()

@@ -5,8 +5,9 @@ dragon_b200/libdragon_gpu.so:
   * the FP64 kernels with --fmad=false, so no a*b+c is fused: together with
     IEEE division and square root this keeps the FP64 path's arithmetic
     identical to the reference's (compiled without contraction);
-  * the mixed-precision kernels (step_mixed.cu) with FMA contraction and fast
-    single-precision division / square root; these flags leave FP64 alone.
+  * the mixed-precision kernels (step_mixed.cu, step_mhd_mixed.cu) with FMA
+    contraction and fast single-precision division / square root; these
+    flags leave FP64 alone.
 """
 from __future__ import annotations
 
@@ -25,7 +26,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 BASE = ["-std=c++17", "-O3", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC", "-I" + os.path.join(ROOT, "include")]
 EXACT = ["--fmad=false"]
 FAST32 = ["--fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
-PER_FILE = {"step_mixed.cu": FAST32}
+PER_FILE = {"step_mixed.cu": FAST32, "step_mhd_mixed.cu": FAST32}
 
 
 def _sources():

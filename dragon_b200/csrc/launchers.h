@@ -9,6 +9,7 @@
 namespace dgpu {
 
 struct MhdScratch;
+struct MhdScratchF;
 struct Hydro3DScratch;
 
 int launch_step1d(bool mhd, int solver, const Geo& G, const double* win, double* wout, StepCtl* ctl,
@@ -19,6 +20,8 @@ int launch_step2d_hydro_mixed(int solver, const Geo& G, const double* win, doubl
                               const StepArgs& sa, cudaStream_t st);
 int launch_step2d_mhd(int solver, const Geo& G, const Geo& FG, const double* w, double* wout, const double* B,
                       double* Bout, const MhdScratch& S, StepCtl* ctl, const StepArgs& sa, cudaStream_t st);
+int launch_step2d_mhd_mixed(int solver, const Geo& G, const Geo& FG, const double* w, double* wout, const double* B,
+                            double* Bout, const MhdScratchF& S, StepCtl* ctl, const StepArgs& sa, cudaStream_t st);
 int launch_init_body_fields(const Geo& G, const Geo& FG, double* w, const double* B, cudaStream_t s);
 int launch_step3d_hydro(int solver, const Geo& G, const double* w, double* wout, const Hydro3DScratch& S,
                         StepCtl* ctl, const StepArgs& sa, cudaStream_t st);

@@ -529,8 +529,12 @@ DHD Cons<R> hlld(Prim<R>& L, Prim<R>& Rt, FaceStats* st) {
     R SR = smax(L.vx + cl, Rt.vx + cr);
     if (SR <= R(0)) return prim_flux<true>(Rt);
 
-    R cutoff = smax(dot3(L.Bx, L.By, L.Bz, L.Bx, L.By, L.Bz) + dot3(Rt.Bx, Rt.By, Rt.Bz, Rt.Bx, Rt.By, Rt.Bz), R(1e-100));
-    if (Bx * Bx < R(1e-12) * cutoff) return hlld_zero_b(L, Rt, SL, SR, st);
+    // floor 1e-100 as in HLLD.cpp:50; FP32 has no such number, so it floors at
+    // 1e-30 and takes a zero normal field to the zero-field branch explicitly
+    // (in FP64 Bx == 0 already satisfies the test).
+    const R floor_b2 = sizeof(R) == sizeof(double) ? R(1e-100) : R(1e-30);
+    R cutoff = smax(dot3(L.Bx, L.By, L.Bz, L.Bx, L.By, L.Bz) + dot3(Rt.Bx, Rt.By, Rt.Bz, Rt.Bx, Rt.By, Rt.Bz), floor_b2);
+    if (Bx * Bx < R(1e-12) * cutoff || Bx == R(0)) return hlld_zero_b(L, Rt, SL, SR, st);
 
     R pTL = L.p + dot3(L.Bx, L.By, L.Bz, L.Bx, L.By, L.Bz) * R(k1_8pi);
     R pTR = Rt.p + dot3(Rt.Bx, Rt.By, Rt.Bz, Rt.Bx, Rt.By, Rt.Bz) * R(k1_8pi);

@@ -187,8 +187,15 @@ int launch_step(dragon_grid* h, int c) {
         rc = launch_step1d(h->mhd, h->solver, h->cg, h->w[c], h->w[c ^ 1], h->ctl, sa, h->stream);
     } else if (h->mhd) {
         if (h->dim != 2) return fail(DRAGON_GPU_EUNSUPPORTED, "3D MHD step is not built in this version");
-        rc = launch_step2d_mhd(h->solver, h->cg, h->fg, h->w[c], h->w[c ^ 1], h->B[c], h->B[c ^ 1], h->mhd_s, h->ctl,
-                               sa, h->stream);
+        if (h->cfg.precision == 1) {
+            const MhdScratchF SF{(float*)h->mhd_s.hs, (float*)h->mhd_s.fx, (float*)h->mhd_s.fy, (float*)h->mhd_s.er,
+                                 (float*)h->mhd_s.e0, (float*)h->mhd_s.eh, h->mhd_s.plane};
+            rc = launch_step2d_mhd_mixed(h->solver, h->cg, h->fg, h->w[c], h->w[c ^ 1], h->B[c], h->B[c ^ 1], SF,
+                                         h->ctl, sa, h->stream);
+        } else {
+            rc = launch_step2d_mhd(h->solver, h->cg, h->fg, h->w[c], h->w[c ^ 1], h->B[c], h->B[c ^ 1], h->mhd_s,
+                                   h->ctl, sa, h->stream);
+        }
         nk = kMhd2DKernels;
     } else if (h->dim == 2) {
         rc = (h->cfg.precision == 1)
@@ -440,9 +447,9 @@ int dragon_gpu_grid_create(int dim, int nx, int ny, int nz, double dx, double dy
         delete h;
         return fail(DRAGON_GPU_EUNSUPPORTED, "the learned star-pressure guess is built for 3D hydro grids");
     }
-    if (h->cfg.precision != 0 && !(dim == 2 && !h->mhd)) {
+    if (h->cfg.precision != 0 && dim != 2) {
         delete h;
-        return fail(DRAGON_GPU_EUNSUPPORTED, "the mixed-precision path is built for 2D hydro grids");
+        return fail(DRAGON_GPU_EUNSUPPORTED, "the mixed-precision path is built for 2D grids");
     }
     h->cg = make_geo(dim, h->n, h->g);
     int nfc[3] = {h->n[0] + 1, h->n[1] + 1, h->n[2] + 1};

@@ -17,6 +17,18 @@ struct MhdScratch {
 };
 constexpr int kMhd2DKernels = 7;
 
+// The same intermediates in FP32 (mixed-precision 2D MHD step); they live in
+// the same allocation, which is sized for the FP64 form.
+struct MhdScratchF {
+    float* hs;
+    float* fx;
+    float* fy;
+    float* er;
+    float* e0;
+    float* eh;
+    long long plane;
+};
+
 // 3D hydro step, on the cell geometry.
 struct Hydro3DScratch {
     double* hs;    // 6 x 5 planes: xL, xR, yL, yR, zL, zR

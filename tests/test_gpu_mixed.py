@@ -1,8 +1,8 @@
-"""The mixed FP32/FP64 2D hydro path against the FP64 oracle.
+"""The mixed FP32/FP64 2D hydro and 2D MHD paths against the FP64 oracle.
 
-The mixed path runs reconstruction, limiters and the Riemann solves in FP32
-while the state, every pressure recovery and the flux-difference accumulation
-stay FP64. Its bar is the north-star one: <= 1e-5 relative L1 per field
+The mixed path runs reconstruction, limiters, the Riemann solves and the CTU
+corrections in FP32 while the state, every pressure recovery, the
+flux-difference accumulation and (MHD) the CT face update stay FP64. Its bar is the north-star one: <= 1e-5 relative L1 per field
 against the FP64 reference after the stated steps."""
 import numpy as np
 import pytest
@@ -74,6 +74,51 @@ def test_mixed_sod_strong_shock_stays_physical():
     assert np.all(np.isfinite(G.w)) and np.all(l1 <= TOL_MIXED), l1
 
 
-def test_mixed_only_on_2d_hydro():
+def test_mixed_only_on_2d_grids():
     with pytest.raises(dg.grid._lib.DragonGPUError):
         dg.Grid3D(4, 4, 4, 0.1, 0.1, 0.1, config=dg.Config(precision=dg.PREC_MIXED))
+
+
+def divb_max(B, g, n, dx, dy):
+    bx, by = B[..., 0], B[..., 1]
+    d = (bx[g + 1:g + n + 1, g:g + n] - bx[g:g + n, g:g + n]) / dx + (by[g:g + n, g + 1:g + n + 1] - by[g:g + n, g:g + n]) / dy
+    return np.abs(d).max()
+
+
+def mhd_oracle(n, dx, dy, riemann, limiter):
+    from oracle import port, refgrid
+    kw = dict(dim=2, n=(n, n), d=(dx, dy), ghosts=3, mhd=True, riemann=riemann, limiter=limiter)
+    return refgrid.RefGrid(**kw) if refgrid.available("mhd") else port.PortGrid(**kw)
+
+
+@pytest.mark.parametrize("riemann,limiter", [(dg.RIEMANN_HLLX, dg.LIMITER_MC), (dg.RIEMANN_HLLE, dg.LIMITER_VANLEER)])
+def test_mixed_orszag_tang_l1_and_divb(riemann, limiter):
+    """2D MHD CTU + CT, mixed: <= 1e-5 relative L1 per nonzero field against
+    the FP64 oracle after t = 0.05, and div B at FP64 roundoff (the face update
+    stays FP64)."""
+    n = 64
+    w0, B0, dx, dy = problems.orszag_tang_2d(n, ghosts=3)
+    G = dg.Grid2D(n, n, dx, dy, ghosts=3, config=dg.Config(mhd=True, riemann=riemann, limiter=limiter,
+                                                          precision=dg.PREC_MIXED))
+    R = mhd_oracle(n, dx, dy, riemann, limiter)
+    G.w[...] = w0
+    G.B[...] = B0
+    R.set_prim(w0)
+    R.set_faceB(B0)
+    G.boundary = dg.Periodic()
+    R.set_boundary([(dg.boundary.PERIODIC, 63, 1, None)])
+    G.initialize_B_fields()
+    R.initialize_B_fields()
+    R.advance(0.05)
+    res = G.advance(0.05)
+    assert res.steps > 5
+    g = 3
+    ref, got = R.get_prim()[g:-g, g:-g], G.w[g:-g, g:-g]
+    l1 = problems.rel_l1(got, ref)
+    nonzero = np.abs(ref).sum(axis=(0, 1)) > 0
+    assert np.all(l1[nonzero] <= TOL_MIXED), l1
+    assert np.all(np.abs(got[..., ~nonzero]) <= 1e-12)
+    lb = problems.rel_l1(G.B[g:-g, g:-g, :2], R.get_faceB()[g:-g, g:-g, :2])
+    assert np.all(lb <= TOL_MIXED), lb
+    assert divb_max(G.B, g, n, dx, dy) * dx < 1e-13
+    assert np.any(got != ref)  # really the FP32 path
