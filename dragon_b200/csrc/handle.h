@@ -44,6 +44,9 @@ struct dragon_grid {
     double* mhd_buf = nullptr;
     // intermediates of the 3D hydro step
     dgpu::Hydro3DScratch h3_s{};
+    // intermediates of the 3D MHD step
+    dgpu::Mhd3DScratch m3_s{};
+    double* m3_buf = nullptr;
     double* h3_buf = nullptr;
     // step-kernel timing (dragon_gpu_profile_*)
     bool prof = false;

@@ -11,6 +11,7 @@ namespace dgpu {
 struct MhdScratch;
 struct MhdScratchF;
 struct Hydro3DScratch;
+struct Mhd3DScratch;
 
 int launch_step1d(bool mhd, int solver, const Geo& G, const double* win, double* wout, StepCtl* ctl,
                   const StepArgs& sa, cudaStream_t st);
@@ -25,5 +26,7 @@ int launch_step2d_mhd_mixed(int solver, const Geo& G, const Geo& FG, const doubl
 int launch_init_body_fields(const Geo& G, const Geo& FG, double* w, const double* B, cudaStream_t s);
 int launch_step3d_hydro(int solver, const Geo& G, const double* w, double* wout, const Hydro3DScratch& S,
                         StepCtl* ctl, const StepArgs& sa, cudaStream_t st);
+int launch_step3d_mhd(int solver, const Geo& G, const Geo& FG, const double* w, double* wout, const double* B,
+                      double* Bout, const Mhd3DScratch& S, StepCtl* ctl, const StepArgs& sa, cudaStream_t st);
 
 }  // namespace dgpu

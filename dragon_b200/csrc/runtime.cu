@@ -186,8 +186,11 @@ int launch_step(dragon_grid* h, int c) {
     if (h->dim == 1) {
         rc = launch_step1d(h->mhd, h->solver, h->cg, h->w[c], h->w[c ^ 1], h->ctl, sa, h->stream);
     } else if (h->mhd) {
-        if (h->dim != 2) return fail(DRAGON_GPU_EUNSUPPORTED, "3D MHD step is not built in this version");
-        if (h->cfg.precision == 1) {
+        if (h->dim == 3) {
+            rc = launch_step3d_mhd(h->solver, h->cg, h->fg, h->w[c], h->w[c ^ 1], h->B[c], h->B[c ^ 1], h->m3_s, h->ctl,
+                                   sa, h->stream);
+            nk = kMhd3DKernels;
+        } else if (h->cfg.precision == 1) {
             const MhdScratchF SF{(float*)h->mhd_s.hs, (float*)h->mhd_s.fx, (float*)h->mhd_s.fy, (float*)h->mhd_s.er,
                                  (float*)h->mhd_s.e0, (float*)h->mhd_s.eh, h->mhd_s.plane};
             rc = launch_step2d_mhd_mixed(h->solver, h->cg, h->fg, h->w[c], h->w[c ^ 1], h->B[c], h->B[c ^ 1], SF,
@@ -196,7 +199,7 @@ int launch_step(dragon_grid* h, int c) {
             rc = launch_step2d_mhd(h->solver, h->cg, h->fg, h->w[c], h->w[c ^ 1], h->B[c], h->B[c ^ 1], h->mhd_s,
                                    h->ctl, sa, h->stream);
         }
-        nk = kMhd2DKernels;
+        if (h->dim == 2) nk = kMhd2DKernels;
     } else if (h->dim == 2) {
         rc = (h->cfg.precision == 1)
                  ? launch_step2d_hydro_mixed(h->solver, h->cg, h->w[c], h->w[c ^ 1], h->ctl, sa, h->stream)
@@ -482,6 +485,19 @@ int dragon_gpu_grid_create(int dim, int nx, int ny, int nz, double dx, double dy
         h->mhd_s.eh = h->mhd_buf + 54 * P;
         h->mhd_s.plane = P;
     }
+    if (h->mhd && dim == 3) {
+        const long long P = h->fg.plane;
+        if (cudaMalloc(&h->m3_buf, sizeof(double) * Mhd3DScratch::kPlanes * P) != cudaSuccess)
+            return cleanup(fail(DRAGON_GPU_ECUDA, "cudaMalloc 3D MHD intermediates failed"));
+        h->m3_s.hs = h->m3_buf;
+        h->m3_s.fx = h->m3_buf + 48 * P;
+        h->m3_s.fy = h->m3_buf + 56 * P;
+        h->m3_s.fz = h->m3_buf + 64 * P;
+        h->m3_s.er = h->m3_buf + 72 * P;
+        h->m3_s.e0 = h->m3_buf + 75 * P;
+        h->m3_s.eh = h->m3_buf + 78 * P;
+        h->m3_s.plane = P;
+    }
     if (!h->mhd && dim == 3) {
         const long long P = h->cg.plane;
         if (cudaMalloc(&h->h3_buf, sizeof(double) * Hydro3DScratch::kPlanes * P) != cudaSuccess)
@@ -518,6 +534,7 @@ int dragon_gpu_grid_destroy(dragon_grid* h) {
     if (h->ctl) cudaFree(h->ctl);
     if (h->mhd_buf) cudaFree(h->mhd_buf);
     if (h->h3_buf) cudaFree(h->h3_buf);
+    if (h->m3_buf) cudaFree(h->m3_buf);
     if (h->hctl) cudaFreeHost(h->hctl);
     if (h->dbcs) cudaFree(h->dbcs);
     if (h->stage) cudaFree(h->stage);

@@ -39,4 +39,18 @@ struct Hydro3DScratch {
 };
 constexpr int kHydro3DKernels = 6;
 
+// 3D MHD step, on the face geometry.
+struct Mhd3DScratch {
+    double* hs;   // 6 x 8 planes: xL, xR, yL, yR, zL, zR half states (primitive)
+    double* fx;   // 8 planes each: predictor, then final fluxes
+    double* fy;
+    double* fz;
+    double* er;   // 3 planes: body E of w
+    double* e0;   // 3 planes: predictor edge E, then final edge E
+    double* eh;   // 3 planes: body E of the half-step cells
+    long long plane;
+    static constexpr int kPlanes = 48 + 24 + 9;
+};
+constexpr int kMhd3DKernels = 7;
+
 }  // namespace dgpu

@@ -55,7 +55,7 @@ __device__ __forceinline__ void stc5(double* a, long long P, long long m, const 
 }
 
 // K1: MUSCL half states along all three axes (computeHalfStates_X/Y/Z, Unsplit.cpp:344-436).
-__global__ void k_h3_halfstates(Step3DArgs A) {
+static __global__ void k_h3_halfstates(Step3DArgs A) {
     __shared__ int s;
     if (h3_skip(A.ctl, &s)) return;
     const Geo& G = A.G;
@@ -179,7 +179,7 @@ __device__ __forceinline__ void h3_ctu_flux_learned(const Step3DArgs& A, const d
     stc5(out, SP, m, F);
 }
 
-__global__ void k_h3_prelim_learned(Step3DArgs A) {
+static __global__ void k_h3_prelim_learned(Step3DArgs A) {
     __shared__ int s;
     if (h3_skip(A.ctl, &s)) return;
     const Geo& G = A.G;
@@ -195,7 +195,7 @@ __global__ void k_h3_prelim_learned(Step3DArgs A) {
     h3_stats(A.ctl, st);
 }
 
-__global__ void k_h3_ctu_learned(Step3DArgs A) {
+static __global__ void k_h3_ctu_learned(Step3DArgs A) {
     __shared__ int s;
     if (h3_skip(A.ctl, &s)) return;
     const Geo& G = A.G;
@@ -219,7 +219,7 @@ __global__ void k_h3_ctu_learned(Step3DArgs A) {
     h3_stats(A.ctl, st);
 }
 
-__global__ void k_h3_final_learned(Step3DArgs A) {
+static __global__ void k_h3_final_learned(Step3DArgs A) {
     __shared__ int s;
     if (h3_skip(A.ctl, &s)) return;
     const Geo& G = A.G;
@@ -329,7 +329,7 @@ __device__ __forceinline__ void h3_correct(const Step3DArgs& A, int state_ax, co
 // K4: x states (cells [-1,nx]x[0,ny)x[0,nz)) by F_Yz then F_Zy; y states
 // ([0,nx)x[-1,ny]x[0,nz)) by F_Xz then F_Zx; z states ([0,nx)x[0,ny)x[-1,nz])
 // by F_Xy then F_Yx (CTU.cpp:246-260).
-__global__ void k_h3_correct(Step3DArgs A) {
+static __global__ void k_h3_correct(Step3DArgs A) {
     __shared__ int s;
     if (h3_skip(A.ctl, &s)) return;
     const Geo& G = A.G;
@@ -376,7 +376,7 @@ __global__ void k_h3_final(Step3DArgs A) {
 
 // K6: conservative update of the interior (applyFluxes 3D, Unsplit.cpp:272-288),
 // physicality, CFL speed of the committed state.
-__global__ void k_h3_update(Step3DArgs A) {
+static __global__ void k_h3_update(Step3DArgs A) {
     __shared__ int s;
     __shared__ double red[32];
     if (h3_skip(A.ctl, &s)) return;
