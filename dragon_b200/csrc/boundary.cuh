@@ -41,10 +41,12 @@ struct PrologueArgs {
 
 // ---------------------------------------------------------------------------
 // Cell ghosts of one entry along one axis. The axis index a in 0..dim-1; the
-// remaining axes are transverse. Thread-strided over (side, transverse point,
-// ghost layer).
+// remaining axes are transverse. Strided over (side, transverse point, ghost
+// layer) by the calling threads: tid of nthreads (one CTA in the prologue, a
+// whole grid in k_bc_pass).
 template <bool MHD>
-__device__ void bc_cells_axis(const Geo& G, double* __restrict__ w, const BCEntry& e, int a) {
+__device__ void bc_cells_axis(const Geo& G, double* __restrict__ w, const BCEntry& e, int a, long long tid,
+                              long long nthreads) {
     const int dim = G.dim, ng = G.g;
     const int na = G.n[a];
     const bool negOn = e.faces & (1 << (2 * a)), posOn = e.faces & (1 << (2 * a + 1));
@@ -66,7 +68,7 @@ __device__ void bc_cells_axis(const Geo& G, double* __restrict__ w, const BCEntr
     const long long span0 = tn[0] - t0[0], span1 = tn[1] - t0[1];
     const long long per_side = span0 * span1 * ng;
     const long long total = 2 * per_side;
-    for (long long t = threadIdx.x; t < total; t += blockDim.x) {
+    for (long long t = tid; t < total; t += nthreads) {
         const int side = (int)(t / per_side);  // 0 negative, 1 positive
         long long r = t - side * per_side;
         const int gl = (int)(r % ng) + 1;
@@ -122,7 +124,8 @@ __device__ void bc_cells_axis(const Geo& G, double* __restrict__ w, const BCEntr
 // Face-B ghosts of one entry along one axis. FG is the face geometry (n+1 per
 // axis); n_cells the cell extents. One thread per (side, transverse point)
 // runs the sequential ghost-layer recurrence.
-__device__ inline void bc_faces_axis(const Geo& FG, const int* ncell, double* __restrict__ B, const BCEntry& e, int a) {
+__device__ inline void bc_faces_axis(const Geo& FG, const int* ncell, double* __restrict__ B, const BCEntry& e, int a,
+                                     long long tid, long long nthreads) {
     const int dim = FG.dim, ng = FG.g;
     const int na = ncell[a];
     const bool negOn = e.faces & (1 << (2 * a)), posOn = e.faces & (1 << (2 * a + 1));
@@ -151,7 +154,7 @@ __device__ inline void bc_faces_axis(const Geo& FG, const int* ncell, double* __
     };
     const int tr0 = (a == 0) ? 1 : 0;          // first transverse component
     const int tr1 = (a == 2) ? 1 : 2;          // second transverse component
-    for (long long t = threadIdx.x; t < 2 * per_side; t += blockDim.x) {
+    for (long long t = tid; t < 2 * per_side; t += nthreads) {
         const int side = (int)(t / per_side);
         long long r = t - side * per_side;
         const int c1 = (int)(r % span1) + t0[1];
@@ -229,18 +232,16 @@ __device__ __forceinline__ void prologue_body(const Geo& G, const Geo& FG, doubl
     if (threadIdx.x == 0) {
         int skip = 0;
         if (ctl->err) skip = 1;
+        else if (ctl->done) skip = 1;
         else if (pa.bookkeeping) {
-            if (ctl->done) skip = 1;
-            else {
-                if (ctl->have_prev) {
-                    ctl->remaining -= ctl->t1;
-                    ctl->steps_done += 1;
-                }
-                ctl->have_prev = 1;
-                if (!(ctl->remaining > pa.tol) || (ctl->max_steps > 0 && ctl->steps_done >= ctl->max_steps)) {
-                    ctl->done = 1;
-                    skip = 1;
-                }
+            if (ctl->have_prev) {
+                ctl->remaining -= ctl->t1;
+                ctl->steps_done += 1;
+            }
+            ctl->have_prev = 1;
+            if (!(ctl->remaining > pa.tol) || (ctl->max_steps > 0 && ctl->steps_done >= ctl->max_steps)) {
+                ctl->done = 1;
+                skip = 1;
             }
         }
         s_skip = skip;
@@ -252,13 +253,13 @@ __device__ __forceinline__ void prologue_body(const Geo& G, const Geo& FG, doubl
         for (int e = 0; e < pa.nbc; e++) {
             const BCEntry be = bcs[e];
             for (int a = 0; a < G.dim; a++) {
-                bc_cells_axis<MHD>(G, w, be, a);
+                bc_cells_axis<MHD>(G, w, be, a, threadIdx.x, blockDim.x);
                 __syncthreads();
             }
             if constexpr (MHD) {
                 if (G.dim >= 2) {
                     for (int a = 0; a < G.dim; a++) {
-                        bc_faces_axis(FG, G.n, B, be, a);
+                        bc_faces_axis(FG, G.n, B, be, a, threadIdx.x, blockDim.x);
                         __syncthreads();
                     }
                 }
@@ -342,6 +343,24 @@ template <bool MHD>
 __global__ void __launch_bounds__(1024) k_prologue(Geo G, Geo FG, double* __restrict__ w, double* __restrict__ B,
                                                    const BCEntry* __restrict__ bcs, StepCtl* ctl, PrologueArgs pa) {
     prologue_body<MHD>(G, FG, w, B, bcs, ctl, pa);
+}
+
+// One ghost-fill pass (entry, axis; cells or faces) spread over a whole grid,
+// for grids whose ghost layers are too large for the one-CTA prologue. The
+// passes run as separate launches in the prologue's order (entry by entry,
+// cells axis by axis, then faces axis by axis), so each sees the corners the
+// earlier ones wrote. Skipped once the step is done or failed.
+template <bool MHD>
+__global__ void k_bc_pass(Geo G, Geo FG, double* __restrict__ w, double* __restrict__ B,
+                          const BCEntry* __restrict__ bcs, StepCtl* ctl, int entry, int axis, int faces) {
+    __shared__ int s_skip;
+    if (threadIdx.x == 0) s_skip = *(const volatile int*)&ctl->err | *(const volatile int*)&ctl->done;
+    __syncthreads();
+    if (s_skip) return;
+    const BCEntry be = bcs[entry];
+    const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x, n = (long long)gridDim.x * blockDim.x;
+    if (faces) bc_faces_axis(FG, G.n, B, be, axis, tid, n);
+    else bc_cells_axis<MHD>(G, w, be, axis, tid, n);
 }
 
 // Interior CFL maximum over all interior cells (multi-CTA), accumulated into

@@ -11,6 +11,7 @@
 // reference's catch block (CFL.cpp:194-209).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -231,10 +232,52 @@ int launch_prologue(dragon_grid* h, int c, int bookkeeping, int apply_bc, int co
     pa.apply_bc = apply_bc;
     pa.compute_dt = compute_dt;
     pa.nbc = h->nbc;
-    if (h->mhd) k_prologue<true><<<1, 1024, 0, h->stream>>>(h->cg, h->fg, h->w[c], h->B[c], h->dbcs, h->ctl, pa);
-    else k_prologue<false><<<1, 1024, 0, h->stream>>>(h->cg, h->fg, h->w[c], h->B[c], h->dbcs, h->ctl, pa);
+    auto one_cta = [&](const PrologueArgs& a) {
+        if (h->mhd) k_prologue<true><<<1, 1024, 0, h->stream>>>(h->cg, h->fg, h->w[c], h->B[c], h->dbcs, h->ctl, a);
+        else k_prologue<false><<<1, 1024, 0, h->stream>>>(h->cg, h->fg, h->w[c], h->B[c], h->dbcs, h->ctl, a);
+        h->launches++;
+    };
+    if (h->dim == 1 || !apply_bc || h->nbc == 0) {
+        one_cta(pa);
+        CK(cudaGetLastError());
+        return 0;
+    }
+    // 2D / 3D: bookkeeping on one CTA, every ghost-fill pass over a whole grid,
+    // then the ring CFL and dt on one CTA (the ghost layers of a large grid are
+    // far too much work for one CTA)
+    PrologueArgs head = pa;
+    head.apply_bc = 0;
+    head.compute_dt = 0;
+    one_cta(head);
+    long long ext_max = 1;  // largest transverse section of a pass, padded
+    for (int a = 0; a < h->dim; a++) {
+        long long sec = 1;
+        for (int b = 0; b < h->dim; b++)
+            if (b != a) sec *= (h->fg.ext[b]);
+        ext_max = std::max(ext_max, sec);
+    }
+    const long long items = 2 * ext_max * h->g;
+    const int blocks = (int)std::max<long long>(1, std::min<long long>((items + 255) / 256, 148 * 8));
+    for (int e = 0; e < h->nbc; e++) {
+        for (int a = 0; a < h->dim; a++) {
+            if (h->mhd) k_bc_pass<true><<<blocks, 256, 0, h->stream>>>(h->cg, h->fg, h->w[c], h->B[c], h->dbcs, h->ctl, e, a, 0);
+            else k_bc_pass<false><<<blocks, 256, 0, h->stream>>>(h->cg, h->fg, h->w[c], h->B[c], h->dbcs, h->ctl, e, a, 0);
+            h->launches++;
+        }
+        if (h->mhd) {
+            for (int a = 0; a < h->dim; a++) {
+                k_bc_pass<true><<<blocks, 256, 0, h->stream>>>(h->cg, h->fg, h->w[c], h->B[c], h->dbcs, h->ctl, e, a, 1);
+                h->launches++;
+            }
+        }
+    }
+    if (compute_dt) {
+        PrologueArgs tail = pa;
+        tail.bookkeeping = 0;
+        tail.apply_bc = 0;
+        one_cta(tail);
+    }
     CK(cudaGetLastError());
-    h->launches++;
     return 0;
 }
 
