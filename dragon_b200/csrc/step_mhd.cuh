@@ -407,12 +407,14 @@ __device__ __forceinline__ void mhd2d_update(const Mhd2DArgs& A, const Tile2& T)
 
 // Kernels of the single-grid step: one 32 x 8 tile per CTA.
 static __global__ void k_mhd2d_halfstates(Mhd2DArgs A) { mhd2d_halfstates(A, launch_tile()); }
+// The flux kernels carry two CTAs per SM (<= 128 registers): at their natural
+// ~166 registers one 256-thread CTA fits, and the HLLD chains stall on latency.
 template <int SOLVER>
-__global__ void k_mhd2d_prelim(Mhd2DArgs A) { mhd2d_prelim<SOLVER>(A, launch_tile()); }
+__global__ void __launch_bounds__(256, 2) k_mhd2d_prelim(Mhd2DArgs A) { mhd2d_prelim<SOLVER>(A, launch_tile()); }
 static __global__ void k_mhd2d_e0(Mhd2DArgs A) { mhd2d_e0(A, launch_tile()); }
-static __global__ void k_mhd2d_half(Mhd2DArgs A) { mhd2d_half(A, launch_tile()); }
+static __global__ void __launch_bounds__(256, 2) k_mhd2d_half(Mhd2DArgs A) { mhd2d_half(A, launch_tile()); }
 template <int SOLVER>
-__global__ void k_mhd2d_final_flux(Mhd2DArgs A) { mhd2d_final_flux<SOLVER>(A, launch_tile()); }
+__global__ void __launch_bounds__(256, 2) k_mhd2d_final_flux(Mhd2DArgs A) { mhd2d_final_flux<SOLVER>(A, launch_tile()); }
 static __global__ void k_mhd2d_efinal(Mhd2DArgs A) { mhd2d_efinal(A, launch_tile()); }
 static __global__ void k_mhd2d_update(Mhd2DArgs A) { mhd2d_update(A, launch_tile()); }
 

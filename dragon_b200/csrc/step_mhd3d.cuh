@@ -118,7 +118,7 @@ __device__ __forceinline__ void m3_face_flux(const Mhd3DArgs& A, int i, int j, i
 // K2 (box [-2, n+1]^3) and K5 (box [-1, n]^3): faces along an axis from its
 // lower bound (-1 predictor, 0 final) up to the box's top.
 template <int SOLVER, bool FINAL>
-__global__ void k_m3_fluxes(Mhd3DArgs A) {
+__global__ void __launch_bounds__(256, 2) k_m3_fluxes(Mhd3DArgs A) {
     __shared__ int s;
     if (h3_skip(A.ctl, &s)) return;
     int i, j, k;

@@ -93,7 +93,7 @@ __global__ void k_mx_halfstates(Mhd2DMixedArgs A) {
 // K2 / K5: FP32 Riemann fluxes over the given ranges (predictor: the x faces
 // [-1, nx+1] x rows [-2, ny+1] and the y faces; final: [0, nx] x [-1, ny]).
 template <int SOLVER, bool FINAL>
-__global__ void k_mx_fluxes(Mhd2DMixedArgs A) {
+__global__ void __launch_bounds__(256, 3) k_mx_fluxes(Mhd2DMixedArgs A) {
     __shared__ int s;
     if (mhd_skip(A.ctl, &s)) return;
     int i, j;
