@@ -128,6 +128,9 @@ SIGNATURES = {
     "dragon_gpu_advance": (
         ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.POINTER(AdvanceStats)]),
     "dragon_gpu_advance_steps": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(AdvanceStats)]),
+    "dragon_gpu_split_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(StepStatus)]),
+    "dragon_gpu_advance_split": (
+        ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.POINTER(AdvanceStats)]),
     "dragon_gpu_stream": (ctypes.c_void_p, [ctypes.c_void_p]),
     "dragon_gpu_device_state": (
         ctypes.c_int,

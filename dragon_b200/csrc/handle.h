@@ -44,6 +44,10 @@ struct dragon_grid {
     double* mhd_buf = nullptr;
     // intermediates of the 3D hydro step
     dgpu::Hydro3DScratch h3_s{};
+    // Strang-split path: third state buffer and the sweep-order counter (Grid::sweep_step)
+    double* wsplit = nullptr;
+    long long sweep_step = 0;
+    bool split_mode = false;
     // intermediates of the 3D MHD step
     dgpu::Mhd3DScratch m3_s{};
     double* m3_buf = nullptr;
@@ -67,7 +71,7 @@ namespace dgpu_rt {
 
 // Step arguments for a step that reads buffer c and accumulates its CFL max into slot_out.
 dgpu::StepArgs step_args(const dragon_grid* h, int slot_out);
-// Enqueues the step kernels reading buffer c, writing c ^ 1.
+// Enqueues the step kernels reading buffer c, writing c ^ 1 (the unsplit step).
 int launch_step(dragon_grid* h, int c);
 // Enqueues the interior CFL maximum of buffer c into vmax[slot].
 int launch_interior_cfl(dragon_grid* h, int c, int slot);

@@ -23,6 +23,9 @@ int launch_step2d_mhd(int solver, const Geo& G, const Geo& FG, const double* w, 
                       double* Bout, const MhdScratch& S, StepCtl* ctl, const StepArgs& sa, cudaStream_t st);
 int launch_step2d_mhd_mixed(int solver, const Geo& G, const Geo& FG, const double* w, double* wout, const double* B,
                             double* Bout, const MhdScratchF& S, StepCtl* ctl, const StepArgs& sa, cudaStream_t st);
+// One Strang-split sweep (Godunov::sweep along every line of an axis), dt = factor * t1.
+int launch_sweep(int solver, int axis, const Geo& G, const double* win, double* wout, StepCtl* ctl, const StepArgs& sa,
+                 double factor, cudaStream_t st);
 int launch_init_body_fields(const Geo& G, const Geo& FG, double* w, const double* B, cudaStream_t s);
 int launch_step3d_hydro(int solver, const Geo& G, const double* w, double* wout, const Hydro3DScratch& S,
                         StepCtl* ctl, const StepArgs& sa, cudaStream_t st);

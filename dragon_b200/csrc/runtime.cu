@@ -218,7 +218,10 @@ int launch_step(dragon_grid* h, int c) {
     return 0;
 }
 
-int launch_prologue(dragon_grid* h, int c, int bookkeeping, int apply_bc, int compute_dt, int slot_in, int slot_out) {
+// w_buf overrides the state buffer (the Strang-split sweeps fill ghosts of their intermediate buffers).
+int launch_prologue(dragon_grid* h, int c, int bookkeeping, int apply_bc, int compute_dt, int slot_in, int slot_out,
+                    double* w_buf = nullptr) {
+    double* W = w_buf ? w_buf : h->w[c];
     PrologueArgs pa;
     pa.dx = h->d[0];
     pa.dy = h->d[1];
@@ -233,8 +236,8 @@ int launch_prologue(dragon_grid* h, int c, int bookkeeping, int apply_bc, int co
     pa.compute_dt = compute_dt;
     pa.nbc = h->nbc;
     auto one_cta = [&](const PrologueArgs& a) {
-        if (h->mhd) k_prologue<true><<<1, 1024, 0, h->stream>>>(h->cg, h->fg, h->w[c], h->B[c], h->dbcs, h->ctl, a);
-        else k_prologue<false><<<1, 1024, 0, h->stream>>>(h->cg, h->fg, h->w[c], h->B[c], h->dbcs, h->ctl, a);
+        if (h->mhd) k_prologue<true><<<1, 1024, 0, h->stream>>>(h->cg, h->fg, W, h->B[c], h->dbcs, h->ctl, a);
+        else k_prologue<false><<<1, 1024, 0, h->stream>>>(h->cg, h->fg, W, h->B[c], h->dbcs, h->ctl, a);
         h->launches++;
     };
     if (h->dim == 1 || !apply_bc || h->nbc == 0) {
@@ -260,13 +263,13 @@ int launch_prologue(dragon_grid* h, int c, int bookkeeping, int apply_bc, int co
     const int blocks = (int)std::max<long long>(1, std::min<long long>((items + 255) / 256, 148 * 8));
     for (int e = 0; e < h->nbc; e++) {
         for (int a = 0; a < h->dim; a++) {
-            if (h->mhd) k_bc_pass<true><<<blocks, 256, 0, h->stream>>>(h->cg, h->fg, h->w[c], h->B[c], h->dbcs, h->ctl, e, a, 0);
-            else k_bc_pass<false><<<blocks, 256, 0, h->stream>>>(h->cg, h->fg, h->w[c], h->B[c], h->dbcs, h->ctl, e, a, 0);
+            if (h->mhd) k_bc_pass<true><<<blocks, 256, 0, h->stream>>>(h->cg, h->fg, W, h->B[c], h->dbcs, h->ctl, e, a, 0);
+            else k_bc_pass<false><<<blocks, 256, 0, h->stream>>>(h->cg, h->fg, W, h->B[c], h->dbcs, h->ctl, e, a, 0);
             h->launches++;
         }
         if (h->mhd) {
             for (int a = 0; a < h->dim; a++) {
-                k_bc_pass<true><<<blocks, 256, 0, h->stream>>>(h->cg, h->fg, h->w[c], h->B[c], h->dbcs, h->ctl, e, a, 1);
+                k_bc_pass<true><<<blocks, 256, 0, h->stream>>>(h->cg, h->fg, W, h->B[c], h->dbcs, h->ctl, e, a, 1);
                 h->launches++;
             }
         }
@@ -290,6 +293,53 @@ int launch_interior_cfl(dragon_grid* h, int c, int slot) {
     CK(cudaGetLastError());
     h->launches++;
     return 0;
+}
+
+// Grid2D/3D::split_step (Splitting.cpp:118-217) reading buffer c, writing
+// c ^ 1: the Strang sequence of sweeps for sweep counter value `order`
+// (2D: XYX / YXY alternating; 3D: the six cyclic and anticyclic orders),
+// each sweep after a ghost fill of its input (advanceX/Y/Z apply the boundary
+// first). Intermediates alternate between c ^ 1 and a third buffer, so buffer
+// c stays intact for a retry. The interior CFL maximum of the result is
+// accumulated into slot c ^ 1 for the next step's dt. 1D grids take the
+// unsplit step (Grid1D::split_step calls unsplit_step).
+int launch_split_step(dragon_grid* h, int c, long long order) {
+    if (h->dim == 1) return launch_step(h, c);
+    if (!h->wsplit) {
+        CK(cudaMalloc(&h->wsplit, sizeof(double) * h->nf * h->cg.plane));
+        CK(cudaMemsetAsync(h->wsplit, 0, sizeof(double) * h->nf * h->cg.plane, h->stream));
+    }
+    struct Sweep { int axis; double f; };
+    Sweep seq[5];
+    int ns = 3;
+    if (h->dim == 2) {
+        const int a = (order % 2 == 0) ? 0 : 1, b = 1 - a;
+        seq[0] = {a, 0.5}; seq[1] = {b, 1.0}; seq[2] = {a, 0.5};
+    } else {
+        static const int orders[6][3] = {{0, 1, 2}, {2, 0, 1}, {1, 2, 0}, {2, 1, 0}, {0, 2, 1}, {1, 0, 2}};
+        const int* o = orders[order % 6];
+        ns = 5;
+        seq[0] = {o[0], 0.5}; seq[1] = {o[1], 0.5}; seq[2] = {o[2], 1.0}; seq[3] = {o[1], 0.5}; seq[4] = {o[0], 0.5};
+    }
+    const StepArgs sa = step_args(h, c ^ 1);
+    double* in = h->w[c];
+    double* out = h->w[c ^ 1];
+    for (int k = 0; k < ns; k++) {
+        int rc = launch_prologue(h, c, 0, 1, 0, 2, 2, in);
+        if (rc) return rc;
+        if (launch_sweep(h->solver, seq[k].axis, h->cg, in, out, h->ctl, sa, seq[k].f, h->stream))
+            return fail(DRAGON_GPU_ECUDA, std::string("sweep launch failed: ") + cudaGetErrorString(cudaGetLastError()));
+        h->launches++;
+        in = out;
+        out = (out == h->w[c ^ 1]) ? h->wsplit : h->w[c ^ 1];
+    }
+    return launch_interior_cfl(h, c ^ 1, c ^ 1);
+}
+
+// The step the current mode takes: unsplit, or split with the sweep order of
+// advance-local step k.
+int launch_any_step(dragon_grid* h, int c, long long k) {
+    return h->split_mode ? launch_split_step(h, c, h->sweep_step + k) : launch_step(h, c);
 }
 
 // Writes the control block's header (everything before vmax) from the host mirror.
@@ -381,7 +431,7 @@ int advance_impl(dragon_grid* h, double remaining, int max_steps, int check_cfl,
             if ((rc = launch_prologue(h, c, 1, 1, 1, c, c ^ 1))) return rc;
             // with a step budget, the prologue after the last step only accounts it
             if (max_steps > 0 && k + b >= max_steps) continue;
-            if ((rc = launch_step(h, c))) return rc;
+            if ((rc = launch_any_step(h, c, k + b))) return rc;
         }
         k += nb;
         if ((rc = pull_ctl(h))) return rc;
@@ -396,6 +446,7 @@ int advance_impl(dragon_grid* h, double remaining, int max_steps, int check_cfl,
             if (st) { st->steps = (int)ks; fill_failure(C, &st->failure, DRAGON_GPU_ESTEP); }
             if (stage == ST_CFL_ZERO) {
                 if (st) st->failure.code = DRAGON_GPU_ECFL;
+                if (h->split_mode) h->sweep_step += ks;
                 return fail(DRAGON_GPU_ECFL, stage_name(stage));
             }
             // CFL.cpp:198-208: halve t1 and retry the same step on the same ghosts.
@@ -405,6 +456,7 @@ int advance_impl(dragon_grid* h, double remaining, int max_steps, int check_cfl,
                 t1 *= 0.5;
                 if (t1 < h->cfg.timestep_tol) {
                     if (st) { st->retries = retries; st->failure.code = DRAGON_GPU_EDT; }
+                    if (h->split_mode) h->sweep_step += ks;
                     return fail(DRAGON_GPU_EDT, std::string("Timestep has fallen below minimum after: ") + stage_name(stage));
                 }
                 C.t1 = t1;
@@ -414,7 +466,7 @@ int advance_impl(dragon_grid* h, double remaining, int max_steps, int check_cfl,
                 C.cap_hits = C.guess_rejects = C.judge_reruns = 0;
                 if ((rc = push_ctl(h))) return rc;
                 if ((rc = zero_slot(h, c ^ 1))) return rc;
-                if ((rc = launch_step(h, c))) return rc;
+                if ((rc = launch_any_step(h, c, ks))) return rc;
                 if ((rc = pull_ctl(h))) return rc;
                 if (!C.err) break;
                 fill_stats(h, C, st);
@@ -427,6 +479,7 @@ int advance_impl(dragon_grid* h, double remaining, int max_steps, int check_cfl,
         if (C.done) {
             h->cur = cur0 ^ (int)(C.steps_done & 1);
             h->imax_valid = true;
+            if (h->split_mode) h->sweep_step += C.steps_done;
             fill_stats(h, C, st);
             if (st) {
                 st->steps = C.steps_done;
@@ -578,6 +631,7 @@ int dragon_gpu_grid_destroy(dragon_grid* h) {
     if (h->mhd_buf) cudaFree(h->mhd_buf);
     if (h->h3_buf) cudaFree(h->h3_buf);
     if (h->m3_buf) cudaFree(h->m3_buf);
+    if (h->wsplit) cudaFree(h->wsplit);
     if (h->hctl) cudaFreeHost(h->hctl);
     if (h->dbcs) cudaFree(h->dbcs);
     if (h->stage) cudaFree(h->stage);
@@ -730,6 +784,46 @@ int dragon_gpu_advance_steps(dragon_grid* h, int nsteps, dragon_advance_stats* s
     if (!h || nsteps < 0) return fail(DRAGON_GPU_EINVAL, "invalid argument");
     if (nsteps == 0) { if (st) std::memset(st, 0, sizeof(*st)); return 0; }
     return advance_impl(h, INFINITY, nsteps, 1, st);
+}
+
+static int split_unsupported(const dragon_grid* h) {
+    if (h->mhd && h->dim >= 2) return fail(DRAGON_GPU_EUNSUPPORTED, "the Strang-split path is built for hydro grids");
+    if (h->cfg.precision != 0) return fail(DRAGON_GPU_EUNSUPPORTED, "the Strang-split path runs in FP64");
+    return 0;
+}
+
+int dragon_gpu_split_step(dragon_grid* h, double dt, dragon_step_status* st) {
+    if (!h) return fail(DRAGON_GPU_EINVAL, "null handle");
+    int rc = split_unsupported(h);
+    if (rc) return rc;
+    if (st) std::memset(st, 0, sizeof(*st));
+    reset_ctl(h, 0.0, 0, 0);
+    h->hctl->t1 = dt;
+    if ((rc = push_ctl(h))) return rc;
+    const int c = h->cur;
+    if ((rc = zero_slot(h, c ^ 1))) return rc;
+    if ((rc = launch_split_step(h, c, h->sweep_step))) return rc;
+    if ((rc = pull_ctl(h))) return rc;
+    add_newton(h, *h->hctl);
+    if (h->hctl->err) {
+        fill_failure(*h->hctl, st, DRAGON_GPU_ESTEP);
+        return fail(DRAGON_GPU_ESTEP, stage_name((int)(h->hctl->err_key >> 56)));
+    }
+    h->cur = c ^ 1;
+    h->imax_valid = true;
+    if (h->dim >= 2) h->sweep_step++;
+    if (st) st->dt = dt;
+    return 0;
+}
+
+int dragon_gpu_advance_split(dragon_grid* h, double interval, int check_cfl, dragon_advance_stats* st) {
+    if (!h) return fail(DRAGON_GPU_EINVAL, "null handle");
+    int rc = split_unsupported(h);
+    if (rc) return rc;
+    h->split_mode = h->dim >= 2;
+    rc = advance_impl(h, interval, 0, check_cfl ? 1 : 0, st);
+    h->split_mode = false;
+    return rc;
 }
 
 void* dragon_gpu_stream(dragon_grid* h) { return h ? (void*)h->stream : nullptr; }

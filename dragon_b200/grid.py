@@ -251,7 +251,24 @@ class _GridBase:
         self._device_ran()
 
     def split_step(self, dt: float):
-        raise NotImplementedError("the Strang-split path is outside the unsplit update")
+        """Grid::split_step (Splitting.cpp:118-217): Strang sequence of 1D
+        sweeps (hydro); raises StepFailed, committing nothing, on failure."""
+        self._to_device()
+        st = _lib.StepStatus()
+        rc = self._lib.dragon_gpu_split_step(self._h, float(dt), ctypes.byref(st))
+        if rc == 3:
+            raise StepFailed(self._lib.dragon_gpu_last_error().decode(), st)
+        _lib.check(rc)
+        self._device_ran()
+
+    def advance_split(self, dt: float, check_cfl: bool = True) -> AdvanceResult:
+        """Grid::advance_split (CFL.cpp:160-184): the advance loop around split_step."""
+        self._to_device()
+        st = _lib.AdvanceStats()
+        rc = self._lib.dragon_gpu_advance_split(self._h, float(dt), int(bool(check_cfl)), ctypes.byref(st))
+        self._device_ran()
+        _lib.check(rc)
+        return _result(st)
 
     def advance(self, dt: float, check_cfl: bool = True) -> AdvanceResult:
         """Grid::advance (CFL.cpp:151-213), run entirely on the device."""

@@ -141,6 +141,15 @@ int dragon_gpu_unsplit_step(dragon_grid* g, double dt, dragon_step_status* st);
 int dragon_gpu_advance(dragon_grid* g, double interval, int check_cfl, dragon_advance_stats* st);
 /* advance by a fixed number of CFL-limited steps (the interval is unbounded). */
 int dragon_gpu_advance_steps(dragon_grid* g, int nsteps, dragon_advance_stats* st);
+/* Grid::split_step(dt) (Hydro/Godunov/Splitting.cpp:118-217): the Strang
+ * sequence of one-dimensional Godunov sweeps, the order alternating with the
+ * grid's sweep counter (2D: XYX / YXY; 3D: the six cyclic and anticyclic
+ * orders); 1D grids take the unsplit step, as the reference does. Hydro grids,
+ * FP64. No commit on failure. */
+int dragon_gpu_split_step(dragon_grid* g, double dt, dragon_step_status* st);
+/* Grid::advance_split(dt, check_cfl) (Hydro/CFL/CFL.cpp:160-184): the advance
+ * loop around split_step. */
+int dragon_gpu_advance_split(dragon_grid* g, double interval, int check_cfl, dragon_advance_stats* st);
 
 /* The CUDA stream the handle's kernels run on (cudaStream_t). */
 void* dragon_gpu_stream(dragon_grid* g);

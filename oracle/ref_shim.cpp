@@ -317,6 +317,30 @@ int ref_advance(void* p, double dt, int check_cfl, char* msg, int len) {
     return 0;
 }
 
+int ref_split_step(void* p, double dt, char* msg, int len) {
+    auto* h = static_cast<Handle*>(p);
+    serial_mode(h);
+    try {
+        h->grid->split_step(dt);
+    } catch (const std::exception& e) {
+        put_msg(msg, len, e.what());
+        return 1;
+    }
+    return 0;
+}
+
+int ref_advance_split(void* p, double dt, int check_cfl, char* msg, int len) {
+    auto* h = static_cast<Handle*>(p);
+    serial_mode(h);
+    try {
+        h->grid->advance_split(dt, check_cfl != 0);
+    } catch (const std::exception& e) {
+        put_msg(msg, len, e.what());
+        return 1;
+    }
+    return 0;
+}
+
 // --- unit-level entry points (pure functions of the reference) ---------------
 
 int ref_limiter(int kind, double a, double b, double* out) {

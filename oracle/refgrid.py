@@ -49,6 +49,8 @@ def load(variant: str) -> ctypes.CDLL:
     L.ref_cfl_time.argtypes = [ctypes.c_void_p, _dp, ctypes.c_char_p, ctypes.c_int]
     L.ref_unsplit_step.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_char_p, ctypes.c_int]
     L.ref_advance.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
+    L.ref_split_step.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_char_p, ctypes.c_int]
+    L.ref_advance_split.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
     L.ref_config.argtypes = [ctypes.c_int] * 5
     L.ref_cfl_speed.restype = ctypes.c_double
     L.ref_cfl_speed.argtypes = [_dp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
@@ -168,6 +170,18 @@ class RefGrid:
         self._cfg()
         msg = ctypes.create_string_buffer(256)
         if self.L.ref_advance(self.h, float(dt), int(check_cfl), msg, 256):
+            raise RefError(msg.value.decode())
+
+    def split_step(self, dt: float):
+        self._cfg()
+        msg = ctypes.create_string_buffer(256)
+        if self.L.ref_split_step(self.h, float(dt), msg, 256):
+            raise RefError(msg.value.decode())
+
+    def advance_split(self, dt: float, check_cfl: bool = True):
+        self._cfg()
+        msg = ctypes.create_string_buffer(256)
+        if self.L.ref_advance_split(self.h, float(dt), int(check_cfl), msg, 256):
             raise RefError(msg.value.decode())
 
     def step_cfl(self) -> float:

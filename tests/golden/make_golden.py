@@ -14,6 +14,9 @@ the CPU oracle to reproduce in seconds:
                     periodic, advance to t = 0.02
   blast_3d_10       3D blast 10^3 (p 10 inside r < 0.1), exact solver, MC,
                     Outflow, three CFL steps
+  kh_split_2d_32    the 2D shear layer through advance_split (Strang), t = 0.05
+  blast_split_3d_12 3D blast 12^3, HLLC, van Leer, Reflective, advance_split
+                    to t = 0.01 (all six sweep orders)
 
 Run: python tests/golden/make_golden.py
 """
@@ -72,8 +75,27 @@ def blast():
     return {"w0": w0, "w": R.get_prim(), "d": d, "dts": np.array(dts)}
 
 
+def kh_split():
+    w0, dx, dy = problems.kelvin_helmholtz_2d(32, ghosts=2, seed=77)
+    R = refgrid.RefGrid(dim=2, n=(32, 32), d=(dx, dy), ghosts=2, riemann=RIEMANN_HLLC, limiter=LIM_VANLEER)
+    R.set_prim(w0)
+    R.set_boundary(bc_entries_from(boundary.as_list(boundary.Periodic())))
+    R.advance_split(0.05)
+    return {"w0": w0, "w": R.get_prim(), "dx": dx, "dy": dy, "t": 0.05}
+
+
+def blast_split():
+    w0, d = problems.blast_3d(12, ghosts=2, p_in=10.0)
+    R = refgrid.RefGrid(dim=3, n=(12, 12, 12), d=(d, d, d), ghosts=2, riemann=RIEMANN_HLLC, limiter=LIM_VANLEER)
+    R.set_prim(w0)
+    R.set_boundary(bc_entries_from(boundary.as_list(boundary.Reflective())))
+    R.advance_split(0.01)
+    return {"w0": w0, "w": R.get_prim(), "d": d, "t": 0.01}
+
+
 def main():
-    for name, fn in (("sod_1d_512", sod), ("kh_2d_32", kh), ("ot_2d_24", ot), ("blast_3d_10", blast)):
+    for name, fn in (("sod_1d_512", sod), ("kh_2d_32", kh), ("ot_2d_24", ot), ("blast_3d_10", blast),
+                     ("kh_split_2d_32", kh_split), ("blast_split_3d_12", blast_split)):
         out = fn()
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
         print(name, {k: np.shape(v) for k, v in out.items()})
