@@ -122,6 +122,8 @@ SIGNATURES = {
     "dragon_gpu_download_faceB": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
     "dragon_gpu_set_boundary": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(BCDesc), ctypes.c_int]),
     "dragon_gpu_apply_boundary": (ctypes.c_int, [ctypes.c_void_p]),
+    "dragon_gpu_boundary_entries": (ctypes.c_int, [ctypes.c_void_p]),
+    "dragon_gpu_apply_boundary_range": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "dragon_gpu_initialize_B_fields": (ctypes.c_int, [ctypes.c_void_p]),
     "dragon_gpu_cfl_time": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
     "dragon_gpu_unsplit_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(StepStatus)]),

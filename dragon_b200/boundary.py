@@ -68,6 +68,19 @@ class GhostFill:
     def state(self) -> Sequence[float]:
         return ()
 
+    def apply(self, grid) -> None:
+        """GhostFill::apply(Grid&) (GhostFill.hpp:16-30). A user element
+        subclasses GhostFill and overrides this to fill grid's ghost cells on
+        the host (grid.w / grid.B, or grid[i, j] with ghost coordinates), like
+        the reference's Jet (Jets.hpp:12-39). Grids then run such lists on the
+        host-driven slow path: the built-in elements stay on the device, the
+        state crosses to the host around each user element."""
+        raise NotImplementedError(f"{type(self).__name__} is a built-in element applied on the device")
+
+    @property
+    def is_custom(self) -> bool:
+        return type(self).apply is not GhostFill.apply
+
     def __add__(self, other):
         return BoundaryList(self) + other
 
@@ -176,6 +189,9 @@ class BoundaryList:
     def __iadd__(self, other):
         self.append(other)
         return self
+
+    def has_custom(self) -> bool:
+        return any(e.is_custom for e in self.elements)
 
     def uncovered_faces(self) -> int:
         m = X | Y | Z

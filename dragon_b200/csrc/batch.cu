@@ -250,6 +250,7 @@ BatchInst make_inst(dragon_grid* h, int tile) {
     pa.apply_bc = 1;
     pa.compute_dt = 1;
     pa.nbc = h->nbc;
+    pa.bc_first = 0;
     I.ntiles[0] = 1;
     I.ntj[0] = 1;
     if (I.kind == K1D) {

@@ -36,7 +36,8 @@ struct PrologueArgs {
     int bookkeeping;    // account for the previous step (advance loop)
     int apply_bc;       // fill ghosts
     int compute_dt;     // compute t1 from the CFL limit
-    int nbc;
+    int nbc;            // entries to apply
+    int bc_first;       // first entry to apply
 };
 
 // ---------------------------------------------------------------------------
@@ -250,7 +251,7 @@ __device__ __forceinline__ void prologue_body(const Geo& G, const Geo& FG, doubl
     if (s_skip) return;
 
     if (pa.apply_bc) {
-        for (int e = 0; e < pa.nbc; e++) {
+        for (int e = pa.bc_first; e < pa.bc_first + pa.nbc; e++) {
             const BCEntry be = bcs[e];
             for (int a = 0; a < G.dim; a++) {
                 bc_cells_axis<MHD>(G, w, be, a, threadIdx.x, blockDim.x);

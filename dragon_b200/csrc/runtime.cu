@@ -220,8 +220,9 @@ int launch_step(dragon_grid* h, int c) {
 
 // w_buf overrides the state buffer (the Strang-split sweeps fill ghosts of their intermediate buffers).
 int launch_prologue(dragon_grid* h, int c, int bookkeeping, int apply_bc, int compute_dt, int slot_in, int slot_out,
-                    double* w_buf = nullptr) {
+                    double* w_buf = nullptr, int bc_first = 0, int bc_count = -1) {
     double* W = w_buf ? w_buf : h->w[c];
+    if (bc_count < 0) bc_count = h->nbc - bc_first;
     PrologueArgs pa;
     pa.dx = h->d[0];
     pa.dy = h->d[1];
@@ -234,13 +235,14 @@ int launch_prologue(dragon_grid* h, int c, int bookkeeping, int apply_bc, int co
     pa.bookkeeping = bookkeeping;
     pa.apply_bc = apply_bc;
     pa.compute_dt = compute_dt;
-    pa.nbc = h->nbc;
+    pa.nbc = bc_count;
+    pa.bc_first = bc_first;
     auto one_cta = [&](const PrologueArgs& a) {
         if (h->mhd) k_prologue<true><<<1, 1024, 0, h->stream>>>(h->cg, h->fg, W, h->B[c], h->dbcs, h->ctl, a);
         else k_prologue<false><<<1, 1024, 0, h->stream>>>(h->cg, h->fg, W, h->B[c], h->dbcs, h->ctl, a);
         h->launches++;
     };
-    if (h->dim == 1 || !apply_bc || h->nbc == 0) {
+    if (h->dim == 1 || !apply_bc || bc_count == 0) {
         one_cta(pa);
         CK(cudaGetLastError());
         return 0;
@@ -261,7 +263,7 @@ int launch_prologue(dragon_grid* h, int c, int bookkeeping, int apply_bc, int co
     }
     const long long items = 2 * ext_max * h->g;
     const int blocks = (int)std::max<long long>(1, std::min<long long>((items + 255) / 256, 148 * 8));
-    for (int e = 0; e < h->nbc; e++) {
+    for (int e = bc_first; e < bc_first + bc_count; e++) {
         for (int a = 0; a < h->dim; a++) {
             if (h->mhd) k_bc_pass<true><<<blocks, 256, 0, h->stream>>>(h->cg, h->fg, W, h->B[c], h->dbcs, h->ctl, e, a, 0);
             else k_bc_pass<false><<<blocks, 256, 0, h->stream>>>(h->cg, h->fg, W, h->B[c], h->dbcs, h->ctl, e, a, 0);
@@ -735,6 +737,19 @@ int dragon_gpu_apply_boundary(dragon_grid* h) {
     int rc = push_ctl(h);
     if (rc) return rc;
     if ((rc = launch_prologue(h, h->cur, 0, 1, 0, 2, 2))) return rc;
+    CK(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int dragon_gpu_boundary_entries(const dragon_grid* h) { return h ? h->nbc : 0; }
+
+int dragon_gpu_apply_boundary_range(dragon_grid* h, int first, int count) {
+    if (!h || first < 0 || count < 0 || first + count > h->nbc) return fail(DRAGON_GPU_EINVAL, "entry range out of bounds");
+    if (count == 0) return 0;
+    reset_ctl(h, 0.0, 0, 0);
+    int rc = push_ctl(h);
+    if (rc) return rc;
+    if ((rc = launch_prologue(h, h->cur, 0, 1, 0, 2, 2, nullptr, first, count))) return rc;
     CK(cudaStreamSynchronize(h->stream));
     return 0;
 }

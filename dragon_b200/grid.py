@@ -20,7 +20,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _lib
-from .boundary import BoundaryList, as_list
+from .boundary import IGNORE, BoundaryList, as_list
 
 # Config ids (DRAGON/Config.h)
 RIEMANN_EXACT, RIEMANN_HLL, RIEMANN_HLLC, RIEMANN_HLLD, RIEMANN_HLLE, RIEMANN_HLLX, RIEMANN_ROE = range(7)
@@ -217,7 +217,8 @@ class _GridBase:
         els = list(self._boundary)
         arr = (_lib.BCDesc * max(1, len(els)))()
         for k, e in enumerate(els):
-            arr[k].type = e.kind
+            # user elements run on the host; on the device they only cover their faces
+            arr[k].type = IGNORE if e.is_custom else e.kind
             arr[k].faces = e.get_faces()
             arr[k].corners = int(e.corners)
             st = list(e.state()) + [0.0] * 8
@@ -225,7 +226,53 @@ class _GridBase:
                 arr[k].state[q] = st[q]
         _lib.check(self._lib.dragon_gpu_set_boundary(self._h, arr, len(els)))
 
+    def _apply_boundary_host(self):
+        """BoundaryList::apply (BoundaryList.hpp:79-93) with user elements: the
+        device applies the runs of built-in entries (the implicit Outflow first),
+        each user element's apply(grid) runs on the host between them."""
+        els = list(self._boundary)
+        off = int(self._lib.dragon_gpu_boundary_entries(self._h)) - len(els)
+        start = 0  # first device entry not yet applied
+        for k, e in enumerate(els + [None]):
+            if e is not None and not e.is_custom:
+                continue
+            stop = off + k
+            if stop > start:
+                self._to_device()
+                _lib.check(self._lib.dragon_gpu_apply_boundary_range(self._h, start, stop - start))
+                self._device_ran()
+            if e is not None:
+                e.apply(self)
+            start = off + k + 1
+
+    def _advance_host(self, dt: float, check_cfl: bool, split: bool) -> AdvanceResult:
+        """Grid::advance_unsplit / advance_split (CFL.cpp:160-213) driven from
+        the host, for boundary lists with user elements."""
+        tol = self.config.timestep_tol
+        res = AdvanceResult()
+        while dt > tol:
+            self._apply_boundary_host()
+            t1 = min(dt, self.cfl_time()) if check_cfl else dt
+            while True:
+                try:
+                    (self.split_step if split else self.unsplit_step)(t1)
+                    break
+                except StepFailed:
+                    res.retries += 1
+                    t1 *= 0.5
+                    if t1 < tol:
+                        raise
+            dt -= t1
+            res.steps += 1
+            res.last_dt = t1
+            res.time_advanced += t1
+        return res
+
     def apply_boundary(self):
+        if self._boundary.has_custom():
+            self._push_boundary()
+            self._apply_boundary_host()
+            return
         self._push_boundary()
         self._to_device()
         _lib.check(self._lib.dragon_gpu_apply_boundary(self._h))
@@ -263,6 +310,8 @@ class _GridBase:
 
     def advance_split(self, dt: float, check_cfl: bool = True) -> AdvanceResult:
         """Grid::advance_split (CFL.cpp:160-184): the advance loop around split_step."""
+        if self._boundary.has_custom():
+            return self._advance_host(dt, check_cfl, split=True)
         self._to_device()
         st = _lib.AdvanceStats()
         rc = self._lib.dragon_gpu_advance_split(self._h, float(dt), int(bool(check_cfl)), ctypes.byref(st))
@@ -271,7 +320,10 @@ class _GridBase:
         return _result(st)
 
     def advance(self, dt: float, check_cfl: bool = True) -> AdvanceResult:
-        """Grid::advance (CFL.cpp:151-213), run entirely on the device."""
+        """Grid::advance (CFL.cpp:151-213), run entirely on the device (on the
+        host-driven path when the boundary list has user elements)."""
+        if self._boundary.has_custom():
+            return self._advance_host(dt, check_cfl, split=False)
         self._to_device()
         st = _lib.AdvanceStats()
         rc = self._lib.dragon_gpu_advance(self._h, float(dt), int(bool(check_cfl)), ctypes.byref(st))
@@ -283,6 +335,16 @@ class _GridBase:
 
     def advance_steps(self, nsteps: int) -> AdvanceResult:
         """nsteps CFL-limited steps (each the reference's advance(cfl_time()))."""
+        if self._boundary.has_custom():
+            res = AdvanceResult()
+            for _ in range(int(nsteps)):
+                self._apply_boundary_host()
+                r = self._advance_host(self.cfl_time(), True, split=False)
+                res.steps += r.steps
+                res.retries += r.retries
+                res.last_dt = r.last_dt
+                res.time_advanced += r.time_advanced
+            return res
         self._to_device()
         st = _lib.AdvanceStats()
         rc = self._lib.dragon_gpu_advance_steps(self._h, int(nsteps), ctypes.byref(st))

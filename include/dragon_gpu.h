@@ -124,6 +124,13 @@ int dragon_gpu_download_faceB(dragon_grid* g, double* host);
 int dragon_gpu_set_boundary(dragon_grid* g, const dragon_bc_desc* list, int n);
 /* boundary.apply(grid) (Boundary/BoundaryList.hpp:79-93) */
 int dragon_gpu_apply_boundary(dragon_grid* g);
+/* Entries of the compiled list (the implicit Outflow first when some face is
+ * uncovered, then the caller's entries in order), and one contiguous range of
+ * them applied alone: a host that owns custom GhostFill elements (passed here
+ * as Ignore entries covering their faces) runs its own fills between ranges,
+ * in list order (BoundaryList.hpp:79-93). */
+int dragon_gpu_boundary_entries(const dragon_grid* g);
+int dragon_gpu_apply_boundary_range(dragon_grid* g, int first, int count);
 /* Grid::initialize_B_fields (MHD/B_fields.cpp:117-149) */
 int dragon_gpu_initialize_B_fields(dragon_grid* g);
 

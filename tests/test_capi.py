@@ -36,3 +36,15 @@ def test_library_exports_every_declared_symbol():
 def test_python_binding_covers_header():
     from dragon_b200 import _lib
     assert set(declared_symbols()) <= set(_lib.SIGNATURES)
+
+
+def test_user_ghostfill_detection():
+    import dragon_b200 as dg
+
+    class Jet(dg.GhostFill):
+        def apply(self, grid):
+            pass
+
+    assert Jet("X-").is_custom and not dg.Outflow().is_custom and not dg.Periodic("Y").is_custom
+    assert (dg.Periodic("Y") + Jet("X-")).has_custom()
+    assert not (dg.Periodic("Y") + dg.Reflective("X")).has_custom()
