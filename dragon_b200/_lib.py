@@ -133,6 +133,14 @@ SIGNATURES = {
     "dragon_gpu_split_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(StepStatus)]),
     "dragon_gpu_advance_split": (
         ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.POINTER(AdvanceStats)]),
+    "dragon_gpu_halo_size": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]),
+    "dragon_gpu_halo_pack": (
+        ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_int] * 5 + [ctypes.c_void_p, ctypes.c_int]),
+    "dragon_gpu_halo_unpack": (
+        ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_int] * 5 + [ctypes.c_void_p, ctypes.c_int]),
+    "dragon_gpu_step_rollback": (ctypes.c_int, [ctypes.c_void_p]),
     "dragon_gpu_stream": (ctypes.c_void_p, [ctypes.c_void_p]),
     "dragon_gpu_device_state": (
         ctypes.c_int,

@@ -44,6 +44,8 @@ struct dragon_grid {
     double* mhd_buf = nullptr;
     // intermediates of the 3D hydro step
     dgpu::Hydro3DScratch h3_s{};
+    // the last unsplit_step committed (a sharded step may still be undone)
+    bool can_rollback = false;
     // Strang-split path: third state buffer and the sweep-order counter (Grid::sweep_step)
     double* wsplit = nullptr;
     long long sweep_step = 0;

@@ -100,6 +100,35 @@ __global__ void k_soa_to_aos(const double* __restrict__ soa, double* __restrict_
     }
 }
 
+// Copies `layers` whole layers along `axis` starting at padded position
+// `first`, every field, between the state and a contiguous buffer ordered
+// field, layer, transverse (the last axis fastest). Transverse axes cover
+// padded positions [t0, t0 + tn).
+__global__ void k_halo(Geo G, double* __restrict__ w, double* __restrict__ buf, int axis, int first, int layers, int nf,
+                       int t0, int tn0, int tn1, int unpack) {
+    int tax[2] = {0, 0}, nt = 0;
+    for (int b = 0; b < G.dim; b++)
+        if (b != axis) tax[nt++] = b;
+    const long long sec = (long long)tn0 * tn1;
+    const long long per_field = (long long)layers * sec;
+    const long long total = per_field * nf;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        const int f = (int)(t / per_field);
+        const long long r = t % per_field;
+        int q[3] = {0, 0, 0};
+        q[axis] = first + (int)(r / sec);
+        const long long tr = r % sec;
+        if (nt > 0) q[tax[0]] = t0 + (int)(tr / tn1);
+        if (nt > 1) q[tax[1]] = t0 + (int)(tr % tn1);
+        long long m;
+        if (G.dim == 1) m = q[0];
+        else if (G.dim == 2) m = (long long)q[0] * G.pitch + q[1];
+        else m = (long long)q[0] * G.pitch2 + (long long)q[1] * G.pitch + q[2];
+        if (unpack) w[f * G.plane + m] = buf[t];
+        else buf[t] = w[f * G.plane + m];
+    }
+}
+
 int solver_id(const dragon_config& c) {
     if (c.mhd) {
         if (c.riemann == RS_HLL) return RS_HLL;
@@ -414,6 +443,7 @@ const char* stage_name(int s) {
 // Shared advance loop. remaining/max_steps select advance(interval) or a step count.
 int advance_impl(dragon_grid* h, double remaining, int max_steps, int check_cfl, dragon_advance_stats* st) {
     if (st) std::memset(st, 0, sizeof(*st));
+    h->can_rollback = false;
     const int cur0 = h->cur;
     reset_ctl(h, remaining, max_steps, check_cfl);
     int rc = push_ctl(h);
@@ -673,6 +703,7 @@ static int transfer(dragon_grid* h, bool up, bool faces, double* host) {
         CK(cudaGetLastError());
         h->launches++;
         h->imax_valid = false;
+        h->can_rollback = false;
     } else {
         k_soa_to_aos<<<blocks, 256, 0, h->stream>>>(dev, h->stage, G, nf);
         CK(cudaGetLastError());
@@ -786,8 +817,101 @@ int dragon_gpu_unsplit_step(dragon_grid* h, double dt, dragon_step_status* st) {
     }
     h->cur = c ^ 1;
     h->imax_valid = true;
+    h->can_rollback = true;
     if (st) st->dt = dt;
     return 0;
+}
+
+int dragon_gpu_step_rollback(dragon_grid* h) {
+    if (!h) return fail(DRAGON_GPU_EINVAL, "null handle");
+    if (!h->can_rollback) return fail(DRAGON_GPU_EINVAL, "no committed unsplit_step to undo");
+    CK(cudaStreamSynchronize(h->stream));
+    h->cur ^= 1;
+    h->imax_valid = false;
+    h->can_rollback = false;
+    return 0;
+}
+
+// Geometry, base pointer and field count of the cell state or face-centred B.
+static int halo_target(dragon_grid* h, int faces, Geo* G, double** base, int* nf) {
+    if (faces) {
+        if (!h->mhd || h->dim < 2) return fail(DRAGON_GPU_EINVAL, "grid has no face-centred B");
+        *G = h->fg;
+        *base = h->B[h->cur];
+        *nf = 3;
+    } else {
+        *G = h->cg;
+        *base = h->w[h->cur];
+        *nf = h->nf;
+    }
+    return 0;
+}
+
+// Transverse extent (padded positions) of a halo along `axis`.
+static void halo_transverse(const Geo& G, int dim, int axis, int corners, int* t0, int tn[2]) {
+    tn[0] = tn[1] = 1;
+    *t0 = corners ? 0 : G.g;
+    int k = 0;
+    for (int b = 0; b < dim; b++)
+        if (b != axis) tn[k++] = corners ? G.ext[b] : G.n[b];
+}
+
+int dragon_gpu_halo_size(const dragon_grid* h, int axis, int layers, int faces, int corners, long long* count) {
+    if (!h || axis < 0 || axis >= h->dim || layers < 1 || !count) return fail(DRAGON_GPU_EINVAL, "invalid halo arguments");
+    Geo G;
+    double* base;
+    int nf;
+    int rc = halo_target(const_cast<dragon_grid*>(h), faces, &G, &base, &nf);
+    if (rc) return rc;
+    if (layers > G.ext[axis]) return fail(DRAGON_GPU_EINVAL, "more layers than the padded extent");
+    int t0, tn[2];
+    halo_transverse(G, h->dim, axis, corners, &t0, tn);
+    *count = (long long)nf * layers * tn[0] * tn[1];
+    return 0;
+}
+
+static int halo_copy(dragon_grid* h, int axis, int first, int layers, int faces, int corners, double* buf, int on_device,
+                     bool pack) {
+    long long count = 0;
+    int rc = dragon_gpu_halo_size(h, axis, layers, faces, corners, &count);
+    if (rc) return rc;
+    Geo G;
+    double* base;
+    int nf;
+    halo_target(h, faces, &G, &base, &nf);
+    if (first < -G.g || first + layers > G.n[axis] + G.g) return fail(DRAGON_GPU_EINVAL, "halo layers outside the padded grid");
+    if (!buf) return fail(DRAGON_GPU_EINVAL, "null buffer");
+    int t0, tn[2];
+    halo_transverse(G, h->dim, axis, corners, &t0, tn);
+    double* dev = buf;
+    if (!on_device) {
+        // the staging buffer holds a whole padded grid, so any set of layers fits
+        if ((size_t)count > h->stage_elems) return fail(DRAGON_GPU_EINVAL, "halo larger than the staging buffer");
+        dev = h->stage;
+    }
+    if (!pack && !on_device) CK(cudaMemcpyAsync(dev, buf, sizeof(double) * count, cudaMemcpyHostToDevice, h->stream));
+    const int blocks = (int)std::min<long long>((count + 255) / 256, 148 * 16);
+    k_halo<<<std::max(blocks, 1), 256, 0, h->stream>>>(G, base, dev, axis, first + G.g, layers, nf, t0, tn[0], tn[1],
+                                                       pack ? 0 : 1);
+    CK(cudaGetLastError());
+    h->launches++;
+    if (pack && !on_device) CK(cudaMemcpyAsync(buf, dev, sizeof(double) * count, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (!pack) {
+        h->imax_valid = false;
+        h->can_rollback = false;
+    }
+    return 0;
+}
+
+int dragon_gpu_halo_pack(dragon_grid* h, int axis, int first, int layers, int faces, int corners, double* buf,
+                         int buf_on_device) {
+    return halo_copy(h, axis, first, layers, faces, corners, buf, buf_on_device, true);
+}
+
+int dragon_gpu_halo_unpack(dragon_grid* h, int axis, int first, int layers, int faces, int corners, const double* buf,
+                           int buf_on_device) {
+    return halo_copy(h, axis, first, layers, faces, corners, const_cast<double*>(buf), buf_on_device, false);
 }
 
 int dragon_gpu_advance(dragon_grid* h, double interval, int check_cfl, dragon_advance_stats* st) {

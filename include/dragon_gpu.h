@@ -158,6 +158,26 @@ int dragon_gpu_split_step(dragon_grid* g, double dt, dragon_step_status* st);
  * loop around split_step. */
 int dragon_gpu_advance_split(dragon_grid* g, double interval, int check_cfl, dragon_advance_stats* st);
 
+/* A grid split across devices (the role of DistGrid's children,
+ * Refinement/DistGrid.cpp:58-346): copies of whole layers along `axis`
+ * between the current state and a contiguous buffer, for the halo exchange.
+ * The layers are [first, first + layers) in interior coordinates (ghost
+ * layers negative or >= n); the transverse axes span the padded extent when
+ * `corners` is set, else their interior (a GhostFill's corner flag,
+ * Boundary/GhostFill.hpp:28). faces = 0 selects the cell-centred fields,
+ * faces = 1 the face-centred B (n + 1 positions per axis, 3 components; MHD
+ * 2D/3D). buf holds halo_size doubles ordered field, layer, transverse (last
+ * axis fastest), in device memory when buf_on_device, else host memory. */
+int dragon_gpu_halo_size(const dragon_grid* g, int axis, int layers, int faces, int corners, long long* count);
+int dragon_gpu_halo_pack(dragon_grid* g, int axis, int first, int layers, int faces, int corners, double* buf,
+                         int buf_on_device);
+int dragon_gpu_halo_unpack(dragon_grid* g, int axis, int first, int layers, int faces, int corners, const double* buf,
+                           int buf_on_device);
+/* Undoes the last unsplit_step if nothing touched the grid since (its input
+ * buffer is intact): the all-or-nothing commit of a step taken by several
+ * devices together (DistGrid.cpp:292-304). */
+int dragon_gpu_step_rollback(dragon_grid* g);
+
 /* The CUDA stream the handle's kernels run on (cudaStream_t). */
 void* dragon_gpu_stream(dragon_grid* g);
 /* Device pointer to the current primitive planes (SoA, NF planes of
