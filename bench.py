@@ -10,7 +10,9 @@ fused update). Metric: cell-updates/s (interior cells x steps / time).
   value      device time of K steps with the state resident in HBM, L2 flushed
              before every step (the 84 MB double-buffered state fits in L2);
   e2e        the same steps through the C ABI with the state uploaded from
-             pinned host memory and downloaded back every step;
+             pinned host memory and downloaded back every step, three grids
+             in flight on their own streams so copies overlap steps
+             (one_grid_value: a single grid, nothing overlapped);
   roofline   the fused step kernel's algorithmic HBM bytes (80 B per cell
              update: 5 FP64 fields read + written) over its CUDA-event time;
   cpu_baseline  the DRAGON reference itself (oracle/_ref, DistGrid2D with
@@ -49,6 +51,61 @@ N = 1024  # grid extent per axis (--grid overrides it, e.g. for profiling captur
 CELL_BYTES = 80  # 5 FP64 primitive fields read + written per cell update
 METRIC = "cell-updates/s (2D unsplit CTU hydro, FP64)"
 WORKLOAD = "kelvin_helmholtz_2d_1024sq_hllc_vanleer_cfl0.3_periodic"
+
+
+E2E_INFLIGHT = 3  # grids whose upload / step / download overlap on separate streams
+
+
+def e2e_run(G0, grids, dev, steps, barrier):
+    """Device time (ms) of `steps` end-to-end steps on each grid in `grids`
+    through the C ABI: upload of the padded state from pinned host memory,
+    one CFL step, download of the result into pinned host memory. Each grid
+    runs on its own stream from its own host thread (the ABI calls release
+    the GIL), so one grid's copies overlap another's step; the time runs from
+    an event every stream waits on to the last stream's final event."""
+    import torch
+    from dragon_b200 import _lib
+    L = G0._lib
+    streams = [torch.cuda.ExternalStream(L.dragon_gpu_stream(g._h), device=dev) for g in grids]
+    pins = []
+    for g in grids:
+        host_in = torch.from_numpy(g.w.copy()).pin_memory()
+        host_out = torch.empty_like(host_in).pin_memory()
+        pins.append((host_in, host_out))
+    barrier()
+    torch.cuda.synchronize()
+    start = torch.cuda.Event(enable_timing=True)
+    start.record(streams[0])
+    for s in streams[1:]:
+        s.wait_event(start)
+    ends = [torch.cuda.Event(enable_timing=True) for _ in grids]
+    errors = []
+
+    def worker(k):
+        try:
+            g, (hin, hout) = grids[k], pins[k]
+            pin_in = hin.numpy().ctypes.data_as(_lib.c_double_p)
+            pin_out = hout.numpy().ctypes.data_as(_lib.c_double_p)
+            for _ in range(steps):
+                _lib.check(L.dragon_gpu_upload_prim(g._h, pin_in))
+                _lib.check(L.dragon_gpu_advance_steps(g._h, 1, None))
+                _lib.check(L.dragon_gpu_download_prim(g._h, pin_out))
+            ends[k].record(streams[k])
+        except Exception as e:  # reported after the join
+            errors.append(e)
+
+    threads = [threading.Thread(target=worker, args=(k,)) for k in range(len(grids))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    if errors:
+        raise errors[0]
+    torch.cuda.synchronize()
+    for g in grids:  # the device now holds the downloaded results; the host mirrors are stale
+        g._host_dirty = False
+        g._device_ran()
+    return max(start.elapsed_time(e) for e in ends)
 
 
 def measured_peaks():
@@ -477,30 +534,25 @@ def run_gpu(args):
         Gm.close()
 
     # ---- e2e: through the C ABI from pinned host memory, every step
-    host_in = torch.from_numpy(G.w.copy()).pin_memory()
-    host_out = torch.empty_like(host_in).pin_memory()
-    pin_in = host_in.numpy()
-    pin_out = host_out.numpy()
-    dptr = _lib.c_double_p
     e2e_steps = max(1, min(args.steps, 10))
-    barrier()
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(e2e_steps):
-        _lib.check(L.dragon_gpu_upload_prim(h, pin_in.ctypes.data_as(dptr)))
-        _lib.check(L.dragon_gpu_advance_steps(h, 1, None))
-        _lib.check(L.dragon_gpu_download_prim(h, pin_out.ctypes.data_as(dptr)))
-    e1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
+    e2e_serial_ms = e2e_run(G, [G], dev, e2e_steps, barrier)
+    e2e_grids = [G]
+    for _ in range(E2E_INFLIGHT - 1):
+        Gx = dg.Grid2D(N, N, dx, dy, ghosts=2, config=cfg)
+        Gx.w[...] = w0
+        Gx.boundary = dg.Periodic()
+        Gx.advance_steps(1)
+        e2e_grids.append(Gx)
+    e2e_ms = e2e_run(G, e2e_grids, dev, e2e_steps, barrier)
+    for Gx in e2e_grids[1:]:
+        Gx.close()
     if ws > 1:
-        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        t = torch.tensor([e2e_ms, e2e_serial_ms], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = t.item()
-    e2e_value = ws * N * N * e2e_steps / (e2e_ms / 1e3)
-    bytes_step = pin_in.nbytes
+        e2e_ms, e2e_serial_ms = t[0].item(), t[1].item()
+    e2e_value = ws * N * N * e2e_steps * len(e2e_grids) / (e2e_ms / 1e3)
+    e2e_serial_value = ws * N * N * e2e_steps / (e2e_serial_ms / 1e3)
+    bytes_step = G.w.nbytes
 
     if rank == 0:
         peak, peak_kind = measured_peaks()
@@ -517,7 +569,8 @@ def run_gpu(args):
                        "precision": "mixed" if args.mixed else "fp64", "l2": "flushed before every timed step",
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
             "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": bytes_step,
-                    "d2h_bytes_per_step": bytes_step, "steps": e2e_steps},
+                    "d2h_bytes_per_step": bytes_step, "steps": e2e_steps * len(e2e_grids),
+                    "grids_in_flight": len(e2e_grids), "one_grid_value": e2e_serial_value},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                          "kernel": "k_step2d_hydro", "kernel_ms_avg": k_avg_ms,
