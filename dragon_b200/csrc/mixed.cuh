@@ -134,4 +134,157 @@ __device__ __forceinline__ bool face_flux_mixed(Prim<float> L, Prim<float> R, fl
     return ok;
 }
 
+// ---------------------------------------------------------------------------
+// Pressure offset (hydro). The FP32 rounding of an absolute pressure p enters
+// the normal-momentum flux rho u^2 + p at |p| * 2^-24, which is large next to
+// a small transverse velocity's momentum. A tile therefore carries every FP32
+// pressure as an offset dp = p - ref from a tile-wide FP64 reference (the
+// smallest pressure the tile loads, so |dp| <= |p|), and the normal-momentum
+// fluxes it computes are rho u^2 + dp: the reference is the same for both faces
+// of every cell the tile updates and cancels exactly in the FP64 flux
+// differences. Wave speeds, energies and the physicality checks use the
+// absolute pressure ref + dp.
+
+// Absolute FP32 view of an offset state.
+__device__ __forceinline__ Prim<float> abs_p(Prim<float> w, float ref_f) {
+    w.p = ref_f + w.p;
+    return w;
+}
+
+// FP64 energy of an offset state.
+__device__ __forceinline__ double energy64_off(const Prim<float>& w, double ref) {
+    Prim<double> d = cvt<double>(w);
+    d.p = ref + d.p;
+    return energy<false>(d);
+}
+
+// Offset primitive state from FP32 momenta / density and an FP64 total energy;
+// *phys: the state is finite with positive density and FP64 pressure.
+__device__ __forceinline__ Prim<float> prim_from_off(const Cons<float>& u, double E64, double ref, bool* phys) {
+    Prim<float> w;
+    w.rho = u.rho;
+    w.vx = u.mx / u.rho;
+    w.vy = u.my / u.rho;
+    w.vz = u.mz / u.rho;
+    const double rho = u.rho, mx = u.mx, my = u.my, mz = u.mz;
+    const double p = kGm1 * (E64 - (mx * mx + my * my + mz * mz) / (2.0 * rho));
+    w.p = (float)(p - ref);
+    w.Bx = w.By = w.Bz = 0.f;
+    if (phys)
+        *phys = sfinite(w.rho) && sfinite(w.vx) && sfinite(w.vy) && sfinite(w.vz) && sfinite(p) && w.rho > 0.f &&
+                p > 0.0;
+    return w;
+}
+
+// muscl_mixed<false> on offset states: slopes and faces of dp, the predictor's
+// normal-momentum flux difference on dp, energies in FP64 on ref + dp.
+__device__ __forceinline__ bool muscl_off(int lim, const Prim<float>& wL, Prim<float>& outL, const Prim<float>& wC,
+                                          Prim<float>& outR, const Prim<float>& wR, float dt_dL, double ref,
+                                          float ref_f) {
+    Prim<float> dW, L, R;
+    dW.rho = limit1(lim, wC.rho - wL.rho, wR.rho - wC.rho);
+    dW.vx = limit1(lim, wC.vx - wL.vx, wR.vx - wC.vx);
+    dW.vy = limit1(lim, wC.vy - wL.vy, wR.vy - wC.vy);
+    dW.vz = limit1(lim, wC.vz - wL.vz, wR.vz - wC.vz);
+    dW.p = limit1(lim, wC.p - wL.p, wR.p - wC.p);
+    L.rho = wC.rho - 0.5f * dW.rho;  R.rho = wC.rho + 0.5f * dW.rho;
+    L.vx = wC.vx - 0.5f * dW.vx;     R.vx = wC.vx + 0.5f * dW.vx;
+    L.vy = wC.vy - 0.5f * dW.vy;     R.vy = wC.vy + 0.5f * dW.vy;
+    L.vz = wC.vz - 0.5f * dW.vz;     R.vz = wC.vz + 0.5f * dW.vz;
+    L.p = wC.p - 0.5f * dW.p;        R.p = wC.p + 0.5f * dW.p;
+    L.Bx = L.By = L.Bz = R.Bx = R.By = R.Bz = 0.f;
+    const Prim<float> La = abs_p(L, ref_f), Ra = abs_p(R, ref_f);
+    const Cons<float> UL = to_cons<false>(La), UR = to_cons<false>(Ra);
+    const float h = 0.5f * dt_dL;
+    Cons<float> corr = c_mul<false>(c_sub<false>(cons_flux<false>(UR, Ra.vx, Ra.vy, Ra.vz),
+                                                 cons_flux<false>(UL, La.vx, La.vy, La.vz)), h);
+    corr.mx = ((UR.mx * Ra.vx + R.p) - (UL.mx * La.vx + L.p)) * h;
+    bool okL, okR;
+    outL = prim_from_off(c_sub<false>(UL, corr), energy64_off(L, ref) - (double)corr.E, ref, &okL);
+    outR = prim_from_off(c_sub<false>(UR, corr), energy64_off(R, ref) - (double)corr.E, ref, &okR);
+    if (okL && okR) return true;
+    outL = wC;
+    outR = wC;
+    return false;
+}
+
+// correct_mixed<false> on an offset state.
+__device__ __forceinline__ Prim<float> correct_off(const Prim<float>& s, const Cons<float>& tr, double ref, float ref_f) {
+    return prim_from_off(c_sub<false>(to_cons<false>(abs_p(s, ref_f)), tr), energy64_off(s, ref) - (double)tr.E, ref,
+                         nullptr);
+}
+
+// Riemann::HLLC (HLL.cpp:103-132) in FP32 on offset states: wave speeds and the
+// star energy from the absolute pressures, the normal-momentum flux on dp
+// (F.mx is the flux minus ref).
+__device__ __forceinline__ Cons<float> hllc_off(const Prim<float>& L, const Prim<float>& Rt, float ref_f) {
+    const Prim<float> La = abs_p(L, ref_f), Ra = abs_p(Rt, ref_f);
+    const Prim<float> M = roe_avg<false>(La, Ra);
+    const float aL = sound_speed(La), aR = sound_speed(Ra), aM = sound_speed(M);
+    const float sl = smin(La.vx - aL, M.vx - aM);
+    const float sr = smax(Ra.vx + aR, M.vx + aM);
+    if (sl >= 0.f) {
+        Cons<float> F = prim_flux<false>(La);
+        F.mx = (La.rho * La.vx) * La.vx + L.p;
+        return F;
+    }
+    if (sr <= 0.f) {
+        Cons<float> F = prim_flux<false>(Ra);
+        F.mx = (Ra.rho * Ra.vx) * Ra.vx + Rt.p;
+        return F;
+    }
+    const float _pr = Rt.p + Ra.rho * Ra.vx * (Ra.vx - sr), _pl = L.p + La.rho * La.vx * (La.vx - sl);
+    const float sc = (_pr - _pl) / (Ra.rho * (Ra.vx - sr) - La.rho * (La.vx - sl));
+    const bool left = sc > 0.f;
+    const Prim<float>& X = left ? La : Ra;
+    const float dpx = left ? L.p : Rt.p;
+    const float sx = left ? sl : sr;
+    const Cons<float> UX = to_cons<false>(X);
+    Cons<float> U = c_div<false>(c_mul<false>(UX, sx - X.vx), sx - sc);
+    U.mx = U.rho * sc;
+    U.E += U.rho * (sc - X.vx) * (sc + X.p / (X.rho * (sx - X.vx)));
+    Cons<float> F = c_add<false>(cons_flux<false>(UX, X.vx, X.vy, X.vz), c_mul<false>(c_sub<false>(U, UX), sx));
+    F.mx = (UX.mx * X.vx + dpx) + (U.mx - UX.mx) * sx;
+    return F;
+}
+
+// face_flux_mixed<false, SOLVER, AX> on offset states. With HLLC the normal
+// momentum flux comes back minus ref (ref_f / ref: the tile's reference); the
+// other solvers run on the absolute FP32 states, which the caller pairs with a
+// zero reference.
+template <int SOLVER, int AX>
+__device__ __forceinline__ bool face_flux_off(Prim<float> L, Prim<float> R, float dt_dL, ExactOpts eo, Cons<float>& F,
+                                              FaceStats* st, double ref, float ref_f) {
+    if constexpr (SOLVER != RS_HLLC) {
+        return face_flux_mixed<false, SOLVER, AX>(abs_p(L, ref_f), abs_p(R, ref_f), dt_dL, eo, F, st);
+    } else {
+        swap_axis<AX>(L);
+        swap_axis<AX>(R);
+        bool ok = true;
+        F = hllc_off(L, R, ref_f);
+        if (dt_dL > 0.f) {
+            const Prim<float> La = abs_p(L, ref_f), Ra = abs_p(R, ref_f);
+            Cons<float> Ft = F;
+            Ft.mx += ref_f;
+            const Cons<float> UL = to_cons<false>(La), UR = to_cons<false>(Ra);
+            if (!(is_physical<false>(c_sub<false>(UL, c_mul<false>(Ft, dt_dL))) &&
+                  is_physical<false>(c_add<false>(UR, c_mul<false>(Ft, dt_dL))))) {
+                if (st) st->pivot_exact++;
+                Prim<double> Ld = cvt<double>(L), Rd = cvt<double>(R);
+                Ld.p = ref + Ld.p;
+                Rd.p = ref + Rd.p;
+                const Cons<double> Fd = exact_flux_default(Ld, Rd, eo, st);
+                const double h = dt_dL;
+                const Cons<double> ULd = to_cons<false>(Ld), URd = to_cons<false>(Rd);
+                ok = is_physical<false>(c_sub<false>(ULd, c_mul<false>(Fd, h))) &&
+                     is_physical<false>(c_add<false>(URd, c_mul<false>(Fd, h)));
+                F = cvt<float>(Fd);
+                F.mx = (float)(Fd.mx - ref);
+            }
+        }
+        swap_axis<AX>(F);
+        return ok;
+    }
+}
+
 }  // namespace dgpu

@@ -5,7 +5,10 @@
 // the tile data and the Riemann/MUSCL arithmetic in FP32 and, per the mixed
 // design, FP64 kept for: the state in HBM, every pressure recovery from a
 // conservative state (mixed.cuh), and the conservative flux-difference
-// accumulation into U. This translation unit is compiled with FMA contraction
+// accumulation into U. With HLLC the tile holds its pressures as offsets from
+// the smallest FP64 pressure it loads (mixed.cuh, pressure offset), so the
+// normal-momentum fluxes do not round the absolute pressure.
+// This translation unit is compiled with FMA contraction
 // and fast single-precision division / square root (--fmad=true
 // -prec-div=false -prec-sqrt=false -ftz=true); none of these flags changes
 // double-precision arithmetic.
@@ -46,6 +49,24 @@ __device__ __forceinline__ void hsm_put(SmemMixed<TI, TJ>& S, int k, int a, int 
     S.hs[k][4][a][b] = r.vz;
 }
 
+// Block-wide minimum of a per-thread value; every thread gets it. scratch: 32 doubles.
+__device__ __forceinline__ double block_min(double v, double* scratch) {
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) scratch[warp] = v;
+    __syncthreads();
+    const int nw = (blockDim.x + 31) >> 5;
+    v = (threadIdx.x < nw) ? scratch[threadIdx.x] : INFINITY;
+    if (warp == 0)
+        for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (threadIdx.x == 0) scratch[0] = v;
+    __syncthreads();
+    v = scratch[0];
+    __syncthreads();
+    return v;
+}
+
 // Three CTAs per SM (80 registers, 72.7 KB shared memory each): measured 14 %
 // faster than two CTAs at 110 registers on a 2048^2 shear layer, same results.
 template <int SOLVER, int TI, int TJ, int NT>
@@ -68,6 +89,19 @@ k_step2d_hydro_mixed(Geo G, const double* __restrict__ win, double* __restrict__
     if (threadIdx.x < 6) S.stat[threadIdx.x] = 0;
 
     constexpr int WI = TI + 4, WJ = TJ + 4;
+    // pressure reference of the tile (mixed.cuh, pressure offset): the smallest
+    // pressure it loads, with HLLC; zero (absolute pressures) otherwise
+    double pref = 0.0;
+    if constexpr (SOLVER == RS_HLLC) {
+        double pmin = INFINITY;
+        for (int t = threadIdx.x; t < WI * WJ; t += NT) {
+            const int i = i0 - 2 + t / WJ, j = j0 - 2 + t % WJ;
+            if (i >= -g && i < nx + g && j >= -g && j < ny + g) pmin = fmin(pmin, win[PL + gidx2(G, i, j)]);
+        }
+        pref = block_min(pmin, S.red);
+        if (!(pref > 0.0 && pref < INFINITY)) pref = 0.0;
+    }
+    const float pref_f = (float)pref;
     for (int t = threadIdx.x; t < WI * WJ; t += NT) {
         const int a = t / WJ, b = t % WJ;
         const int i = i0 - 2 + a, j = j0 - 2 + b;
@@ -75,6 +109,7 @@ k_step2d_hydro_mixed(Geo G, const double* __restrict__ win, double* __restrict__
             const long long m = gidx2(G, i, j);
 #pragma unroll
             for (int f = 0; f < 5; f++) S.u.w[f][a][b] = (float)win[f * PL + m];
+            S.u.w[1][a][b] = (float)(win[PL + m] - pref);
         }
     }
     __syncthreads();
@@ -90,12 +125,12 @@ k_step2d_hydro_mixed(Geo G, const double* __restrict__ win, double* __restrict__
         };
         const Prim<float> wc = W(a + 1, b + 1);
         Prim<float> oL, oR;
-        first_order += !muscl_mixed<false>(sa.limiter, W(a, b + 1), oL, wc, oR, W(a + 2, b + 1), fdx, 0.f, 0.f, 0.f);
+        first_order += !muscl_off(sa.limiter, W(a, b + 1), oL, wc, oR, W(a + 2, b + 1), fdx, pref, pref_f);
         hsm_put(S, HS_XL, a, b, oL);
         hsm_put(S, HS_XR, a, b, oR);
         Prim<float> yl = W(a + 1, b), yc = wc, yr = W(a + 1, b + 2);
         swap_xy(yl); swap_xy(yc); swap_xy(yr);
-        first_order += !muscl_mixed<false>(sa.limiter, yl, oL, yc, oR, yr, fdy, 0.f, 0.f, 0.f);
+        first_order += !muscl_off(sa.limiter, yl, oL, yc, oR, yr, fdy, pref, pref_f);
         swap_xy(oL); swap_xy(oR);
         hsm_put(S, HS_YL, a, b, oL);
         hsm_put(S, HS_YR, a, b, oR);
@@ -109,7 +144,8 @@ k_step2d_hydro_mixed(Geo G, const double* __restrict__ win, double* __restrict__
             const int a = t / (TJ + 2), b = t % (TJ + 2);
             const int i = i0 + a, j = j0 - 1 + b;
             if (!(i <= nx && j >= -1 && j <= ny)) continue;
-            if (!face_flux_mixed<false, SOLVER, 0>(hsm_get(S, HS_XR, a, b), hsm_get(S, HS_XL, a + 1, b), fdx, eo, F, &st))
+            if (!face_flux_off<SOLVER, 0>(hsm_get(S, HS_XR, a, b), hsm_get(S, HS_XL, a + 1, b), fdx, eo, F, &st, pref,
+                                          pref_f))
                 record_error(ctl, ST_PRELIM_FLUX, (long long)(i + g) * (ny + 2 * g) + (j + g));
             S.u.f.fx[0][a][b] = F.rho; S.u.f.fx[1][a][b] = F.E; S.u.f.fx[2][a][b] = F.mx;
             S.u.f.fx[3][a][b] = F.my; S.u.f.fx[4][a][b] = F.mz;
@@ -118,7 +154,8 @@ k_step2d_hydro_mixed(Geo G, const double* __restrict__ win, double* __restrict__
             const int a = q / (TJ + 1), b = q % (TJ + 1);
             const int i = i0 - 1 + a, j = j0 + b;
             if (!(i >= -1 && i <= nx && j <= ny)) continue;
-            if (!face_flux_mixed<false, SOLVER, 1>(hsm_get(S, HS_YR, a, b), hsm_get(S, HS_YL, a, b + 1), fdy, eo, F, &st))
+            if (!face_flux_off<SOLVER, 1>(hsm_get(S, HS_YR, a, b), hsm_get(S, HS_YL, a, b + 1), fdy, eo, F, &st, pref,
+                                          pref_f))
                 record_error(ctl, ST_PRELIM_FLUX, (long long)(i + g) * (ny + 2 * g) + (j + g));
             S.u.f.fy[0][a][b] = F.rho; S.u.f.fy[1][a][b] = F.E; S.u.f.fy[2][a][b] = F.mx;
             S.u.f.fy[3][a][b] = F.my; S.u.f.fy[4][a][b] = F.mz;
@@ -139,8 +176,8 @@ k_step2d_hydro_mixed(Geo G, const double* __restrict__ win, double* __restrict__
             tr.my = (S.u.f.fy[3][a][b] - S.u.f.fy[3][a][b - 1]) * hdy;
             tr.mz = (S.u.f.fy[4][a][b] - S.u.f.fy[4][a][b - 1]) * hdy;
             tr.Bx = tr.By = tr.Bz = 0.f;
-            hsm_put(S, HS_XL, a, b, correct_mixed<false>(hsm_get(S, HS_XL, a, b), tr));
-            hsm_put(S, HS_XR, a, b, correct_mixed<false>(hsm_get(S, HS_XR, a, b), tr));
+            hsm_put(S, HS_XL, a, b, correct_off(hsm_get(S, HS_XL, a, b), tr, pref, pref_f));
+            hsm_put(S, HS_XR, a, b, correct_off(hsm_get(S, HS_XR, a, b), tr, pref, pref_f));
         } else {
             const int q = t - NCX;
             const int a = q / HJ + 1, b = q % HJ;
@@ -153,8 +190,8 @@ k_step2d_hydro_mixed(Geo G, const double* __restrict__ win, double* __restrict__
             tr.my = (S.u.f.fx[3][a][b] - S.u.f.fx[3][a - 1][b]) * hdx;
             tr.mz = (S.u.f.fx[4][a][b] - S.u.f.fx[4][a - 1][b]) * hdx;
             tr.Bx = tr.By = tr.Bz = 0.f;
-            hsm_put(S, HS_YL, a, b, correct_mixed<false>(hsm_get(S, HS_YL, a, b), tr));
-            hsm_put(S, HS_YR, a, b, correct_mixed<false>(hsm_get(S, HS_YR, a, b), tr));
+            hsm_put(S, HS_YL, a, b, correct_off(hsm_get(S, HS_YL, a, b), tr, pref, pref_f));
+            hsm_put(S, HS_YR, a, b, correct_off(hsm_get(S, HS_YR, a, b), tr, pref, pref_f));
         }
     }
     __syncthreads();
@@ -166,8 +203,8 @@ k_step2d_hydro_mixed(Geo G, const double* __restrict__ win, double* __restrict__
             const int a = t / TJ, b = t % TJ;
             const int i = i0 + a, j = j0 + b;
             if (!(i <= nx && j < ny)) continue;
-            if (!face_flux_mixed<false, SOLVER, 0>(hsm_get(S, HS_XR, a, b + 1), hsm_get(S, HS_XL, a + 1, b + 1), fdx, eo, F,
-                                                   &st))
+            if (!face_flux_off<SOLVER, 0>(hsm_get(S, HS_XR, a, b + 1), hsm_get(S, HS_XL, a + 1, b + 1), fdx, eo, F, &st,
+                                          pref, pref_f))
                 record_error(ctl, ST_FINAL_FLUX, (long long)(i + g) * (ny + 2 * g) + (j + g));
             S.u.f.fx[0][a][b + 1] = F.rho; S.u.f.fx[1][a][b + 1] = F.E; S.u.f.fx[2][a][b + 1] = F.mx;
             S.u.f.fx[3][a][b + 1] = F.my; S.u.f.fx[4][a][b + 1] = F.mz;
@@ -176,8 +213,8 @@ k_step2d_hydro_mixed(Geo G, const double* __restrict__ win, double* __restrict__
             const int a = q / (TJ + 1), b = q % (TJ + 1);
             const int i = i0 + a, j = j0 + b;
             if (!(i < nx && j <= ny)) continue;
-            if (!face_flux_mixed<false, SOLVER, 1>(hsm_get(S, HS_YR, a + 1, b), hsm_get(S, HS_YL, a + 1, b + 1), fdy, eo, F,
-                                                   &st))
+            if (!face_flux_off<SOLVER, 1>(hsm_get(S, HS_YR, a + 1, b), hsm_get(S, HS_YL, a + 1, b + 1), fdy, eo, F, &st,
+                                          pref, pref_f))
                 record_error(ctl, ST_FINAL_FLUX, (long long)(i + g) * (ny + 2 * g) + (j + g));
             S.u.f.fy[0][a + 1][b] = F.rho; S.u.f.fy[1][a + 1][b] = F.E; S.u.f.fy[2][a + 1][b] = F.mx;
             S.u.f.fy[3][a + 1][b] = F.my; S.u.f.fy[4][a + 1][b] = F.mz;

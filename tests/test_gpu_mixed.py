@@ -17,9 +17,13 @@ from dragon_b200 import problems  # noqa: E402
 TOL_MIXED = 1e-5
 # vy of the shear layer is the seeded perturbation itself (amplitude 0.01 against
 # |vx| = 0.5), so its L1 norm is ~100x smaller than the other fields' and the
-# same absolute FP32 rounding in the y-momentum flux (the absolute pressure
-# term) shows up ~100x larger relative to it. Held to its measured level.
+# same absolute FP32 rounding shows up ~100x larger relative to it. With HLLC the
+# tile carries pressures as offsets from an FP64 reference (mixed.cuh), which
+# takes the absolute-pressure rounding out of the normal-momentum fluxes and
+# halves vy's error; what is left comes from the FP32 mass and energy fluxes
+# through the pressure gradient. Held to the measured levels.
 TOL_MIXED_PERTURBATION = 5e-5
+TOL_MIXED_PERTURBATION_HLLC = 2e-5
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -53,7 +57,8 @@ def test_mixed_kh_l1_vs_fp64_oracle(riemann, limiter):
     g = 2
     l1 = problems.rel_l1(G.w[g:-g, g:-g], R.get_prim()[g:-g, g:-g])
     assert np.all(l1[[0, 1, 2, 4]] <= TOL_MIXED), l1      # rho, p, vx, vz
-    assert l1[3] <= TOL_MIXED_PERTURBATION, l1            # vy: the seeded perturbation
+    # vy: the seeded perturbation
+    assert l1[3] <= (TOL_MIXED_PERTURBATION_HLLC if riemann == dg.RIEMANN_HLLC else TOL_MIXED_PERTURBATION), l1
     assert np.any(G.w[g:-g, g:-g] != R.get_prim()[g:-g, g:-g])  # really the FP32 path
 
 
