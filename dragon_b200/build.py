@@ -57,9 +57,18 @@ def needs_build() -> bool:
     return any(os.path.getmtime(p) > t for p in _deps())
 
 
+def _host_stale() -> bool:
+    deps = [HOST_SRC, os.path.join(ROOT, "include", "dragon", "dragon.hpp"), os.path.join(ROOT, "include", "dragon_gpu.h"),
+            LIB]
+    return any(not os.path.exists(o) or any(os.path.getmtime(d) > os.path.getmtime(o) for d in deps)
+               for o in HOST_LIBS.values())
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     """Compiles dragon_b200/libdragon_gpu.so with nvcc (cross-compiles without a GPU)."""
     if not force and not needs_build():
+        if _host_stale():
+            build_host(verbose=verbose)
         return LIB
     nvcc = os.environ.get("NVCC", "nvcc")
     os.makedirs(OBJ, exist_ok=True)
@@ -80,7 +89,31 @@ def build(force: bool = False, verbose: bool = False) -> str:
         objs = list(ex.map(compile_one, _sources()))
     subprocess.run([nvcc, *ARCH, "-shared", "-o", LIB + ".tmp", *objs], check=True)
     os.replace(LIB + ".tmp", LIB)
+    build_host(force=True, verbose=verbose)
     return LIB
+
+
+HOST_SRC = os.path.join(HERE, "host", "dragon_host.cpp")
+HOST_LIBS = {"": os.path.join(HERE, "libdragon_host.so"), "-DMHD": os.path.join(HERE, "libdragon_host_mhd.so")}
+
+
+def build_host(force: bool = False, verbose: bool = False) -> None:
+    """Compiles the C++23 host layer (include/dragon/dragon.hpp) over the C ABI:
+    libdragon_host.so (hydro) and libdragon_host_mhd.so (built with MHD), both
+    linked against libdragon_gpu.so in the same directory."""
+    cxx = os.environ.get("CXX", "g++")
+    deps = [HOST_SRC, os.path.join(ROOT, "include", "dragon", "dragon.hpp"), os.path.join(ROOT, "include", "dragon_gpu.h"),
+            LIB]
+    for flag, out in HOST_LIBS.items():
+        if not force and os.path.exists(out) and all(os.path.getmtime(d) <= os.path.getmtime(out) for d in deps):
+            continue
+        cmd = [cxx, "-std=c++23", "-O2", "-fPIC", "-Wall", "-Wextra", "-shared", *([flag] if flag else []),
+               "-I" + os.path.join(ROOT, "include"), HOST_SRC, "-L" + HERE, "-ldragon_gpu", "-Wl,-rpath,$ORIGIN",
+               "-o", out + ".tmp"]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+        os.replace(out + ".tmp", out)
 
 
 if __name__ == "__main__":
