@@ -327,8 +327,9 @@ def mhd_report(n=1024, steps=20, warmup=3):
                 a = torch.cuda.Event(enable_timing=True)
                 b = torch.cuda.Event(enable_timing=True)
                 a.record(stream)
-            G.advance_steps(1)
+            G.advance_steps_async(1)
             b.record(stream)
+            G.advance_wait()
             ev.append((a, b))
         torch.cuda.synchronize()
         ms = sum(a.elapsed_time(b) for a, b in ev) / steps
@@ -464,9 +465,11 @@ def run_gpu(args):
                 e0 = torch.cuda.Event(enable_timing=True)
                 e1 = torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
+            # enqueue the step, mark its end on the stream, then read its outcome
             st = _lib.AdvanceStats()
-            _lib.check(L.dragon_gpu_advance_steps(h, 1, __import__("ctypes").byref(st)))
+            _lib.check(L.dragon_gpu_advance_steps_async(h, 1))
             e1.record(stream)
+            _lib.check(L.dragon_gpu_advance_wait(h, __import__("ctypes").byref(st)))
             step_ms.append((e0, e1))
         torch.cuda.synchronize()
         t_wall = time.perf_counter() - t_wall
@@ -508,8 +511,9 @@ def run_gpu(args):
                 a_ = torch.cuda.Event(enable_timing=True)
                 b_ = torch.cuda.Event(enable_timing=True)
                 a_.record(stream_m)
-            _lib.check(Lm.dragon_gpu_advance_steps(hm, 1, None))
+            _lib.check(Lm.dragon_gpu_advance_steps_async(hm, 1))
             b_.record(stream_m)
+            _lib.check(Lm.dragon_gpu_advance_wait(hm, None))
             ev.append((a_, b_))
         torch.cuda.synchronize()
         barrier()

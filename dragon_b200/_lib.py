@@ -133,6 +133,8 @@ SIGNATURES = {
     "dragon_gpu_split_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(StepStatus)]),
     "dragon_gpu_advance_split": (
         ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.POINTER(AdvanceStats)]),
+    "dragon_gpu_advance_steps_async": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "dragon_gpu_advance_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "dragon_gpu_halo_size": (
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]),

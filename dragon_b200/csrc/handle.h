@@ -16,6 +16,17 @@ namespace dgpu {
 struct MlpNet;
 }
 
+// The device advance loop between its first batch and its completion
+// (dragon_gpu_advance_steps_async / dragon_gpu_advance_wait).
+struct AdvanceState {
+    bool pending = false;
+    int cur0 = 0;         // buffer step 0 reads
+    long long k = 0;      // advance-local index of the next step to enqueue
+    int retries = 0;
+    double remaining = 0;
+    int max_steps = 0;
+};
+
 struct dragon_grid {
     int dim = 0;
     int n[3] = {1, 1, 1};
@@ -67,6 +78,7 @@ struct dragon_grid {
     int nlog_stride = 1;
     dgpu::MlpNet* mlp_dev = nullptr;
     dragon_newton_stats ntot{};
+    AdvanceState adv{};
 };
 
 namespace dgpu_rt {

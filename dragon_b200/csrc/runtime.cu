@@ -441,31 +441,60 @@ const char* stage_name(int s) {
 }
 
 // Shared advance loop. remaining/max_steps select advance(interval) or a step count.
-int advance_impl(dragon_grid* h, double remaining, int max_steps, int check_cfl, dragon_advance_stats* st) {
-    if (st) std::memset(st, 0, sizeof(*st));
+// One batch of up to kBatch steps of the advance in flight: for step k the
+// prologue (bookkeeping, ghost fill, CFL dt) reads buffer cur0 ^ (k & 1) and
+// the step writes the other buffer.
+static int enqueue_batch(dragon_grid* h) {
+    AdvanceState& A = h->adv;
+    int nb = kBatch;
+    if (A.max_steps > 0) nb = (int)std::min<long long>(kBatch, (long long)A.max_steps + 1 - A.k);
+    if (nb < 1) nb = 1;
+    int rc;
+    for (int b = 0; b < nb; b++) {
+        const int c = A.cur0 ^ (int)((A.k + b) & 1);
+        // with a step budget, the prologue after the last step only accounts it
+        // (bookkeeping alone: no ghost fill, no CFL time)
+        const bool account_only = A.max_steps > 0 && A.k + b >= A.max_steps;
+        if ((rc = launch_prologue(h, c, 1, account_only ? 0 : 1, account_only ? 0 : 1, c, c ^ 1))) return rc;
+        if (account_only) continue;
+        if ((rc = launch_any_step(h, c, A.k + b))) return rc;
+    }
+    A.k += nb;
+    return 0;
+}
+
+int advance_begin(dragon_grid* h, double remaining, int max_steps, int check_cfl) {
+    if (h->adv.pending) return fail(DRAGON_GPU_EINVAL, "an asynchronous advance is in flight: call dragon_gpu_advance_wait");
     h->can_rollback = false;
-    const int cur0 = h->cur;
+    AdvanceState& A = h->adv;
+    A = AdvanceState{};
+    A.cur0 = h->cur;
+    A.remaining = remaining;
+    A.max_steps = max_steps;
     reset_ctl(h, remaining, max_steps, check_cfl);
     int rc = push_ctl(h);
     if (rc) return rc;
     if (!h->imax_valid) {
-        if ((rc = zero_slot(h, cur0))) return rc;
-        if ((rc = launch_interior_cfl(h, cur0, cur0))) return rc;
+        if ((rc = zero_slot(h, A.cur0))) return rc;
+        if ((rc = launch_interior_cfl(h, A.cur0, A.cur0))) return rc;
     }
-    long long k = 0;  // advance-local index of the next step to launch
-    int retries = 0;
+    A.pending = true;
+    rc = enqueue_batch(h);
+    if (rc) A.pending = false;
+    return rc;
+}
+
+// Reads the control block after each batch: on a failed step halves t1 and
+// retries it on the same ghosts (CFL.cpp:198-208), otherwise enqueues the next
+// batch until the advance is done.
+int advance_finish(dragon_grid* h, dragon_advance_stats* st) {
+    if (st) std::memset(st, 0, sizeof(*st));
+    AdvanceState& A = h->adv;
+    if (!A.pending) return fail(DRAGON_GPU_EINVAL, "no advance in flight");
+    A.pending = false;
+    const int cur0 = A.cur0;
+    int rc;
     for (;;) {
-        int nb = kBatch;
-        if (max_steps > 0) nb = (int)std::min<long long>(kBatch, (long long)max_steps + 1 - k);
-        if (nb < 1) nb = 1;
-        for (int b = 0; b < nb; b++) {
-            const int c = cur0 ^ (int)((k + b) & 1);
-            if ((rc = launch_prologue(h, c, 1, 1, 1, c, c ^ 1))) return rc;
-            // with a step budget, the prologue after the last step only accounts it
-            if (max_steps > 0 && k + b >= max_steps) continue;
-            if ((rc = launch_any_step(h, c, k + b))) return rc;
-        }
-        k += nb;
         if ((rc = pull_ctl(h))) return rc;
         StepCtl& C = *h->hctl;
         if (C.err) {
@@ -484,10 +513,10 @@ int advance_impl(dragon_grid* h, double remaining, int max_steps, int check_cfl,
             // CFL.cpp:198-208: halve t1 and retry the same step on the same ghosts.
             double t1 = C.t1;
             for (;;) {
-                retries++;
+                A.retries++;
                 t1 *= 0.5;
                 if (t1 < h->cfg.timestep_tol) {
-                    if (st) { st->retries = retries; st->failure.code = DRAGON_GPU_EDT; }
+                    if (st) { st->retries = A.retries; st->failure.code = DRAGON_GPU_EDT; }
                     if (h->split_mode) h->sweep_step += ks;
                     return fail(DRAGON_GPU_EDT, std::string("Timestep has fallen below minimum after: ") + stage_name(stage));
                 }
@@ -503,9 +532,10 @@ int advance_impl(dragon_grid* h, double remaining, int max_steps, int check_cfl,
                 if (!C.err) break;
                 fill_stats(h, C, st);
             }
-            // success: the next prologue accounts the retried step
-            k = ks + 1;
-            // keep cur0 parity consistent: step k reads buffer cur0 ^ (k & 1) == c ^ 1
+            // success: the next prologue accounts the retried step; step k reads
+            // buffer cur0 ^ (k & 1) == c ^ 1
+            A.k = ks + 1;
+            if ((rc = enqueue_batch(h))) return rc;
             continue;
         }
         if (C.done) {
@@ -515,13 +545,21 @@ int advance_impl(dragon_grid* h, double remaining, int max_steps, int check_cfl,
             fill_stats(h, C, st);
             if (st) {
                 st->steps = C.steps_done;
-                st->retries = retries;
+                st->retries = A.retries;
                 st->last_dt = C.t1;
-                st->time_advanced = (remaining - C.remaining);
+                st->time_advanced = (A.remaining - C.remaining);
             }
             return 0;
         }
+        if ((rc = enqueue_batch(h))) return rc;
     }
+}
+
+int advance_impl(dragon_grid* h, double remaining, int max_steps, int check_cfl, dragon_advance_stats* st) {
+    if (st) std::memset(st, 0, sizeof(*st));
+    int rc = advance_begin(h, remaining, max_steps, check_cfl);
+    if (rc) return rc;
+    return advance_finish(h, st);
 }
 
 }  // namespace dgpu_rt
@@ -691,6 +729,7 @@ size_t dragon_gpu_faceB_count(const dragon_grid* h) {
 
 static int transfer(dragon_grid* h, bool up, bool faces, double* host) {
     if (!h || !host) return fail(DRAGON_GPU_EINVAL, "null argument");
+    if (h->adv.pending) return fail(DRAGON_GPU_EINVAL, "an asynchronous advance is in flight");
     if (faces && !(h->mhd && h->dim >= 2)) return fail(DRAGON_GPU_EINVAL, "grid has no face-centred B");
     const Geo& G = faces ? h->fg : h->cg;
     const int nf = faces ? 3 : h->nf;
@@ -720,6 +759,7 @@ int dragon_gpu_upload_faceB(dragon_grid* h, const double* host) { return transfe
 int dragon_gpu_download_faceB(dragon_grid* h, double* host) { return transfer(h, false, true, host); }
 
 int dragon_gpu_set_boundary(dragon_grid* h, const dragon_bc_desc* list, int n) {
+    if (h && h->adv.pending) return fail(DRAGON_GPU_EINVAL, "an asynchronous advance is in flight");
     if (!h || n < 0 || (n > 0 && !list)) return fail(DRAGON_GPU_EINVAL, "invalid boundary list");
     std::vector<BCEntry> v;
     // implicit Outflow over every face no entry covers (BoundaryList.hpp:97-104)
@@ -763,6 +803,7 @@ int dragon_gpu_set_boundary(dragon_grid* h, const dragon_bc_desc* list, int n) {
 }
 
 int dragon_gpu_apply_boundary(dragon_grid* h) {
+    if (h && h->adv.pending) return fail(DRAGON_GPU_EINVAL, "an asynchronous advance is in flight");
     if (!h) return fail(DRAGON_GPU_EINVAL, "null handle");
     reset_ctl(h, 0.0, 0, 0);
     int rc = push_ctl(h);
@@ -775,6 +816,7 @@ int dragon_gpu_apply_boundary(dragon_grid* h) {
 int dragon_gpu_boundary_entries(const dragon_grid* h) { return h ? h->nbc : 0; }
 
 int dragon_gpu_apply_boundary_range(dragon_grid* h, int first, int count) {
+    if (h && h->adv.pending) return fail(DRAGON_GPU_EINVAL, "an asynchronous advance is in flight");
     if (!h || first < 0 || count < 0 || first + count > h->nbc) return fail(DRAGON_GPU_EINVAL, "entry range out of bounds");
     if (count == 0) return 0;
     reset_ctl(h, 0.0, 0, 0);
@@ -786,6 +828,7 @@ int dragon_gpu_apply_boundary_range(dragon_grid* h, int first, int count) {
 }
 
 int dragon_gpu_cfl_time(dragon_grid* h, double* dt_out) {
+    if (h && h->adv.pending) return fail(DRAGON_GPU_EINVAL, "an asynchronous advance is in flight");
     if (!h || !dt_out) return fail(DRAGON_GPU_EINVAL, "null argument");
     reset_ctl(h, INFINITY, 0, 1);
     int rc = push_ctl(h);
@@ -800,6 +843,7 @@ int dragon_gpu_cfl_time(dragon_grid* h, double* dt_out) {
 }
 
 int dragon_gpu_unsplit_step(dragon_grid* h, double dt, dragon_step_status* st) {
+    if (h && h->adv.pending) return fail(DRAGON_GPU_EINVAL, "an asynchronous advance is in flight");
     if (!h) return fail(DRAGON_GPU_EINVAL, "null handle");
     if (st) std::memset(st, 0, sizeof(*st));
     reset_ctl(h, 0.0, 0, 0);
@@ -823,6 +867,7 @@ int dragon_gpu_unsplit_step(dragon_grid* h, double dt, dragon_step_status* st) {
 }
 
 int dragon_gpu_step_rollback(dragon_grid* h) {
+    if (h && h->adv.pending) return fail(DRAGON_GPU_EINVAL, "an asynchronous advance is in flight");
     if (!h) return fail(DRAGON_GPU_EINVAL, "null handle");
     if (!h->can_rollback) return fail(DRAGON_GPU_EINVAL, "no committed unsplit_step to undo");
     CK(cudaStreamSynchronize(h->stream));
@@ -906,11 +951,13 @@ static int halo_copy(dragon_grid* h, int axis, int first, int layers, int faces,
 
 int dragon_gpu_halo_pack(dragon_grid* h, int axis, int first, int layers, int faces, int corners, double* buf,
                          int buf_on_device) {
+    if (h && h->adv.pending) return fail(DRAGON_GPU_EINVAL, "an asynchronous advance is in flight");
     return halo_copy(h, axis, first, layers, faces, corners, buf, buf_on_device, true);
 }
 
 int dragon_gpu_halo_unpack(dragon_grid* h, int axis, int first, int layers, int faces, int corners, const double* buf,
                            int buf_on_device) {
+    if (h && h->adv.pending) return fail(DRAGON_GPU_EINVAL, "an asynchronous advance is in flight");
     return halo_copy(h, axis, first, layers, faces, corners, const_cast<double*>(buf), buf_on_device, false);
 }
 
@@ -925,6 +972,17 @@ int dragon_gpu_advance_steps(dragon_grid* h, int nsteps, dragon_advance_stats* s
     return advance_impl(h, INFINITY, nsteps, 1, st);
 }
 
+int dragon_gpu_advance_steps_async(dragon_grid* h, int nsteps) {
+    if (!h || nsteps < 1) return fail(DRAGON_GPU_EINVAL, "invalid argument");
+    if (h->adv.pending) return fail(DRAGON_GPU_EINVAL, "an advance is already in flight");
+    return advance_begin(h, INFINITY, nsteps, 1);
+}
+
+int dragon_gpu_advance_wait(dragon_grid* h, dragon_advance_stats* st) {
+    if (!h) return fail(DRAGON_GPU_EINVAL, "null handle");
+    return advance_finish(h, st);
+}
+
 static int split_unsupported(const dragon_grid* h) {
     if (h->mhd && h->dim >= 2) return fail(DRAGON_GPU_EUNSUPPORTED, "the Strang-split path is built for hydro grids");
     if (h->cfg.precision != 0) return fail(DRAGON_GPU_EUNSUPPORTED, "the Strang-split path runs in FP64");
@@ -932,6 +990,7 @@ static int split_unsupported(const dragon_grid* h) {
 }
 
 int dragon_gpu_split_step(dragon_grid* h, double dt, dragon_step_status* st) {
+    if (h && h->adv.pending) return fail(DRAGON_GPU_EINVAL, "an asynchronous advance is in flight");
     if (!h) return fail(DRAGON_GPU_EINVAL, "null handle");
     int rc = split_unsupported(h);
     if (rc) return rc;
@@ -994,6 +1053,7 @@ int dragon_gpu_profile_read(dragon_grid* h, double* ms_total, long long* launche
 }
 
 int dragon_gpu_initialize_B_fields(dragon_grid* h) {
+    if (h && h->adv.pending) return fail(DRAGON_GPU_EINVAL, "an asynchronous advance is in flight");
     if (!h) return fail(DRAGON_GPU_EINVAL, "null handle");
     if (!(h->mhd && h->dim >= 2)) return fail(DRAGON_GPU_EINVAL, "grid has no face-centred B");
     int rc = dragon_gpu_apply_boundary(h);

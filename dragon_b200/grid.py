@@ -352,6 +352,22 @@ class _GridBase:
         _lib.check(rc)
         return _result(st)
 
+    def advance_steps_async(self, nsteps: int) -> None:
+        """Enqueues nsteps CFL-limited steps on the grid's stream and returns
+        without waiting for the device; advance_wait() completes them (retries
+        included). The grid takes no other call in between."""
+        if self._boundary.has_custom():
+            raise RuntimeError("boundary lists with user elements advance from the host")
+        self._to_device()
+        _lib.check(self._lib.dragon_gpu_advance_steps_async(self._h, int(nsteps)))
+
+    def advance_wait(self) -> AdvanceResult:
+        st = _lib.AdvanceStats()
+        rc = self._lib.dragon_gpu_advance_wait(self._h, ctypes.byref(st))
+        self._device_ran()
+        _lib.check(rc)
+        return _result(st)
+
     def initialize_B_fields(self):
         """Grid::initialize_B_fields (B_fields.cpp:117-149)."""
         self._push_boundary()

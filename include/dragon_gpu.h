@@ -148,6 +148,12 @@ int dragon_gpu_unsplit_step(dragon_grid* g, double dt, dragon_step_status* st);
 int dragon_gpu_advance(dragon_grid* g, double interval, int check_cfl, dragon_advance_stats* st);
 /* advance by a fixed number of CFL-limited steps (the interval is unbounded). */
 int dragon_gpu_advance_steps(dragon_grid* g, int nsteps, dragon_advance_stats* st);
+/* dragon_gpu_advance_steps in two halves: _async enqueues the first batch of
+ * steps on the handle's stream and returns without waiting for the device;
+ * _wait reads the outcome, runs any retry and further batches, and fills st.
+ * Between the two the handle takes no other call. */
+int dragon_gpu_advance_steps_async(dragon_grid* g, int nsteps);
+int dragon_gpu_advance_wait(dragon_grid* g, dragon_advance_stats* st);
 /* Grid::split_step(dt) (Hydro/Godunov/Splitting.cpp:118-217): the Strang
  * sequence of one-dimensional Godunov sweeps, the order alternating with the
  * grid's sweep counter (2D: XYX / YXY; 3D: the six cyclic and anticyclic
