@@ -15,6 +15,9 @@ fused update). Metric: cell-updates/s (interior cells x steps / time).
              (one_grid_value: a single grid, nothing overlapped);
   roofline   the fused step kernel's algorithmic HBM bytes (80 B per cell
              update: 5 FP64 fields read + written) over its CUDA-event time;
+  roofline_fp64  the same kernel's executed FP64 operations per cell update
+             (ncu counters, profiles/step2d_hydro_kh.json) over its time, against
+             a cuBLAS DGEMM measured in the run: the bound that applies;
   cpu_baseline  the DRAGON reference itself (oracle/_ref, DistGrid2D with
              core_count = host threads) on a bounded number of full steps;
   mixed      the mixed FP32/FP64 path on the same workload, with its relative
@@ -108,6 +111,19 @@ def e2e_run(G0, grids, dev, steps, barrier):
     return max(start.elapsed_time(e) for e in ends)
 
 
+def roofline_fp64(k_avg_ms, dev):
+    """The fused FP64 step against FP64 throughput: it is bound by FP64 issue, not
+    by HBM, so this is the roofline that explains it."""
+    fpc = fp64_flops_per_cell()
+    if not fpc or not k_avg_ms:
+        return None
+    peak = fp64_peak_tflops(dev)
+    achieved = fpc * N * N / (k_avg_ms / 1e3) / 1e12
+    return {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "flops_per_cell": fpc, "kernel": "k_step2d_hydro",
+            "peak_source": "cuBLAS DGEMM 4096^3 measured in this run (no FP64 figure in MEASURED_PEAKS.json)"}
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -124,6 +140,39 @@ def traffic_from_profile():
             d = json.load(f)
         return d.get("dram_bytes_per_launch_full")
     return None
+
+
+def fp64_flops_per_cell():
+    """FP64 operations the fused step executes per cell update (ncu instruction
+    counters dadd + dmul + 2 dfma of one launch over its cells)."""
+    p = os.path.join(ROOT, "profiles", "step2d_hydro_kh.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f).get("fp64_flops_per_cell_update")
+    return None
+
+
+def fp64_peak_tflops(dev):
+    """FP64 throughput of a cuBLAS DGEMM (4096^3, best of 5, CUDA events) on this
+    GPU: the denominator of the FP64 compute roofline."""
+    import torch
+    n = 4096
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = float("inf")
+    for _ in range(5):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    return 2.0 * n ** 3 / (best / 1e3) / 1e12
 
 
 class ClockSampler:
@@ -579,6 +628,7 @@ def run_gpu(args):
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                          "kernel": "k_step2d_hydro", "kernel_ms_avg": k_avg_ms,
                          "bytes_per_cell": CELL_BYTES, "peak_source": peak_kind},
+            "roofline_fp64": roofline_fp64(k_avg_ms, dev),
             "gpu_launches": launches,
             "clocks": clocks,
             "wall_s_timed": t_wall,
