@@ -58,10 +58,10 @@ def needs_build() -> bool:
 
 
 def _host_stale() -> bool:
-    deps = [HOST_SRC, os.path.join(ROOT, "include", "dragon", "dragon.hpp"), os.path.join(ROOT, "include", "dragon_gpu.h"),
-            LIB]
-    return any(not os.path.exists(o) or any(os.path.getmtime(d) > os.path.getmtime(o) for d in deps)
-               for o in HOST_LIBS.values())
+    deps = [HOST_SRC, DIST_SRC, os.path.join(ROOT, "include", "dragon", "dragon.hpp"),
+            os.path.join(ROOT, "include", "dragon", "dist.hpp"), os.path.join(ROOT, "include", "dragon_gpu.h"), LIB]
+    outs = list(HOST_LIBS.values()) + [os.path.join(HERE, "libdragon_dist.so"), os.path.join(HERE, "libdragon_dist_mhd.so")]
+    return any(not os.path.exists(o) or any(os.path.getmtime(d) > os.path.getmtime(o) for d in deps) for o in outs)
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
@@ -94,6 +94,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
 
 
 HOST_SRC = os.path.join(HERE, "host", "dragon_host.cpp")
+DIST_SRC = os.path.join(HERE, "host", "dragon_dist.cpp")
+CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 HOST_LIBS = {"": os.path.join(HERE, "libdragon_host.so"), "-DMHD": os.path.join(HERE, "libdragon_host_mhd.so")}
 
 
@@ -110,6 +112,29 @@ def build_host(force: bool = False, verbose: bool = False) -> None:
         cmd = [cxx, "-std=c++23", "-O2", "-fPIC", "-Wall", "-Wextra", "-shared", *([flag] if flag else []),
                "-I" + os.path.join(ROOT, "include"), HOST_SRC, "-L" + HERE, "-ldragon_gpu", "-Wl,-rpath,$ORIGIN",
                "-o", out + ".tmp"]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+        os.replace(out + ".tmp", out)
+    build_dist(force=force, verbose=verbose)
+
+
+def build_dist(force: bool = False, verbose: bool = False) -> None:
+    """Compiles the C++ DistGrid (include/dragon/dist.hpp) over NCCL:
+    libdragon_dist.so and libdragon_dist_mhd.so, linked against the host layer
+    of the same physics, libdragon_gpu.so, libcudart and libnccl."""
+    cxx = os.environ.get("CXX", "g++")
+    deps = [DIST_SRC, os.path.join(ROOT, "include", "dragon", "dist.hpp"), os.path.join(ROOT, "include", "dragon", "dragon.hpp"),
+            LIB]
+    for flag, host_out in HOST_LIBS.items():
+        sfx = "_mhd" if flag else ""
+        out = os.path.join(HERE, f"libdragon_dist{sfx}.so")
+        if not force and os.path.exists(out) and all(os.path.getmtime(d) <= os.path.getmtime(out) for d in deps):
+            continue
+        cmd = [cxx, "-std=c++23", "-O2", "-fPIC", "-Wall", "-Wextra", "-shared", *([flag] if flag else []),
+               "-I" + os.path.join(ROOT, "include"), "-I" + os.path.join(CUDA_HOME, "include"), DIST_SRC,
+               "-L" + HERE, f"-ldragon_host{sfx}", "-ldragon_gpu", "-L" + os.path.join(CUDA_HOME, "lib64"), "-lcudart",
+               "-lnccl", "-Wl,-rpath,$ORIGIN", "-Wl,-rpath," + os.path.join(CUDA_HOME, "lib64"), "-o", out + ".tmp"]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.run(cmd, check=True)
