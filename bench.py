@@ -433,7 +433,7 @@ def batch_report(steps=500, one_by_one_steps=50):
     grids = make()
     b = batch.Batch(grids)
     t0 = time.perf_counter()
-    tune, _ = b.autotune(3)
+    tune, _ = b.autotune(6)
     tune_s = time.perf_counter() - t0
     b.advance_steps(3)
     torch.cuda.synchronize()
@@ -463,7 +463,7 @@ def batch_report(steps=500, one_by_one_steps=50):
             "work_items_per_step": st["work_items"], "graph_replays": st["graph_replays"],
             "retries": st["retries"], "spin_timeouts": st["spin_timeouts"],
             "tuning": {"tile_1d": tune.tile_1d, "ctas_per_sm": tune.ctas_per_sm, "order": tune.order,
-                       "graph_steps": tune.graph_steps}, "autotune_seconds": tune_s}
+                       "graph_steps": tune.graph_steps, "mhd_tiles": tune.mhd_tiles}, "autotune_seconds": tune_s}
 
 
 def run_gpu(args):

@@ -46,7 +46,9 @@ enum Kind : int { K1D = 0, KMHD2D = 1 };
 struct BatchInst {
     int kind;
     int last_phase;
-    int ntiles[kPhases];
+    int ntiles[kPhases];     // work items of each phase
+    int rtiles[kPhases];     // 32 x 8 tiles of each 2D MHD phase
+    int group;               // MHD tiles per work item
     int ntj[kPhases];        // MHD phases: tiles along j
     Geo G, FG;
     double* w[2];
@@ -68,9 +70,10 @@ struct Summary {
     int err, done, steps_done, cur;
 };
 
-// counters: [0] dependency waits that gave up (kept), [1] queue head,
-// [2 + kPhases * m + p] finished items of member m, phase p (both reset per step)
-constexpr int kCtrTimeouts = 0, kCtrHead = 1, kCtrDone = 2;
+// counters: [0] dependency waits that gave up and [1] members that have not
+// finished the advance (both kept across the launches of an advance), [2] queue
+// head, [3 + kPhases * m + p] finished items of member m, phase p (reset per step)
+constexpr int kCtrTimeouts = 0, kCtrActive = 1, kCtrHead = 2, kCtrDone = 3;
 
 int fail(int code, const std::string& msg) {
     dragon_gpu_set_error_message(msg.c_str());
@@ -99,13 +102,18 @@ __device__ __forceinline__ void wait_count(const unsigned* counter, unsigned tar
 }
 
 template <int S1D, int SMHD, int TS>
-__device__ __forceinline__ void run_item(const BatchInst& I, const WorkItem& wi, int cur) {
+__device__ __forceinline__ void run_item(const BatchInst& I, const WorkItem& wi, int cur, unsigned* active) {
     if (wi.phase == 0) {
+        __shared__ int s_was_done;
+        if (threadIdx.x == 0) s_was_done = ldv(&I.ctl->done);
         PrologueArgs pa = I.pa;
         pa.slot_in = cur;
         pa.slot_out = cur ^ 1;
         if (I.kind == K1D) prologue_body<false>(I.G, I.FG, I.w[cur], nullptr, I.bcs, I.ctl, pa);
         else prologue_body<true>(I.G, I.FG, I.w[cur], I.B[cur], I.bcs, I.ctl, pa);
+        __syncthreads();
+        // the member finished its steps in this prologue: one fewer to wait for
+        if (threadIdx.x == 0 && !s_was_done && ldv(&I.ctl->done)) atomicSub(active, 1u);
         return;
     }
     StepArgs sa = I.sa;
@@ -126,23 +134,31 @@ __device__ __forceinline__ void run_item(const BatchInst& I, const WorkItem& wi,
     }
     const Mhd2DArgs A{I.G, I.FG, I.w[cur], I.w[cur ^ 1], I.B[cur], I.B[cur ^ 1], I.S, I.ctl, sa};
     const int nbx = I.ntj[wi.phase];
-    const Tile2 T{wi.tile % nbx, wi.tile / nbx, (int)(threadIdx.x % kTileJ), (int)(threadIdx.x / kTileJ)};
-    switch (wi.phase) {
-        case 2: mhd2d_halfstates(A, T); break;
-        case 3: mhd2d_prelim<SMHD>(A, T); break;
-        case 4: mhd2d_e0(A, T); break;
-        case 5: mhd2d_half(A, T); break;
-        case 6: mhd2d_final_flux<SMHD>(A, T); break;
-        case 7: mhd2d_efinal(A, T); break;
-        default: mhd2d_update(A, T); break;
+    for (int k = 0; k < I.group; k++) {
+        const int tile = wi.tile * I.group + k;
+        if (tile >= I.rtiles[wi.phase]) break;  // uniform across the CTA
+        if (k) __syncthreads();                 // the previous tile's shared words are read
+        const Tile2 T{tile % nbx, tile / nbx, (int)(threadIdx.x % kTileJ), (int)(threadIdx.x / kTileJ)};
+        switch (wi.phase) {
+            case 2: mhd2d_halfstates(A, T); break;
+            case 3: mhd2d_prelim<SMHD>(A, T); break;
+            case 4: mhd2d_e0(A, T); break;
+            case 5: mhd2d_half(A, T); break;
+            case 6: mhd2d_final_flux<SMHD>(A, T); break;
+            case 7: mhd2d_efinal(A, T); break;
+            default: mhd2d_update(A, T); break;
+        }
     }
 }
 
 template <int S1D, int SMHD, int TS>
-__global__ void __launch_bounds__(kThreads) k_batch_step(const BatchInst* __restrict__ insts,
+__global__ void __launch_bounds__(kThreads, 2) k_batch_step(const BatchInst* __restrict__ insts,
                                                          const WorkItem* __restrict__ items, int nitems,
                                                          unsigned* ctr) {
     __shared__ int s_item;
+    // every member has finished its steps (a launch after the last one a graph
+    // replay needs): nothing to take from the queue
+    if (*(const volatile unsigned*)&ctr[kCtrActive] == 0) return;
     for (;;) {
         __syncthreads();  // the previous item's users of shared memory are done
         if (threadIdx.x == 0) s_item = (int)atomicAdd(&ctr[kCtrHead], 1u);
@@ -152,11 +168,14 @@ __global__ void __launch_bounds__(kThreads) k_batch_step(const BatchInst* __rest
         const WorkItem wi = items[it];
         const BatchInst& I = insts[wi.inst];
         unsigned* done = ctr + kCtrDone + (size_t)kPhases * wi.inst;
-        if (wi.phase > 0 && threadIdx.x == 0)
+        // a member that has finished its steps (or failed this one) has nothing
+        // left to do in this launch: its items only count themselves, without
+        // waiting for the phase before them
+        if (wi.phase > 0 && threadIdx.x == 0 && !(ldv(&I.ctl->done) | ldv(&I.ctl->err)))
             wait_count(done + wi.phase - 1, (unsigned)I.ntiles[wi.phase - 1], &ctr[kCtrTimeouts]);
         __syncthreads();
         const int cur = ldv(&I.ctl->cur);
-        run_item<S1D, SMHD, TS>(I, wi, cur);
+        run_item<S1D, SMHD, TS>(I, wi, cur, &ctr[kCtrActive]);
         __syncthreads();
         if (threadIdx.x == 0) {
             __threadfence();
@@ -189,7 +208,7 @@ StepKernel pick_kernel(int s1d, int tile) {
 
 struct dragon_batch {
     std::vector<dragon_grid*> members;
-    dragon_batch_tuning tune{256, 0, 0, 32};
+    dragon_batch_tuning tune{256, 0, 0, 32, 1};
     int s1d = -1;
     cudaStream_t stream = nullptr;
     BatchInst* d_insts = nullptr;
@@ -225,7 +244,7 @@ void release_device(dragon_batch* b) {
 
 int tiles_along(int n, int t) { return (n + t - 1) / t; }
 
-BatchInst make_inst(dragon_grid* h, int tile) {
+BatchInst make_inst(dragon_grid* h, int tile, int group) {
     BatchInst I;
     std::memset(&I, 0, sizeof(I));
     I.kind = h->dim == 1 ? K1D : KMHD2D;
@@ -253,6 +272,7 @@ BatchInst make_inst(dragon_grid* h, int tile) {
     pa.bc_first = 0;
     I.ntiles[0] = 1;
     I.ntj[0] = 1;
+    I.group = group < 1 ? 1 : group;
     if (I.kind == K1D) {
         I.last_phase = 1;
         I.ntiles[1] = tiles_along(h->n[0] + 2 * h->g, tile);
@@ -270,7 +290,8 @@ BatchInst make_inst(dragon_grid* h, int tile) {
     for (int k = 0; k < 7; k++) {
         const int ni = nx + ext[k], nj = ny + ext[k];
         I.ntj[2 + k] = tiles_along(nj, kTileJ);
-        I.ntiles[2 + k] = I.ntj[2 + k] * tiles_along(ni, kTileI);
+        I.rtiles[2 + k] = I.ntj[2 + k] * tiles_along(ni, kTileI);
+        I.ntiles[2 + k] = tiles_along(I.rtiles[2 + k], I.group);
     }
     return I;
 }
@@ -312,7 +333,7 @@ int build(dragon_batch* b) {
     const int n = (int)b->members.size();
     std::vector<BatchInst> insts;
     insts.reserve(n);
-    for (dragon_grid* h : b->members) insts.push_back(make_inst(h, b->tune.tile_1d));
+    for (dragon_grid* h : b->members) insts.push_back(make_inst(h, b->tune.tile_1d, b->tune.mhd_tiles));
     const std::vector<WorkItem> q = make_queue(insts, b->tune.order);
     b->nitems = (int)q.size();
     b->ctr_words = kCtrDone + (size_t)kPhases * n;
@@ -397,6 +418,11 @@ int advance(dragon_batch* b, int nsteps, dragon_batch_stats* st) {
     for (dragon_grid* h : b->members) CKB(cudaStreamSynchronize(h->stream));
     if (b->dirty && (rc = build(b))) return rc;
     CKB(cudaMemsetAsync(b->d_ctr + kCtrTimeouts, 0, sizeof(unsigned), b->stream));
+    {
+        const unsigned active = (unsigned)n;
+        CKB(cudaMemcpyAsync(b->d_ctr + kCtrActive, &active, sizeof(unsigned), cudaMemcpyHostToDevice, b->stream));
+        CKB(cudaStreamSynchronize(b->stream));
+    }
     int retries = 0, replays = 0;
     float ms_total = 0.f;
     const int max_replays = (nsteps + 1) / b->tune.graph_steps + 2;
@@ -498,9 +524,11 @@ int dragon_gpu_batch_size(const dragon_batch* b) { return b ? (int)b->members.si
 int dragon_gpu_batch_set_tuning(dragon_batch* b, const dragon_batch_tuning* t) {
     if (!b || !t) return fail(DRAGON_GPU_EINVAL, "null argument");
     if ((t->tile_1d != 128 && t->tile_1d != 256) || t->ctas_per_sm < 0 || t->ctas_per_sm > 8 || t->order < 0 ||
-        t->order > 2 || t->graph_steps < 1 || t->graph_steps > 1024)
+        t->order > 2 || t->graph_steps < 1 || t->graph_steps > 1024 ||
+        !(t->mhd_tiles == 0 || t->mhd_tiles == 1 || t->mhd_tiles == 2 || t->mhd_tiles == 4 || t->mhd_tiles == 8))
         return fail(DRAGON_GPU_EINVAL, "invalid batch tuning");
     b->tune = *t;
+    if (b->tune.mhd_tiles == 0) b->tune.mhd_tiles = 1;
     b->dirty = true;
     return 0;
 }
@@ -570,19 +598,34 @@ int dragon_gpu_batch_autotune(dragon_batch* b, int steps, dragon_batch_tuning* b
     dragon_batch_tuning win = keep;
     double win_ms = INFINITY;
     int rc = 0;
+    auto trial = [&](const dragon_batch_tuning& t) -> int {
+        b->tune = t;
+        b->dirty = true;
+        dragon_batch_stats s{};
+        int r = advance(b, steps, &s);
+        if (r) return r;
+        if ((r = restore())) return r;
+        if (s.replay_ms < win_ms) {
+            win_ms = s.replay_ms;
+            win = t;
+        }
+        return 0;
+    };
+    // launch shape and queue order with one MHD tile per item, then the MHD
+    // tiles per item for the best of those
     for (int tile : {128, 256})
         for (int per_sm : {1, 2, 4, 8})
-            for (int order : {0, 1, 2}) {
-                dragon_batch_tuning t{tile, per_sm, order, steps};
-                b->tune = t;
-                b->dirty = true;
-                dragon_batch_stats s{};
-                if ((rc = advance(b, steps, &s))) break;
-                if ((rc = restore())) break;
-                if (s.replay_ms < win_ms) {
-                    win_ms = s.replay_ms;
-                    win = t;
-                }
+            for (int order : {0, 1, 2})
+                if (!rc) rc = trial(dragon_batch_tuning{tile, per_sm, order, steps, 1});
+    const dragon_batch_tuning base = win;
+    bool any_mhd = false;
+    for (dragon_grid* h : b->members) any_mhd |= h->dim == 2;
+    if (any_mhd)
+        for (int group : {2, 4, 8})
+            if (!rc) {
+                dragon_batch_tuning t = base;
+                t.mhd_tiles = group;
+                rc = trial(t);
             }
     free_snaps();
     win.graph_steps = keep.graph_steps;

@@ -55,8 +55,9 @@ def assert_same(a, b):
             np.testing.assert_array_equal(b1, b2)
 
 
-@pytest.mark.parametrize("tile,order,per_sm", [(256, 0, 0), (128, 1, 1), (256, 2, 2)])
-def test_batch_matches_single_grid_advance(workload, tile, order, per_sm):
+@pytest.mark.parametrize("tile,order,per_sm,group", [(256, 0, 0, 1), (128, 1, 1, 1), (256, 2, 2, 1), (256, 0, 0, 2),
+                                                     (128, 2, 1, 4), (256, 1, 2, 8)])
+def test_batch_matches_single_grid_advance(workload, tile, order, per_sm, group):
     one, two = workload
     steps = 9
     ref = make_grids(one, two)
@@ -64,7 +65,7 @@ def test_batch_matches_single_grid_advance(workload, tile, order, per_sm):
         G.advance_steps(steps)
     grids = make_grids(one, two)
     b = batch.Batch(grids)
-    b.tuning = batch.Tuning(tile_1d=tile, ctas_per_sm=per_sm, order=order, graph_steps=4)
+    b.tuning = batch.Tuning(tile_1d=tile, ctas_per_sm=per_sm, order=order, graph_steps=4, mhd_tiles=group)
     st = b.advance_steps(steps)
     assert st["spin_timeouts"] == 0 and st["graph_replays"] >= 3
     assert_same(states(grids), states(ref))
