@@ -23,7 +23,7 @@ class Tuning:
     ctas_per_sm: int = 0     # 0: as many as fit
     order: int = ORDER_PHASE_MAJOR
     graph_steps: int = 32
-    mhd_tiles: int = 1       # 32 x 8 tiles of a 2D MHD phase per work item
+    mhd_tiles: int = 8       # 32 x 8 tiles of a 2D MHD phase per work item
 
     def to_c(self):
         return _lib.BatchTuning(self.tile_1d, self.ctas_per_sm, self.order, self.graph_steps, self.mhd_tiles)

@@ -208,7 +208,7 @@ StepKernel pick_kernel(int s1d, int tile) {
 
 struct dragon_batch {
     std::vector<dragon_grid*> members;
-    dragon_batch_tuning tune{256, 0, 0, 32, 1};
+    dragon_batch_tuning tune{256, 0, 0, 32, 8};
     int s1d = -1;
     cudaStream_t stream = nullptr;
     BatchInst* d_insts = nullptr;

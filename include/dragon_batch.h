@@ -35,7 +35,7 @@ typedef struct dragon_batch_tuning {
     int order;        /* queue order: 0 phase-major (all grids' phase k before phase k+1, 1D tiles after
                          the first MHD phase), 1 1D grids first, 2 largest grids first within each phase */
     int graph_steps;  /* steps captured per CUDA graph */
-    int mhd_tiles;    /* 32 x 8 tiles of a 2D MHD phase per work item: 1, 2, 4 or 8 (0 reads as 1) */
+    int mhd_tiles;    /* 32 x 8 tiles of a 2D MHD phase per work item: 1, 2, 4 or 8 (0 reads as 1; default 8) */
 } dragon_batch_tuning;
 
 typedef struct dragon_batch_stats {
