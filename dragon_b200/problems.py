@@ -110,6 +110,112 @@ def riemann_1d(n, left, right, ghosts=2, x0=0.5):
     return sod_1d(n, ghosts=ghosts, x0=x0, left=left, right=right)
 
 
+def diagonal_advection(dim, n, ghosts=2, rho0=1.0, rho1=0.1, p=1.0):
+    """Smooth density wave advected along the diagonal of the periodic unit
+    square / cube (Examples/Diagonal/Problem2D.cpp:16-37, Problem3D.cpp:24-36):
+    rho = rho0 + rho1 sin(2 pi (x + y [+ z])), p = 1, v = (1, 1[, 1]), cells
+    n per side, dx = 1/n, centres at (i + 1/2) dx."""
+    d = 1.0 / n
+    c = (np.arange(n) + 0.5) * d
+    g = ghosts
+    w = np.zeros((n + 2 * g,) * dim + (5,))
+    sl = (slice(g, g + n),) * dim
+    s = sum(np.meshgrid(*([c] * dim), indexing="ij"))
+    w[sl + (0,)] = rho0 + rho1 * np.sin(2 * math.pi * s)
+    w[sl + (1,)] = p
+    for a in range(dim):
+        w[sl + (2 + a,)] = 1.0
+    return w, d
+
+
+def diagonal_errors(w, n, t, ghosts, rho0=1.0, rho1=0.1):
+    """L1, L2 and max error of the density against the advected wave at time t
+    (Examples/Diagonal/Problem2D.cpp:72-99): the exact density at a centre is
+    rho0 + rho1 sin(2 pi (x + y - 2 t)) in 2D, (x + y + z - 3 t) in 3D; L1 and
+    L2 are means over the n^dim cells."""
+    dim = w.ndim - 1
+    c = (np.arange(n) + 0.5) / n
+    s = sum(np.meshgrid(*([c] * dim), indexing="ij"))
+    exact = rho0 + rho1 * np.sin(2.0 * math.pi * (s - dim * t))
+    err = np.abs(w[(slice(ghosts, ghosts + n),) * dim + (0,)] - exact)
+    cells = float(n ** dim)
+    return float(err.sum() / cells), float(math.sqrt((err * err).sum() / cells)), float(err.max())
+
+
+def loop_potential(nx, ny, d, gaussian=False, B0=1e-6, centre=(1.0, 0.5)):
+    """Vector potential A_z of the field loop at the grid nodes (i dx, j dy),
+    i <= nx, j <= ny (Examples/LoopAdvection/Problem2D.cpp:54-60,
+    Problem3D.cpp:53-58; independent of z): B0 max(r0 - r, 0) with r0 = 0.2
+    (uniform |B| inside the loop), or B0 exp(-r^2 / (2 r0^2)) with r0 = 0.1."""
+    r0 = 0.1 if gaussian else 0.2
+    X, Y = np.meshgrid(np.arange(nx + 1) * d - centre[0], np.arange(ny + 1) * d - centre[1], indexing="ij")
+    r = np.sqrt(X * X + Y * Y)
+    if gaussian:
+        return B0 * np.exp(-0.5 * (r / r0) ** 2)
+    return B0 * np.maximum(r0 - r, 0.0)
+
+
+def faces_from_potential(Az, d, ghosts, nz=None):
+    """Face-centred B of A = (0, 0, A_z(x, y)) by CT::Faraday(A, B, -1/dx,
+    -1/dy[, -1/dz], 0) on a zero field (MHD/B_fields.cpp:21-66): x faces (i, j)
+    take (A[i, j+1] - A[i, j]) / dy, y faces (i, j) take -(A[i+1, j] - A[i, j]) /
+    dx, z faces zero, each evaluated as the reference does (0 - diff * (-1/d));
+    with nz the same values on every z layer of a 3D face array. Ghost faces
+    stay zero for the boundary fill."""
+    nx, ny = Az.shape[0] - 1, Az.shape[1] - 1
+    g = ghosts
+    inv = -1.0 / d
+    bx = 0.0 - (Az[:, 1:] - Az[:, :-1]) * inv
+    by = 0.0 - (-(Az[1:, :] - Az[:-1, :]) * inv)
+    if nz is None:
+        B = np.zeros((nx + 1 + 2 * g, ny + 1 + 2 * g, 3))
+        B[g:g + nx + 1, g:g + ny, 0] = bx
+        B[g:g + nx, g:g + ny + 1, 1] = by
+        return B
+    B = np.zeros((nx + 1 + 2 * g, ny + 1 + 2 * g, nz + 1 + 2 * g, 3))
+    B[g:g + nx + 1, g:g + ny, g:g + nz, 0] = bx[:, :, None]
+    B[g:g + nx, g:g + ny + 1, g:g + nz, 1] = by[:, :, None]
+    return B
+
+
+def field_loop(dim, n, ghosts=3, gaussian=False, rho=1.0, p=5.0, B0=1e-6):
+    """Field-loop advection on the periodic [0,2] x [0,1] (x [0,1]) box with
+    n x n/2 (x n/2) cells of width 2/n (Examples/LoopAdvection/Problem2D.cpp:
+    17-52, Problem3D.cpp:17-51): rho = 1, p = 5, v = (2, 0.5) in 2D and (2, 1,
+    1) in 3D, B from the loop's potential (loop_potential). Returns the cell
+    array (cell B left zero: initialize_B_fields fills it), the face array and
+    dx."""
+    ns = (n, n // 2) if dim == 2 else (n, n // 2, n // 2)
+    v = (2.0, 0.5) if dim == 2 else (2.0, 1.0, 1.0)
+    d = 2.0 / n
+    g = ghosts
+    w = np.zeros(tuple(x + 2 * g for x in ns) + (8,))
+    sl = tuple(slice(g, g + x) for x in ns)
+    w[sl + (0,)] = rho
+    w[sl + (1,)] = p
+    for a in range(dim):
+        w[sl + (2 + a,)] = v[a]
+    Az = loop_potential(ns[0], ns[1], d, gaussian, B0)
+    B = faces_from_potential(Az, d, g, nz=None if dim == 2 else ns[2])
+    return w, B, d
+
+
+def loop_errors(w, w0, n, ghosts, B0=1e-6):
+    """L1, L2 and max of | |B|^2 - |B_0|^2 | / B0^2 over the cells against the
+    initial cell field w0 (Examples/LoopAdvection/Problem2D.cpp:87-117,
+    Problem3D.cpp:71-95; at the final time the loop is back where it
+    started). L1 and L2 divide by n^dim, as the reference's problemComplete
+    does, although the box holds n^dim / 2^(dim-1) cells."""
+    g = ghosts
+    dim = w.ndim - 1
+    sl = tuple(slice(g, g + x) for x in ((n, n // 2) if dim == 2 else (n, n // 2, n // 2)))
+    b2 = (w[sl + (slice(5, 8),)] ** 2).sum(axis=-1)
+    b2e = (w0[sl + (slice(5, 8),)] ** 2).sum(axis=-1)
+    err = np.abs(b2 - b2e) / (B0 * B0)
+    cells = float(n ** dim)
+    return float(err.sum() / cells), float(math.sqrt((err * err).sum() / cells)), float(err.max())
+
+
 def batch_instances(n1d=2048, n2d=256, seed=5, sizes_1d=(64, 4096), sizes_2d=(64, 128, 256)):
     """The batched uneven-instance workload: n1d 1D hydro Riemann problems with
     N log-uniform in sizes_1d and per-side rho log-uniform in [0.01, 10], p

@@ -1,0 +1,126 @@
+"""Generates tests/golden/convergence.json: the reference's accuracy studies
+(Examples/Diagonal, Examples/LoopAdvection) run at small sizes through the
+DRAGON reference itself (oracle/_ref, driven through its Grid / Boundary / CFL
+API), together with the tables the reference publishes for the full sizes
+(Examples/Diagonal/Outputs/Validation_data.md:23-44,
+Examples/LoopAdvection/Outputs/Validation_data.md:20-53).
+
+Each run follows the examples' main loop (DRAGON/main/main.cpp:124-150):
+while t < final_time, advance(dt) and t += dt, then the problem's
+problemComplete norms at that t.
+  diagonal   HLLC, CTU, CFL_ADD 0.3, periodic, dt 0.05 to t = 1
+  field loop HLLD (HLLX), MC, CTU + CT with CT_CONSV_TOTAL_E, periodic,
+             dt 0.1 to t = 4
+
+Two published tables are not what the reference computes from its example
+sources: the 2D uniform loop (the example's uniform potential,
+std::max(r0 - r, 0), does not compile as shipped; its Linf column matches at
+n = 64 and 128, L1 and L2 do not) and the 3D diagonal wave (within 2e-3).
+Those rows are kept for the record; "reproduced" lists the tables whose every
+row was matched to the printed digits by running the example (the reference
+itself for 2D MC n = 128, the device path, which is the reference's
+arithmetic bit for bit, for all of them). The small-size runs below are the
+reference's own output.
+
+Run: python tests/golden/make_convergence.py
+"""
+import json
+import os
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from dragon_b200 import boundary, problems  # noqa: E402
+from oracle import refgrid  # noqa: E402
+from oracle.refgrid import bc_entries_from  # noqa: E402
+
+RIEMANN_HLLC, RIEMANN_HLLX = 2, 5
+LIMITERS = {"minmod": 0, "mc": 1, "superbee": 3}
+CT_CONSV_TOTAL_E = 0
+
+# Published (6 significant digits as printed by the reference): L1, L2, Linf.
+PUBLISHED = {
+    "diagonal": {
+        "2d_minmod": {256: (0.000286346, 0.000449423, 0.00151213), 512: (7.83388e-05, 0.000142185, 0.000610277)},
+        "2d_mc": {128: (0.000224884, 0.000310695, 0.000942581), 256: (5.63051e-05, 9.3146e-05, 0.000387981),
+                  512: (1.40658e-05, 2.81185e-05, 0.000159312)},
+        "2d_superbee": {128: (0.000693177, 0.00090973, 0.00278401), 256: (0.000198661, 0.00029218, 0.00127189)},
+        "3d_mc": {64: (0.00116811, 0.00139005, 0.00291), 128: (0.000321543, 0.000424485, 0.00121935),
+                  256: (8.19464e-05, 0.000128312, 0.000514205)},
+    },
+    "loop": {
+        "2d_uniform": {64: (0.0286387, 0.152378, 0.996704), 128: (0.0172391, 0.0949274, 0.997576),
+                       256: (0.00968561, 0.0666294, 0.996234), 512: (0.00641105, 0.0512477, 0.99921)},
+        "2d_gaussian": {64: (0.601428, 3.53229, 31.4691), 128: (0.273266, 1.7344, 20.7554),
+                        256: (0.0753625, 0.521772, 8.74698), 512: (0.0261989, 0.187809, 3.77506)},
+        "3d_uniform": {64: (0.0139403, 0.107475, 0.999567), 128: (0.00866564, 0.066301, 0.998004),
+                       256: (0.00485955, 0.0461968, 0.993108)},
+        "3d_gaussian": {64: (0.323758, 2.65926, 32.7321), 128: (0.161105, 1.43543, 22.2412),
+                        256: (0.0459888, 0.438878, 9.38652)},
+    },
+}
+# Tables whose published rows the example reproduces to every printed digit.
+REPRODUCED = {"diagonal": ["2d_minmod", "2d_mc", "2d_superbee"], "loop": ["2d_gaussian", "3d_uniform", "3d_gaussian"]}
+
+
+def run_main_loop(grid, dt, final_time):
+    t = 0.0
+    while t < final_time:
+        grid.advance(dt)
+        t += dt
+    return t
+
+
+def diagonal(dim, n, limiter):
+    R = refgrid.RefGrid(dim, (n,) * dim, (1.0 / n,) * dim, ghosts=2, riemann=RIEMANN_HLLC,
+                        limiter=LIMITERS[limiter], cfl=1)
+    w0, _ = problems.diagonal_advection(dim, n, ghosts=R.ghosts)
+    R.set_prim(w0)
+    R.set_boundary(bc_entries_from(boundary.as_list(boundary.Periodic())))
+    t = run_main_loop(R, 0.05, 1.0)
+    return problems.diagonal_errors(R.get_prim(), n, t, R.ghosts)
+
+
+def loop(dim, n, gaussian):
+    ns = (n, n // 2) if dim == 2 else (n, n // 2, n // 2)
+    R = refgrid.RefGrid(dim, ns, (2.0 / n,) * dim, ghosts=3, mhd=True, ct_runtime=True, riemann=RIEMANN_HLLX,
+                        limiter=LIMITERS["mc"], cfl=1, ct_energy=CT_CONSV_TOTAL_E)
+    w, B, _ = problems.field_loop(dim, n, ghosts=R.ghosts, gaussian=gaussian)
+    R.set_prim(w)
+    R.set_faceB(B)
+    R.set_boundary(bc_entries_from(boundary.as_list(boundary.Periodic())))
+    R.initialize_B_fields()
+    w0 = R.get_prim()
+    run_main_loop(R, 0.1, 4.0)
+    return problems.loop_errors(R.get_prim(), w0, n, R.ghosts)
+
+
+SMALL = [
+    ("diagonal", "2d_mc", 32, lambda: diagonal(2, 32, "mc")),
+    ("diagonal", "2d_minmod", 32, lambda: diagonal(2, 32, "minmod")),
+    ("diagonal", "2d_superbee", 32, lambda: diagonal(2, 32, "superbee")),
+    ("diagonal", "3d_mc", 16, lambda: diagonal(3, 16, "mc")),
+    ("loop", "2d_uniform", 32, lambda: loop(2, 32, False)),
+    ("loop", "2d_uniform", 64, lambda: loop(2, 64, False)),
+    ("loop", "2d_gaussian", 32, lambda: loop(2, 32, True)),
+    ("loop", "3d_uniform", 16, lambda: loop(3, 16, False)),
+]
+
+
+def main():
+    assert refgrid.available("hydro") and refgrid.available("mhd_rt"), "build oracle/_ref first"
+    out = {"published": {}, "reproduced": REPRODUCED, "reference": {}}
+    for study, rows in PUBLISHED.items():
+        out["published"][study] = {k: {str(n): v for n, v in r.items()} for k, r in rows.items()}
+    for study, case, n, fn in SMALL:
+        norms = fn()
+        out["reference"].setdefault(study, {}).setdefault(case, {})[str(n)] = norms
+        print(study, case, n, norms, flush=True)
+    with open(os.path.join(HERE, "convergence.json"), "w") as f:
+        json.dump(out, f, indent=1)
+
+
+if __name__ == "__main__":
+    main()
