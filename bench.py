@@ -111,6 +111,50 @@ def e2e_run(G0, grids, dev, steps, barrier):
     return max(start.elapsed_time(e) for e in ends)
 
 
+def copy_bound(dev, nbytes, cells, reps=8):
+    """The host-link ceiling of the end-to-end step: `reps` pinned uploads and
+    `reps` pinned downloads of one step's state, each direction on its own
+    stream, alone and both at once (the two copy directions overlap), timed
+    with CUDA events. Returns the per-direction bandwidths, the duplex time per
+    step and the cell-updates/s a step could reach if the copies were its only
+    cost."""
+    import torch
+    host_in = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    host_out = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    d_in = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    d_out = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    up, down = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+
+    def timed(streams_ops):
+        torch.cuda.synchronize()
+        start = torch.cuda.Event(enable_timing=True)
+        start.record(torch.cuda.current_stream(dev))
+        ends = []
+        for s, op in streams_ops:
+            s.wait_event(start)
+            with torch.cuda.stream(s):
+                for _ in range(reps):
+                    op()
+                e = torch.cuda.Event(enable_timing=True)
+                e.record(s)
+                ends.append(e)
+        torch.cuda.synchronize()
+        return max(start.elapsed_time(e) for e in ends) / reps
+
+    def h2d():
+        d_in.copy_(host_in, non_blocking=True)
+
+    def d2h():
+        host_out.copy_(d_out, non_blocking=True)
+
+    timed([(up, h2d), (down, d2h)])  # warm-up
+    h2d_ms = timed([(up, h2d)])
+    d2h_ms = timed([(down, d2h)])
+    duplex_ms = timed([(up, h2d), (down, d2h)])
+    return {"h2d_gbs": nbytes / (h2d_ms / 1e3) / 1e9, "d2h_gbs": nbytes / (d2h_ms / 1e3) / 1e9,
+            "duplex_ms_per_step": duplex_ms, "value": cells / (duplex_ms / 1e3), "unit": "cell-updates/s"}
+
+
 def roofline_fp64(k_avg_ms, dev):
     """The fused FP64 step against FP64 throughput: it is bound by FP64 issue, not
     by HBM, so this is the roofline that explains it."""
@@ -606,6 +650,7 @@ def run_gpu(args):
     e2e_value = ws * N * N * e2e_steps * len(e2e_grids) / (e2e_ms / 1e3)
     e2e_serial_value = ws * N * N * e2e_steps / (e2e_serial_ms / 1e3)
     bytes_step = G.w.nbytes
+    link = copy_bound(dev, bytes_step, N * N)
 
     if rank == 0:
         peak, peak_kind = measured_peaks()
@@ -623,7 +668,8 @@ def run_gpu(args):
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
             "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": bytes_step,
                     "d2h_bytes_per_step": bytes_step, "steps": e2e_steps * len(e2e_grids),
-                    "grids_in_flight": len(e2e_grids), "one_grid_value": e2e_serial_value},
+                    "grids_in_flight": len(e2e_grids), "one_grid_value": e2e_serial_value,
+                    "copy_bound": link, "frac_of_copy_bound": e2e_value / ws / link["value"]},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                          "kernel": "k_step2d_hydro", "kernel_ms_avg": k_avg_ms,
