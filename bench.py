@@ -26,7 +26,8 @@ fused update). Metric: cell-updates/s (interior cells x steps / time).
              with the reference's mean guess, the analytic guess and the
              GPU-trained network's guess (training included);
   batch      2048 1D hydro + 256 2D MHD grids of uneven sizes advanced by the
-             persistent work-queue kernel, against the same grids one by one;
+             persistent work-queue kernel, against the same grids one by one,
+             in mixed FP32/FP64 (with its L1 per field from FP64) and FP64;
   mhd        2D MHD Orszag-Tang 1024^2, FP64 and mixed, with the mixed path's
              L1 per field and max |div B| of both.
 
@@ -443,12 +444,10 @@ def mhd_report(n=1024, steps=20, warmup=3):
     return out
 
 
-def batch_report(steps=500, one_by_one_steps=50):
-    """Batched uneven instances: 2048 1D hydro Riemann problems (N log-uniform
-    in [64, 4096], seeded states) and 256 2D MHD blasts (64^2 / 128^2 / 256^2,
-    HLLD + CT, periodic), each with its own CFL dt, advanced together by the
-    persistent work-queue kernel (autotuned launch shape, CUDA-graph replays);
-    against the same grids advanced one after another."""
+def _batch_run(precision, steps, one_by_one_steps):
+    """One precision of the batched uneven-instance workload: the batch
+    (autotuned, then timed over `steps` steps) and the same grids advanced one
+    after another. Returns the report and the batch's grids (still open)."""
     import torch
 
     import dragon_b200 as dg
@@ -460,12 +459,14 @@ def batch_report(steps=500, one_by_one_steps=50):
         grids = []
         for spec in one:
             G = dg.Grid1D(spec["n"], spec["dx"], ghosts=2, config=dg.Config(riemann=dg.RIEMANN_HLLX,
-                                                                              limiter=dg.LIMITER_MC))
+                                                                              limiter=dg.LIMITER_MC,
+                                                                              precision=precision))
             G.w[...] = spec["w"]
             grids.append(G)
         for spec in two:
             n = spec["n"]
-            G = dg.Grid2D(n, n, spec["dx"], spec["dx"], ghosts=3, config=dg.Config(mhd=True, riemann=dg.RIEMANN_HLLX))
+            G = dg.Grid2D(n, n, spec["dx"], spec["dx"], ghosts=3,
+                          config=dg.Config(mhd=True, riemann=dg.RIEMANN_HLLX, precision=precision))
             G.w[...] = spec["w"]
             G.B[...] = spec["B"]
             G.boundary = dg.Periodic()
@@ -484,8 +485,6 @@ def batch_report(steps=500, one_by_one_steps=50):
     t0 = time.perf_counter()
     st = b.advance_steps(steps)
     wall = time.perf_counter() - t0
-    for G in grids:
-        G.close()
     ref = make()
     for G in ref:
         G.advance_steps(3)
@@ -499,15 +498,48 @@ def batch_report(steps=500, one_by_one_steps=50):
         G.close()
     rate = cells * steps / wall
     rate1 = cells * one_by_one_steps / wall1
-    return {"workload": "2048 1D hydro Riemann problems (N log-uniform [64,4096]) + 256 2D MHD blasts "
-                        "(64^2/128^2/256^2), HLLC / HLLD, MC, own CFL dt each, FP64",
-            "instances": len(one) + len(two), "cells_per_step": cells, "steps": steps,
-            "value": rate, "unit": "cell-updates/s", "device_value": cells * steps / (st["replay_ms"] / 1e3),
-            "one_by_one_value": rate1, "one_by_one_steps": one_by_one_steps, "speedup_vs_one_by_one": rate / rate1,
-            "work_items_per_step": st["work_items"], "graph_replays": st["graph_replays"],
-            "retries": st["retries"], "spin_timeouts": st["spin_timeouts"],
-            "tuning": {"tile_1d": tune.tile_1d, "ctas_per_sm": tune.ctas_per_sm, "order": tune.order,
-                       "graph_steps": tune.graph_steps, "mhd_tiles": tune.mhd_tiles}, "autotune_seconds": tune_s}
+    report = {"instances": len(one) + len(two), "cells_per_step": cells, "steps": steps,
+              "value": rate, "unit": "cell-updates/s", "device_value": cells * steps / (st["replay_ms"] / 1e3),
+              "one_by_one_value": rate1, "one_by_one_steps": one_by_one_steps, "speedup_vs_one_by_one": rate / rate1,
+              "work_items_per_step": st["work_items"], "graph_replays": st["graph_replays"],
+              "retries": st["retries"], "spin_timeouts": st["spin_timeouts"],
+              "tuning": {"tile_1d": tune.tile_1d, "ctas_per_sm": tune.ctas_per_sm, "order": tune.order,
+                         "graph_steps": tune.graph_steps, "mhd_tiles": tune.mhd_tiles}, "autotune_seconds": tune_s}
+    return report, grids
+
+
+def batch_report(steps=500, one_by_one_steps=50):
+    """Batched uneven instances: 2048 1D hydro Riemann problems (N log-uniform
+    in [64, 4096], seeded states) and 256 2D MHD blasts (64^2 / 128^2 / 256^2,
+    HLLD + CT, periodic), each with its own CFL dt, advanced together by the
+    persistent work-queue kernel (autotuned launch shape, CUDA-graph replays);
+    against the same grids advanced one after another. The workload runs in
+    mixed FP32/FP64 (the reported value) and in FP64; after the timed steps the
+    mixed states are compared with the FP64 ones (relative L1 per field, summed
+    over the members of each kind)."""
+    import dragon_b200 as dg
+
+    mixed, gm = _batch_run(dg.PREC_MIXED, steps, one_by_one_steps)
+    fp64, gf = _batch_run(dg.PREC_FP64, steps, one_by_one_steps)
+    names = {1: ["rho", "p", "vx", "vy", "vz"], 2: ["rho", "p", "vx", "vy", "vz", "Bx", "By", "Bz"]}
+    num, den = {}, {}
+    for G, R in zip(gm, gf):
+        g = G.ghosts
+        sl = tuple(slice(g, g + n) for n in G.n)
+        a, r = G.w[sl].reshape(-1, G.w.shape[-1]), R.w[sl].reshape(-1, R.w.shape[-1])
+        num[G.dim] = num.get(G.dim, 0) + np.abs(a - r).sum(axis=0)
+        den[G.dim] = den.get(G.dim, 0) + np.abs(r).sum(axis=0)
+    l1 = {("1d_hydro" if d == 1 else "2d_mhd"): {k: float(v) for k, v in zip(names[d], num[d] / np.where(den[d] > 0, den[d], 1))}
+          for d in num}
+    for G in gm + gf:
+        G.close()
+    out = {"workload": "2048 1D hydro Riemann problems (N log-uniform [64,4096]) + 256 2D MHD blasts "
+                       "(64^2/128^2/256^2), HLLC / HLLD, MC, own CFL dt each, mixed FP32/FP64",
+           **mixed, "l1_vs_fp64_after_steps": l1,
+           "fp64": {k: fp64[k] for k in ("value", "device_value", "one_by_one_value", "speedup_vs_one_by_one",
+                                         "retries", "tuning")}}
+    out["mixed_vs_fp64"] = mixed["value"] / fp64["value"]
+    return out
 
 
 def run_gpu(args):

@@ -5,9 +5,11 @@ dragon_b200/libdragon_gpu.so:
   * the FP64 kernels with --fmad=false, so no a*b+c is fused: together with
     IEEE division and square root this keeps the FP64 path's arithmetic
     identical to the reference's (compiled without contraction);
-  * the mixed-precision kernels (step_mixed.cu, step_mhd_mixed.cu) with FMA
-    contraction and fast single-precision division / square root; these
-    flags leave FP64 alone.
+  * the mixed-precision kernels (step_mixed.cu, step_mhd_mixed.cu,
+    step1d_mixed.cu, batch_mixed.cu) with FMA contraction and fast
+    single-precision division / square root; the division, square-root and
+    denormal flags act on FP32 only, and the contraction also fuses the FP64
+    arithmetic of these files (the mixed path is not held to bit parity).
 """
 from __future__ import annotations
 
@@ -26,7 +28,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 BASE = ["-std=c++17", "-O3", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC", "-I" + os.path.join(ROOT, "include")]
 EXACT = ["--fmad=false"]
 FAST32 = ["--fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
-PER_FILE = {"step_mixed.cu": FAST32, "step_mhd_mixed.cu": FAST32}
+PER_FILE = {"step_mixed.cu": FAST32, "step_mhd_mixed.cu": FAST32, "step1d_mixed.cu": FAST32,
+            "batch_mixed.cu": FAST32}
 
 
 def _sources():

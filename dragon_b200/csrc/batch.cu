@@ -1,21 +1,11 @@
 // Batched step of many independent grids (include/dragon_batch.h): one
-// persistent kernel per step over a device work queue, the per-step launches
-// captured in a CUDA graph, and an autotuner over the launch shape.
-//
-// Work items of one member and one step, in dependency order:
-//   phase 0      the prologue: step bookkeeping, ghost fill, CFL dt (one item)
-//   1D hydro     phase 1: step tiles of tile_1d cells
-//   2D MHD       phase 1: copy of the state and face B into the output buffer,
-//                phases 2-8: the seven phases of the single-grid step, one
-//                32 x 8 cell tile per item
-// A CTA takes the next item from a global counter, waits until every item of
-// the member's previous phase has finished, runs it and counts it done. The
-// queue lists a member's phases in order, so every item a CTA can wait for was
-// taken earlier by a CTA that is running and never waits on a later item: the
-// waits always end (each is bounded anyway, and a wait that gives up is
-// counted and reported). The CTA that finishes a member's last item of the
-// step flips the member's current buffer unless the step failed or was not
-// taken. Every member therefore follows exactly its own single-grid advance.
+// persistent kernel per step over a device work queue (batch_kernel.cuh), the
+// per-step launches captured in a CUDA graph, and an autotuner over the launch
+// shape. Members of a batch share one precision: the FP64 batch runs the
+// kernel instantiated here; a mixed FP32/FP64 batch runs the one in
+// batch_mixed.cu and its prologues in k_batch_prologue below. Every member
+// follows its own single-grid advance: exactly in FP64, and in mixed
+// precision exactly for 1D members and to FP32 rounding for 2D MHD members.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -25,55 +15,16 @@
 #include <vector>
 
 #include "../../include/dragon_batch.h"
-#include "boundary.cuh"
+#include "batch_kernel.cuh"
 #include "handle.h"
-#include "step_hydro.cuh"
-#include "step_mhd.cuh"
 
 void dragon_gpu_set_error_message(const char* msg);
 
 using namespace dgpu;
 using namespace dgpu_rt;
+using namespace dgpu_batch;
 
 namespace {
-
-constexpr int kPhases = 9;
-constexpr int kThreads = 256;
-constexpr int kCopyChunk = kThreads * 16;     // doubles per copy item
-constexpr long long kSpinLimit = 1LL << 24;   // polls of a dependency wait (each >= 64 ns)
-enum Kind : int { K1D = 0, KMHD2D = 1 };
-
-struct BatchInst {
-    int kind;
-    int last_phase;
-    int ntiles[kPhases];     // work items of each phase
-    int rtiles[kPhases];     // 32 x 8 tiles of each 2D MHD phase
-    int group;               // MHD tiles per work item
-    int ntj[kPhases];        // MHD phases: tiles along j
-    Geo G, FG;
-    double* w[2];
-    double* B[2];
-    MhdScratch S;
-    StepCtl* ctl;
-    const BCEntry* bcs;
-    StepArgs sa;
-    PrologueArgs pa;
-    long long wcount, bcount;  // doubles of the state / face B copied by phase 1 (MHD)
-};
-
-struct WorkItem {
-    int inst, phase, tile, pad;
-};
-
-// What the host needs after a replay, per member.
-struct Summary {
-    int err, done, steps_done, cur;
-};
-
-// counters: [0] dependency waits that gave up and [1] members that have not
-// finished the advance (both kept across the launches of an advance), [2] queue
-// head, [3 + kPhases * m + p] finished items of member m, phase p (reset per step)
-constexpr int kCtrTimeouts = 0, kCtrActive = 1, kCtrHead = 2, kCtrDone = 3;
 
 int fail(int code, const std::string& msg) {
     dragon_gpu_set_error_message(msg.c_str());
@@ -87,104 +38,15 @@ int fail(int code, const std::string& msg) {
             return fail(DRAGON_GPU_ECUDA, std::string(#x) + ": " + cudaGetErrorString(e_));   \
     } while (0)
 
-__device__ __forceinline__ int ldv(const int* p) { return *(const volatile int*)p; }
-
-__device__ __forceinline__ void wait_count(const unsigned* counter, unsigned target, unsigned* timeouts) {
-    long long polls = 0;
-    while (*(const volatile unsigned*)counter < target) {
-        if (++polls > kSpinLimit) {
-            atomicAdd(timeouts, 1u);
-            break;
-        }
-        __nanosleep(64);
-    }
-    __threadfence();
-}
-
-template <int S1D, int SMHD, int TS>
-__device__ __forceinline__ void run_item(const BatchInst& I, const WorkItem& wi, int cur, unsigned* active) {
-    if (wi.phase == 0) {
-        __shared__ int s_was_done;
-        if (threadIdx.x == 0) s_was_done = ldv(&I.ctl->done);
-        PrologueArgs pa = I.pa;
-        pa.slot_in = cur;
-        pa.slot_out = cur ^ 1;
-        if (I.kind == K1D) prologue_body<false>(I.G, I.FG, I.w[cur], nullptr, I.bcs, I.ctl, pa);
-        else prologue_body<true>(I.G, I.FG, I.w[cur], I.B[cur], I.bcs, I.ctl, pa);
-        __syncthreads();
-        // the member finished its steps in this prologue: one fewer to wait for
-        if (threadIdx.x == 0 && !s_was_done && ldv(&I.ctl->done)) atomicSub(active, 1u);
-        return;
-    }
-    StepArgs sa = I.sa;
-    sa.slot_out = cur ^ 1;
-    if (I.kind == K1D) {
-        step1d_tile<false, S1D, TS>(I.G, I.w[cur], I.w[cur ^ 1], I.ctl, sa, wi.tile);
-        return;
-    }
-    if (wi.phase == 1) {
-        if (ldv(&I.ctl->err) | ldv(&I.ctl->done)) return;
-        const long long base = (long long)wi.tile * kCopyChunk;
-        const long long end = base + kCopyChunk < I.wcount + I.bcount ? base + kCopyChunk : I.wcount + I.bcount;
-        for (long long e = base + threadIdx.x; e < end; e += blockDim.x) {
-            if (e < I.wcount) I.w[cur ^ 1][e] = I.w[cur][e];
-            else I.B[cur ^ 1][e - I.wcount] = I.B[cur][e - I.wcount];
-        }
-        return;
-    }
-    const Mhd2DArgs A{I.G, I.FG, I.w[cur], I.w[cur ^ 1], I.B[cur], I.B[cur ^ 1], I.S, I.ctl, sa};
-    const int nbx = I.ntj[wi.phase];
-    for (int k = 0; k < I.group; k++) {
-        const int tile = wi.tile * I.group + k;
-        if (tile >= I.rtiles[wi.phase]) break;  // uniform across the CTA
-        if (k) __syncthreads();                 // the previous tile's shared words are read
-        const Tile2 T{tile % nbx, tile / nbx, (int)(threadIdx.x % kTileJ), (int)(threadIdx.x / kTileJ)};
-        switch (wi.phase) {
-            case 2: mhd2d_halfstates(A, T); break;
-            case 3: mhd2d_prelim<SMHD>(A, T); break;
-            case 4: mhd2d_e0(A, T); break;
-            case 5: mhd2d_half(A, T); break;
-            case 6: mhd2d_final_flux<SMHD>(A, T); break;
-            case 7: mhd2d_efinal(A, T); break;
-            default: mhd2d_update(A, T); break;
-        }
-    }
-}
-
-template <int S1D, int SMHD, int TS>
-__global__ void __launch_bounds__(kThreads, 2) k_batch_step(const BatchInst* __restrict__ insts,
-                                                         const WorkItem* __restrict__ items, int nitems,
-                                                         unsigned* ctr) {
-    __shared__ int s_item;
-    // every member has finished its steps (a launch after the last one a graph
-    // replay needs): nothing to take from the queue
+// The prologues of a mixed batch's members for one step: one CTA per member
+// at a time (the step kernel then finds phase 0 complete).
+__global__ void __launch_bounds__(kThreads) k_batch_prologue(const BatchInst* __restrict__ insts, int n,
+                                                           unsigned* ctr) {
     if (*(const volatile unsigned*)&ctr[kCtrActive] == 0) return;
-    for (;;) {
-        __syncthreads();  // the previous item's users of shared memory are done
-        if (threadIdx.x == 0) s_item = (int)atomicAdd(&ctr[kCtrHead], 1u);
+    for (int m = blockIdx.x; m < n; m += gridDim.x) {
+        const BatchInst& I = insts[m];
+        prologue_item(I, ldv(&I.ctl->cur), &ctr[kCtrActive]);
         __syncthreads();
-        const int it = s_item;
-        if (it >= nitems) return;
-        const WorkItem wi = items[it];
-        const BatchInst& I = insts[wi.inst];
-        unsigned* done = ctr + kCtrDone + (size_t)kPhases * wi.inst;
-        // a member that has finished its steps (or failed this one) has nothing
-        // left to do in this launch: its items only count themselves, without
-        // waiting for the phase before them
-        if (wi.phase > 0 && threadIdx.x == 0 && !(ldv(&I.ctl->done) | ldv(&I.ctl->err)))
-            wait_count(done + wi.phase - 1, (unsigned)I.ntiles[wi.phase - 1], &ctr[kCtrTimeouts]);
-        __syncthreads();
-        const int cur = ldv(&I.ctl->cur);
-        run_item<S1D, SMHD, TS>(I, wi, cur, &ctr[kCtrActive]);
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            __threadfence();
-            const unsigned prev = atomicAdd(done + wi.phase, 1u);
-            if (wi.phase == I.last_phase && prev + 1 == (unsigned)I.ntiles[wi.phase]) {
-                StepCtl* c = I.ctl;
-                if (!ldv(&c->err) && !ldv(&c->done)) *(volatile int*)&c->cur = cur ^ 1;
-            }
-        }
     }
 }
 
@@ -195,13 +57,12 @@ __global__ void k_batch_summary(const BatchInst* __restrict__ insts, int n, Summ
     out[i] = Summary{ldv(&c->err), ldv(&c->done), ldv(&c->steps_done), ldv(&c->cur)};
 }
 
-using StepKernel = void (*)(const BatchInst*, const WorkItem*, int, unsigned*);
-
 // Built solver combinations: 1D hydro {HLLC, exact} x 2D MHD {HLLD} x tile {128, 256}.
 StepKernel pick_kernel(int s1d, int tile) {
     const bool exact = s1d == RS_EXACT;
-    if (tile == 128) return exact ? k_batch_step<RS_EXACT, RS_HLLD, 128> : k_batch_step<RS_HLLC, RS_HLLD, 128>;
-    return exact ? k_batch_step<RS_EXACT, RS_HLLD, 256> : k_batch_step<RS_HLLC, RS_HLLD, 256>;
+    if (tile == 128)
+        return exact ? k_batch_step<false, RS_EXACT, RS_HLLD, 128> : k_batch_step<false, RS_HLLC, RS_HLLD, 128>;
+    return exact ? k_batch_step<false, RS_EXACT, RS_HLLD, 256> : k_batch_step<false, RS_HLLC, RS_HLLD, 256>;
 }
 
 }  // namespace
@@ -210,6 +71,7 @@ struct dragon_batch {
     std::vector<dragon_grid*> members;
     dragon_batch_tuning tune{256, 0, 0, 32, 8};
     int s1d = -1;
+    int prec = -1;  // the members' precision (0 FP64, 1 mixed)
     cudaStream_t stream = nullptr;
     BatchInst* d_insts = nullptr;
     WorkItem* d_items = nullptr;
@@ -244,7 +106,7 @@ void release_device(dragon_batch* b) {
 
 int tiles_along(int n, int t) { return (n + t - 1) / t; }
 
-BatchInst make_inst(dragon_grid* h, int tile, int group) {
+BatchInst make_inst(dragon_grid* h, int tile, int group, bool mixed) {
     BatchInst I;
     std::memset(&I, 0, sizeof(I));
     I.kind = h->dim == 1 ? K1D : KMHD2D;
@@ -270,12 +132,12 @@ BatchInst make_inst(dragon_grid* h, int tile, int group) {
     pa.compute_dt = 1;
     pa.nbc = h->nbc;
     pa.bc_first = 0;
-    I.ntiles[0] = 1;
+    I.ntiles[0] = mixed ? 0 : 1;  // a mixed batch runs its prologues in k_batch_prologue
     I.ntj[0] = 1;
     I.group = group < 1 ? 1 : group;
     if (I.kind == K1D) {
         I.last_phase = 1;
-        I.ntiles[1] = tiles_along(h->n[0] + 2 * h->g, tile);
+        I.ntiles[1] = tiles_along(h->n[0] + 2 * h->g, mixed ? kMx1dTile : tile);
         I.ntj[1] = 1;
         return I;
     }
@@ -333,7 +195,8 @@ int build(dragon_batch* b) {
     const int n = (int)b->members.size();
     std::vector<BatchInst> insts;
     insts.reserve(n);
-    for (dragon_grid* h : b->members) insts.push_back(make_inst(h, b->tune.tile_1d, b->tune.mhd_tiles));
+    const bool mixed = b->prec == 1;
+    for (dragon_grid* h : b->members) insts.push_back(make_inst(h, b->tune.tile_1d, b->tune.mhd_tiles, mixed));
     const std::vector<WorkItem> q = make_queue(insts, b->tune.order);
     b->nitems = (int)q.size();
     b->ctr_words = kCtrDone + (size_t)kPhases * n;
@@ -347,7 +210,7 @@ int build(dragon_batch* b) {
     CKB(cudaMemsetAsync(b->d_ctr, 0, sizeof(unsigned) * b->ctr_words, b->stream));
     CKB(cudaStreamSynchronize(b->stream));
 
-    const StepKernel kern = pick_kernel(b->s1d, b->tune.tile_1d);
+    const StepKernel kern = mixed ? pick_kernel_mx(b->s1d, b->tune.tile_1d) : pick_kernel(b->s1d, b->tune.tile_1d);
     int dev = 0, sms = 0, occ = 0;
     CKB(cudaGetDevice(&dev));
     CKB(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -359,6 +222,7 @@ int build(dragon_batch* b) {
     CKB(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < b->tune.graph_steps; k++) {
         cudaMemsetAsync(b->d_ctr + kCtrHead, 0, sizeof(unsigned) * (b->ctr_words - kCtrHead), b->stream);
+        if (mixed) k_batch_prologue<<<std::min(n, sms * 8), kThreads, 0, b->stream>>>(b->d_insts, n, b->d_ctr);
         kern<<<b->grid_ctas, kThreads, 0, b->stream>>>(b->d_insts, b->d_items, b->nitems, b->d_ctr);
     }
     k_batch_summary<<<(n + 255) / 256, 256, 0, b->stream>>>(b->d_insts, n, b->d_sum);
@@ -498,7 +362,9 @@ int dragon_gpu_batch_destroy(dragon_batch* b) {
 
 int dragon_gpu_batch_add_instance(dragon_batch* b, dragon_grid* h, int* index) {
     if (!b || !h) return fail(DRAGON_GPU_EINVAL, "null argument");
-    if (h->cfg.precision != 0) return fail(DRAGON_GPU_EUNSUPPORTED, "batched members run the FP64 path");
+    if (h->cfg.precision != 0 && h->cfg.precision != 1) return fail(DRAGON_GPU_EINVAL, "unknown precision");
+    if (b->prec >= 0 && b->prec != h->cfg.precision)
+        return fail(DRAGON_GPU_EUNSUPPORTED, "batched members share one precision (FP64 or mixed)");
     if (h->dim == 1 && !h->mhd) {
         if (h->solver != RS_HLLC && h->solver != RS_EXACT)
             return fail(DRAGON_GPU_EUNSUPPORTED, "batched 1D members use HLLC / HLLX or the exact solver");
@@ -514,6 +380,7 @@ int dragon_gpu_batch_add_instance(dragon_batch* b, dragon_grid* h, int* index) {
     for (dragon_grid* m : b->members)
         if (m == h) return fail(DRAGON_GPU_EINVAL, "grid is already in the batch");
     if (index) *index = (int)b->members.size();
+    b->prec = h->cfg.precision;
     b->members.push_back(h);
     b->dirty = true;
     return 0;

@@ -15,6 +15,9 @@ struct Mhd3DScratch;
 
 int launch_step1d(bool mhd, int solver, const Geo& G, const double* win, double* wout, StepCtl* ctl,
                   const StepArgs& sa, cudaStream_t st);
+// Mixed FP32/FP64 1D hydro sweep (step1d_mixed.cu).
+int launch_step1d_mixed(int solver, const Geo& G, const double* win, double* wout, StepCtl* ctl, const StepArgs& sa,
+                        cudaStream_t st);
 int launch_step2d_hydro(int solver, const Geo& G, const double* win, double* wout, StepCtl* ctl, const StepArgs& sa,
                         cudaStream_t st);
 int launch_step2d_hydro_mixed(int solver, const Geo& G, const double* win, double* wout, StepCtl* ctl,

@@ -214,7 +214,9 @@ int launch_step(dragon_grid* h, int c) {
     }
     int rc = 0, nk = 1;
     if (h->dim == 1) {
-        rc = launch_step1d(h->mhd, h->solver, h->cg, h->w[c], h->w[c ^ 1], h->ctl, sa, h->stream);
+        rc = (h->cfg.precision == 1)
+                 ? launch_step1d_mixed(h->solver, h->cg, h->w[c], h->w[c ^ 1], h->ctl, sa, h->stream)
+                 : launch_step1d(h->mhd, h->solver, h->cg, h->w[c], h->w[c ^ 1], h->ctl, sa, h->stream);
     } else if (h->mhd) {
         if (h->dim == 3) {
             rc = launch_step3d_mhd(h->solver, h->cg, h->fg, h->w[c], h->w[c ^ 1], h->B[c], h->B[c ^ 1], h->m3_s, h->ctl,
@@ -616,9 +618,9 @@ int dragon_gpu_grid_create(int dim, int nx, int ny, int nz, double dx, double dy
         delete h;
         return fail(DRAGON_GPU_EUNSUPPORTED, "the learned star-pressure guess is built for 3D hydro grids");
     }
-    if (h->cfg.precision != 0 && dim != 2) {
+    if (h->cfg.precision != 0 && !(dim == 2 || (dim == 1 && !h->mhd))) {
         delete h;
-        return fail(DRAGON_GPU_EUNSUPPORTED, "the mixed-precision path is built for 2D grids");
+        return fail(DRAGON_GPU_EUNSUPPORTED, "the mixed-precision path is built for 1D hydro and 2D grids");
     }
     h->cg = make_geo(dim, h->n, h->g);
     int nfc[3] = {h->n[0] + 1, h->n[1] + 1, h->n[2] + 1};

@@ -9,12 +9,16 @@
  * kernel per step: CTAs take work items from a device queue (each grid's
  * ghost fill + CFL dt, then its step tiles in dependency order), and the
  * per-step launches are captured in a CUDA graph. After
- * dragon_gpu_batch_advance_steps every grid holds exactly the state its own
- * dragon_gpu_advance_steps would have produced.
+ * dragon_gpu_batch_advance_steps every FP64 grid holds exactly the state its
+ * own dragon_gpu_advance_steps would have produced (mixed members: below).
  *
  * Supported members: 1D hydro grids (HLLC / HLLX or the exact solver) and 2D
- * MHD grids (HLLD / HLLX); all 1D members share one solver. No counterpart in
- * the reference (its batch is a loop over grids).
+ * MHD grids (HLLD / HLLX); all 1D members share one solver, and all members
+ * one precision: FP64 (dragon_config.precision 0) or mixed FP32/FP64 (1). A
+ * mixed batch's 1D members end exactly where their own mixed advance ends, its
+ * 2D MHD members to FP32 rounding of it (the compiler may fuse FP32
+ * multiply-adds differently in the batched kernel). No counterpart in the
+ * reference (its batch is a loop over grids).
  */
 #ifndef DRAGON_BATCH_H
 #define DRAGON_BATCH_H
@@ -30,7 +34,7 @@ typedef struct dragon_batch dragon_batch;
 /* Launch shape of the batched step, chosen by dragon_gpu_batch_autotune or
  * set by the caller. */
 typedef struct dragon_batch_tuning {
-    int tile_1d;      /* cells per 1D work item: 128 or 256 */
+    int tile_1d;      /* cells per 1D work item: 128 or 256 (FP64 batches; mixed: always 128) */
     int ctas_per_sm;  /* resident CTAs of the persistent kernel per SM (1..8, capped by occupancy) */
     int order;        /* queue order: 0 phase-major (all grids' phase k before phase k+1, 1D tiles after
                          the first MHD phase), 1 1D grids first, 2 largest grids first within each phase */

@@ -1,4 +1,4 @@
-"""The mixed FP32/FP64 2D hydro and 2D MHD paths against the FP64 oracle.
+"""The mixed FP32/FP64 1D hydro, 2D hydro and 2D MHD paths against the FP64 oracle.
 
 The mixed path runs reconstruction, limiters, the Riemann solves and the CTU
 corrections in FP32 while the state, every pressure recovery, the
@@ -79,9 +79,47 @@ def test_mixed_sod_strong_shock_stays_physical():
     assert np.all(np.isfinite(G.w)) and np.all(l1 <= TOL_MIXED), l1
 
 
-def test_mixed_only_on_2d_grids():
+def test_mixed_only_on_1d_hydro_and_2d_grids():
     with pytest.raises(dg.grid._lib.DragonGPUError):
         dg.Grid3D(4, 4, 4, 0.1, 0.1, 0.1, config=dg.Config(precision=dg.PREC_MIXED))
+    with pytest.raises(dg.grid._lib.DragonGPUError):
+        dg.Grid1D(16, 1 / 16, config=dg.Config(mhd=True, precision=dg.PREC_MIXED))
+
+
+# The 1D two-state problems of the reference's Examples/1D (rho, u, p left /
+# right): Sod, Lax, a strong shock (pressure ratio 1e5), and a 1-2-3 double
+# rarefaction (Toro's test 2).
+RIEMANN_1D = {
+    "sod": ((1.0, 0.0, 1.0), (0.125, 0.0, 0.1)),
+    "lax": ((0.445, 0.698, 3.528), (0.5, 0.0, 0.571)),
+    "strong": ((1.0, 0.0, 1000.0), (1.0, 0.0, 0.01)),
+    "123": ((1.0, -2.0, 0.4), (1.0, 2.0, 0.4)),
+}
+
+
+@pytest.mark.parametrize("case", list(RIEMANN_1D))
+@pytest.mark.parametrize("riemann,limiter", [(dg.RIEMANN_HLLC, dg.LIMITER_MINMOD), (dg.RIEMANN_EXACT, dg.LIMITER_MC),
+                                             (dg.RIEMANN_HLLE, dg.LIMITER_VANLEER)])
+def test_mixed_1d_riemann_l1_vs_fp64_oracle(case, riemann, limiter):
+    """1D mixed sweep against the reference to t = 0.1 (512 cells, outflow):
+    rho, p and u within the mixed bar; vy and vz stay exactly zero."""
+    n = 512
+    left, right = RIEMANN_1D[case]
+    w0, dx = problems.riemann_1d(n, left, right, ghosts=2)
+    G = dg.Grid1D(n, dx, ghosts=2, config=dg.Config(riemann=riemann, limiter=limiter, precision=dg.PREC_MIXED))
+    R = oracle_grid(dim=1, n=(n,), d=(dx,), ghosts=2, riemann=riemann, limiter=limiter)
+    G.w[...] = w0
+    R.set_prim(w0)
+    t = 0.1 if case != "strong" else 0.004
+    R.advance(t)
+    res = G.advance(t)
+    assert res.steps > 20
+    g = 2
+    ref = R.get_prim()[g:-g]
+    l1 = problems.rel_l1(G.w[g:-g], ref)
+    assert np.all(np.isfinite(G.w)) and np.all(l1[:3] <= TOL_MIXED), l1
+    assert np.all(G.w[g:-g, 3:] == 0.0)
+    assert np.any(G.w[g:-g] != ref)  # really the FP32 path
 
 
 def divb_max(B, g, n, dx, dy):
