@@ -4,7 +4,7 @@ profiling and quick checks on a GPU):
     python -m dragon_b200.workloads kh      --n 1024 --steps 5 [--mixed]
     python -m dragon_b200.workloads ot      --n 512  --steps 5 [--mixed]
     python -m dragon_b200.workloads blast3d --n 128  --steps 3 [--riemann exact] [--mhd]
-    python -m dragon_b200.workloads batch   --n1d 256 --n2d 32 --steps 5
+    python -m dragon_b200.workloads batch   --n1d 256 --n2d 32 --steps 5 [--mixed]
 
 kh: 2D shear layer (HLLC, van Leer, periodic); ot: 2D MHD Orszag-Tang (HLLD,
 MC, CT, periodic); blast3d: 3D blast (MC, outflow; HLLC by default, or the
@@ -63,16 +63,18 @@ def blast3d(n, riemann, mhd):
     return G
 
 
-def batch(n1d, n2d):
+def batch(n1d, n2d, mixed=False):
     one, two = problems.batch_instances(n1d=n1d, n2d=n2d)
+    prec = _grid.PREC_MIXED if mixed else _grid.PREC_FP64
     grids = []
     for spec in one:
-        G = _grid.Grid1D(spec["n"], spec["dx"], ghosts=2, config=_grid.Config(riemann=_grid.RIEMANN_HLLX))
+        G = _grid.Grid1D(spec["n"], spec["dx"], ghosts=2, config=_grid.Config(riemann=_grid.RIEMANN_HLLX,
+                                                                                precision=prec))
         G.w[...] = spec["w"]
         grids.append(G)
     for spec in two:
         n = spec["n"]
-        G = _grid.Grid2D(n, n, spec["dx"], spec["dx"], ghosts=3, config=_grid.Config(mhd=True))
+        G = _grid.Grid2D(n, n, spec["dx"], spec["dx"], ghosts=3, config=_grid.Config(mhd=True, precision=prec))
         G.w[...] = spec["w"]
         G.B[...] = spec["B"]
         G.boundary = Periodic()
@@ -95,7 +97,7 @@ def main(argv=None):
     rs = {"hllc": _grid.RIEMANN_HLLC, "exact": _grid.RIEMANN_EXACT, "hll": _grid.RIEMANN_HLL,
           "hlle": _grid.RIEMANN_HLLE, "roe": _grid.RIEMANN_ROE}[a.riemann]
     if a.workload == "batch":
-        b, grids = batch(a.n1d, a.n2d)
+        b, grids = batch(a.n1d, a.n2d, a.mixed)
         b.advance_steps(1)
         t = time.perf_counter()
         st = b.advance_steps(a.steps)

@@ -22,7 +22,9 @@ itself for 2D MC n = 128, the device path, which is the reference's
 arithmetic bit for bit, for all of them). The small-size runs below are the
 reference's own output.
 
-Run: python tests/golden/make_convergence.py
+Run: python tests/golden/make_convergence.py, then
+     python tests/golden/make_convergence.py --large   (adds the 3D diagonal wave
+     at n = 64, about 45 minutes of one core)
 """
 import json
 import os
@@ -97,6 +99,12 @@ def loop(dim, n, gaussian):
     return problems.loop_errors(R.get_prim(), w0, n, R.ghosts)
 
 
+# Cases that take the reference most of an hour on one core, run with --large
+# and merged into an existing convergence.json.
+LARGE = [
+    ("diagonal", "3d_mc", 64, lambda: diagonal(3, 64, "mc")),
+]
+
 SMALL = [
     ("diagonal", "2d_mc", 32, lambda: diagonal(2, 32, "mc")),
     ("diagonal", "2d_minmod", 32, lambda: diagonal(2, 32, "minmod")),
@@ -111,14 +119,21 @@ SMALL = [
 
 def main():
     assert refgrid.available("hydro") and refgrid.available("mhd_rt"), "build oracle/_ref first"
-    out = {"published": {}, "reproduced": REPRODUCED, "reference": {}}
-    for study, rows in PUBLISHED.items():
-        out["published"][study] = {k: {str(n): v for n, v in r.items()} for k, r in rows.items()}
-    for study, case, n, fn in SMALL:
+    path = os.path.join(HERE, "convergence.json")
+    if "--large" in sys.argv:
+        with open(path) as f:
+            out = json.load(f)
+        cases = LARGE
+    else:
+        out = {"published": {}, "reproduced": REPRODUCED, "reference": {}}
+        for study, rows in PUBLISHED.items():
+            out["published"][study] = {k: {str(n): v for n, v in r.items()} for k, r in rows.items()}
+        cases = SMALL
+    for study, case, n, fn in cases:
         norms = fn()
         out["reference"].setdefault(study, {}).setdefault(case, {})[str(n)] = norms
         print(study, case, n, norms, flush=True)
-    with open(os.path.join(HERE, "convergence.json"), "w") as f:
+    with open(path, "w") as f:
         json.dump(out, f, indent=1)
 
 
