@@ -504,7 +504,8 @@ def _batch_run(precision, steps, one_by_one_steps):
               "work_items_per_step": st["work_items"], "graph_replays": st["graph_replays"],
               "retries": st["retries"], "spin_timeouts": st["spin_timeouts"],
               "tuning": {"tile_1d": tune.tile_1d, "ctas_per_sm": tune.ctas_per_sm, "order": tune.order,
-                         "graph_steps": tune.graph_steps, "mhd_tiles": tune.mhd_tiles}, "autotune_seconds": tune_s}
+                         "graph_steps": tune.graph_steps, "mhd_tiles": tune.mhd_tiles, "wave": tune.wave},
+              "autotune_seconds": tune_s}
     return report, grids
 
 

@@ -90,7 +90,7 @@ class BatchTuning(ctypes.Structure):
     """dragon_batch_tuning (include/dragon_batch.h)."""
 
     _fields_ = [("tile_1d", ctypes.c_int), ("ctas_per_sm", ctypes.c_int), ("order", ctypes.c_int),
-                ("graph_steps", ctypes.c_int), ("mhd_tiles", ctypes.c_int)]
+                ("graph_steps", ctypes.c_int), ("mhd_tiles", ctypes.c_int), ("wave", ctypes.c_int)]
 
 
 class BatchStats(ctypes.Structure):

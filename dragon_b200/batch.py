@@ -14,7 +14,7 @@ from dataclasses import dataclass
 
 from . import _lib
 
-ORDER_PHASE_MAJOR, ORDER_1D_FIRST, ORDER_LARGEST_FIRST = 0, 1, 2
+ORDER_PHASE_MAJOR, ORDER_1D_FIRST, ORDER_LARGEST_FIRST, ORDER_WAVEFRONT = 0, 1, 2, 3
 
 
 @dataclass
@@ -24,13 +24,15 @@ class Tuning:
     order: int = ORDER_PHASE_MAJOR
     graph_steps: int = 32
     mhd_tiles: int = 8       # 32 x 8 tiles of a 2D MHD phase per work item
+    wave: int = 1            # ORDER_WAVEFRONT: 2D MHD grids per wavefront group
 
     def to_c(self):
-        return _lib.BatchTuning(self.tile_1d, self.ctas_per_sm, self.order, self.graph_steps, self.mhd_tiles)
+        return _lib.BatchTuning(self.tile_1d, self.ctas_per_sm, self.order, self.graph_steps, self.mhd_tiles,
+                                self.wave)
 
     @staticmethod
     def from_c(t):
-        return Tuning(t.tile_1d, t.ctas_per_sm, t.order, t.graph_steps, t.mhd_tiles or 1)
+        return Tuning(t.tile_1d, t.ctas_per_sm, t.order, t.graph_steps, t.mhd_tiles or 1, t.wave or 1)
 
 
 class Batch:

@@ -69,7 +69,7 @@ StepKernel pick_kernel(int s1d, int tile) {
 
 struct dragon_batch {
     std::vector<dragon_grid*> members;
-    dragon_batch_tuning tune{256, 0, 0, 32, 8};
+    dragon_batch_tuning tune{256, 0, 0, 32, 8, 1};
     int s1d = -1;
     int prec = -1;  // the members' precision (0 FP64, 1 mixed)
     cudaStream_t stream = nullptr;
@@ -158,7 +158,7 @@ BatchInst make_inst(dragon_grid* h, int tile, int group, bool mixed) {
     return I;
 }
 
-std::vector<WorkItem> make_queue(const std::vector<BatchInst>& insts, int order) {
+std::vector<WorkItem> make_queue(const std::vector<BatchInst>& insts, int order, int wave) {
     std::vector<int> idx(insts.size());
     for (size_t i = 0; i < idx.size(); i++) idx[i] = (int)i;
     auto cells = [&](int i) {
@@ -179,6 +179,27 @@ std::vector<WorkItem> make_queue(const std::vector<BatchInst>& insts, int order)
         for (int p = 0; p < kPhases; p++) emit_kind_phase(KMHD2D, p);
         return q;
     }
+    if (order == 3) {
+        // wavefront: diagonal t holds phase p of MHD group t - p, so a group's
+        // phases follow one another one diagonal apart; every item of a
+        // member's phase p - 1 sits on an earlier diagonal than its phase p
+        for (int p = 0; p < kPhases; p++) emit_kind_phase(K1D, p);
+        std::vector<std::vector<int>> groups;
+        for (int i : idx) {
+            if (insts[i].kind != KMHD2D) continue;
+            if (groups.empty() || (int)groups.back().size() >= wave) groups.emplace_back();
+            groups.back().push_back(i);
+        }
+        const int ng = (int)groups.size();
+        for (int t = 0; t < ng + kPhases - 1; t++)
+            for (int p = kPhases - 1; p >= 0; p--) {
+                const int g = t - p;
+                if (g < 0 || g >= ng) continue;
+                for (int i : groups[g])
+                    if (p <= insts[i].last_phase) emit(i, p);
+            }
+        return q;
+    }
     // phase-major; the 1D steps sit after the MHD copies so that they fill
     // the gaps of the MHD phase chain
     for (int i : idx) emit(i, 0);
@@ -197,7 +218,7 @@ int build(dragon_batch* b) {
     insts.reserve(n);
     const bool mixed = b->prec == 1;
     for (dragon_grid* h : b->members) insts.push_back(make_inst(h, b->tune.tile_1d, b->tune.mhd_tiles, mixed));
-    const std::vector<WorkItem> q = make_queue(insts, b->tune.order);
+    const std::vector<WorkItem> q = make_queue(insts, b->tune.order, std::max(1, b->tune.wave));
     b->nitems = (int)q.size();
     b->ctr_words = kCtrDone + (size_t)kPhases * n;
     CKB(cudaMalloc(&b->d_insts, sizeof(BatchInst) * n));
@@ -391,11 +412,13 @@ int dragon_gpu_batch_size(const dragon_batch* b) { return b ? (int)b->members.si
 int dragon_gpu_batch_set_tuning(dragon_batch* b, const dragon_batch_tuning* t) {
     if (!b || !t) return fail(DRAGON_GPU_EINVAL, "null argument");
     if ((t->tile_1d != 128 && t->tile_1d != 256) || t->ctas_per_sm < 0 || t->ctas_per_sm > 8 || t->order < 0 ||
-        t->order > 2 || t->graph_steps < 1 || t->graph_steps > 1024 ||
-        !(t->mhd_tiles == 0 || t->mhd_tiles == 1 || t->mhd_tiles == 2 || t->mhd_tiles == 4 || t->mhd_tiles == 8))
+        t->order > 3 || t->graph_steps < 1 || t->graph_steps > 1024 ||
+        !(t->mhd_tiles == 0 || t->mhd_tiles == 1 || t->mhd_tiles == 2 || t->mhd_tiles == 4 || t->mhd_tiles == 8) ||
+        t->wave < 0 || t->wave > 64)
         return fail(DRAGON_GPU_EINVAL, "invalid batch tuning");
     b->tune = *t;
     if (b->tune.mhd_tiles == 0) b->tune.mhd_tiles = 1;
+    if (b->tune.wave == 0) b->tune.wave = 1;
     b->dirty = true;
     return 0;
 }
@@ -479,21 +502,31 @@ int dragon_gpu_batch_autotune(dragon_batch* b, int steps, dragon_batch_tuning* b
         return 0;
     };
     // launch shape and queue order with one MHD tile per item, then the MHD
-    // tiles per item for the best of those
+    // tiles per item for the best of those, then the wavefront order
     for (int tile : {128, 256})
         for (int per_sm : {1, 2, 4, 8})
             for (int order : {0, 1, 2})
-                if (!rc) rc = trial(dragon_batch_tuning{tile, per_sm, order, steps, 1});
+                if (!rc) rc = trial(dragon_batch_tuning{tile, per_sm, order, steps, 1, 1});
     const dragon_batch_tuning base = win;
     bool any_mhd = false;
     for (dragon_grid* h : b->members) any_mhd |= h->dim == 2;
-    if (any_mhd)
+    if (any_mhd) {
         for (int group : {2, 4, 8})
             if (!rc) {
                 dragon_batch_tuning t = base;
                 t.mhd_tiles = group;
                 rc = trial(t);
             }
+        // the wavefront order over MHD groups of a few sizes, with the best shape so far
+        const dragon_batch_tuning shaped = win;
+        for (int wave : {1, 4, 16})
+            if (!rc) {
+                dragon_batch_tuning t = shaped;
+                t.order = 3;
+                t.wave = wave;
+                rc = trial(t);
+            }
+    }
     free_snaps();
     win.graph_steps = keep.graph_steps;
     b->tune = win;

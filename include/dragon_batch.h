@@ -37,9 +37,13 @@ typedef struct dragon_batch_tuning {
     int tile_1d;      /* cells per 1D work item: 128 or 256 (FP64 batches; mixed: always 128) */
     int ctas_per_sm;  /* resident CTAs of the persistent kernel per SM (1..8, capped by occupancy) */
     int order;        /* queue order: 0 phase-major (all grids' phase k before phase k+1, 1D tiles after
-                         the first MHD phase), 1 1D grids first, 2 largest grids first within each phase */
+                         the first MHD phase), 1 1D grids first, 2 largest grids first within each phase,
+                         3 wavefront: 1D grids first, then the 2D MHD grids in groups of `wave`, group g's
+                         phase k queued with group g+1's phase k-1 (a group's intermediates are reused
+                         while they are still in L2) */
     int graph_steps;  /* steps captured per CUDA graph */
     int mhd_tiles;    /* 32 x 8 tiles of a 2D MHD phase per work item: 1, 2, 4 or 8 (0 reads as 1; default 8) */
+    int wave;         /* order 3: 2D MHD grids per wavefront group, 1..64 (0 reads as 1) */
 } dragon_batch_tuning;
 
 typedef struct dragon_batch_stats {

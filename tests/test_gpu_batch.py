@@ -59,9 +59,10 @@ def assert_same(a, b):
             np.testing.assert_array_equal(b1, b2)
 
 
-@pytest.mark.parametrize("tile,order,per_sm,group", [(256, 0, 0, 1), (128, 1, 1, 1), (256, 2, 2, 1), (256, 0, 0, 2),
-                                                     (128, 2, 1, 4), (256, 1, 2, 8)])
-def test_batch_matches_single_grid_advance(workload, tile, order, per_sm, group):
+@pytest.mark.parametrize("tile,order,per_sm,group,wave", [(256, 0, 0, 1, 1), (128, 1, 1, 1, 1), (256, 2, 2, 1, 1),
+                                                          (256, 0, 0, 2, 1), (128, 2, 1, 4, 1), (256, 1, 2, 8, 1),
+                                                          (256, 3, 2, 8, 1), (128, 3, 0, 2, 3)])
+def test_batch_matches_single_grid_advance(workload, tile, order, per_sm, group, wave):
     one, two = workload
     steps = 9
     ref = make_grids(one, two)
@@ -69,7 +70,7 @@ def test_batch_matches_single_grid_advance(workload, tile, order, per_sm, group)
         G.advance_steps(steps)
     grids = make_grids(one, two)
     b = batch.Batch(grids)
-    b.tuning = batch.Tuning(tile_1d=tile, ctas_per_sm=per_sm, order=order, graph_steps=4, mhd_tiles=group)
+    b.tuning = batch.Tuning(tile_1d=tile, ctas_per_sm=per_sm, order=order, graph_steps=4, mhd_tiles=group, wave=wave)
     st = b.advance_steps(steps)
     assert st["spin_timeouts"] == 0 and st["graph_replays"] >= 3
     assert_same(states(grids), states(ref))
@@ -97,7 +98,7 @@ def test_autotune_keeps_states(workload):
     before = states(grids)
     b = batch.Batch(grids)
     t, ms = b.autotune(2)
-    assert ms > 0 and t.tile_1d in (128, 256) and t.order in (0, 1, 2)
+    assert ms > 0 and t.tile_1d in (128, 256) and t.order in (0, 1, 2, 3)
     assert_same(states(grids), before)
     ref = make_grids(one, two)
     for G in ref:
@@ -119,8 +120,8 @@ TOL_MIXED = 1e-5
 TOL_MIXED_BATCH_MHD = 1e-6  # relative L1, mixed batch vs single-grid mixed, 9 steps
 
 
-@pytest.mark.parametrize("tile,order,per_sm,group", [(256, 0, 0, 1), (128, 2, 1, 8)])
-def test_mixed_batch_matches_single_grid_mixed_advance(workload, tile, order, per_sm, group):
+@pytest.mark.parametrize("tile,order,per_sm,group,wave", [(256, 0, 0, 1, 1), (128, 2, 1, 8, 1), (256, 3, 2, 8, 2)])
+def test_mixed_batch_matches_single_grid_mixed_advance(workload, tile, order, per_sm, group, wave):
     one, two = workload
     steps = 9
     ref = make_grids(one, two, precision=dg.PREC_MIXED)
@@ -128,7 +129,7 @@ def test_mixed_batch_matches_single_grid_mixed_advance(workload, tile, order, pe
         G.advance_steps(steps)
     grids = make_grids(one, two, precision=dg.PREC_MIXED)
     b = batch.Batch(grids)
-    b.tuning = batch.Tuning(tile_1d=tile, ctas_per_sm=per_sm, order=order, graph_steps=4, mhd_tiles=group)
+    b.tuning = batch.Tuning(tile_1d=tile, ctas_per_sm=per_sm, order=order, graph_steps=4, mhd_tiles=group, wave=wave)
     st = b.advance_steps(steps)
     assert st["spin_timeouts"] == 0
     for G, R in zip(grids, ref):
