@@ -10,9 +10,9 @@
 //
 // One tile of TS cells per call: the single-grid sweep (step1d_mixed.cu) runs
 // one tile per CTA, the batched step (batch_mixed.cu) runs tiles as work
-// items. Translation units including this header are compiled with FMA
-// contraction and fast single-precision division / square root, so both run
-// the same arithmetic.
+// items; both translation units are compiled with FMA contraction and fast
+// single-precision division / square root, and both run the same arithmetic
+// (batch.cu includes this header for the FP64 batch, which never runs it).
 #pragma once
 
 #include "mixed.cuh"

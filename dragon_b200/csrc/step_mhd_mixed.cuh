@@ -12,9 +12,10 @@
 //     fluxes.
 // Each phase is a device body over one 32 x 8 tile (Tile2): the single-grid
 // step (step_mhd_mixed.cu) runs one tile per CTA, the batched step
-// (batch_mixed.cu) runs tiles as work items. Translation units that include
-// this header are compiled with FMA contraction and fast single-precision
-// division / square root. Where the compiler fuses a multiply into an add
+// (batch_mixed.cu) runs tiles as work items; both translation units are
+// compiled with FMA contraction and fast single-precision division / square
+// root (batch.cu includes this header for the FP64 batch, which never runs
+// these bodies). Where the compiler fuses a multiply into an add
 // depends on the code a body is inlined into, so the two kernels can round an
 // FP32 value differently (kept inline: out of line, the single-grid step ran
 // 21 % slower).
