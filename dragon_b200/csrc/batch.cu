@@ -142,10 +142,9 @@ BatchInst make_inst(dragon_grid* h, int tile, int group, bool mixed) {
         return I;
     }
     const int nx = h->n[0], ny = h->n[1];
-    I.wcount = 8 * h->cg.plane;
-    I.bcount = 3 * h->fg.plane;
+    I.frame = mhd2d_frame_points(h->cg);
     I.last_phase = 8;
-    I.ntiles[1] = (int)((I.wcount + I.bcount + kCopyChunk - 1) / kCopyChunk);
+    I.ntiles[1] = (int)std::max<long long>(1, (I.frame + kCopyChunk - 1) / kCopyChunk);
     I.ntj[1] = 1;
     // the seven sweeps of the single-grid step and their cell ranges
     const int ext[7] = {4, 4, 3, 2, 2, 1, 0};

@@ -15,7 +15,8 @@
 //                arithmetic of the single-grid prologue)
 //   1D hydro     phase 1: step tiles of tile_1d cells (mixed: kMx1dTile cells,
 //                the single-grid mixed sweep's tiling)
-//   2D MHD       phase 1: copy of the state and face B into the output buffer,
+//   2D MHD       phase 1: copy of the ghost frame of the state and face B into
+//                the output buffers (mhd2d_copy_frame),
 //                phases 2-8: the seven phases of the single-grid step, one
 //                or more 32 x 8 cell tiles per item
 // A CTA takes the next item from a global counter, waits until every item of
@@ -42,7 +43,7 @@ using namespace dgpu;
 
 constexpr int kPhases = 9;
 constexpr int kThreads = 256;
-constexpr int kCopyChunk = kThreads * 16;     // doubles per copy item
+constexpr int kCopyChunk = kThreads * 16;     // ghost-frame points per copy item
 constexpr long long kSpinLimit = 1LL << 24;   // polls of a dependency wait (each >= 64 ns)
 enum Kind : int { K1D = 0, KMHD2D = 1 };
 
@@ -61,7 +62,7 @@ struct BatchInst {
     const BCEntry* bcs;
     StepArgs sa;
     PrologueArgs pa;
-    long long wcount, bcount;  // doubles of the state / face B copied by phase 1 (MHD)
+    long long frame;         // ghost-frame points copied by phase 1 (MHD, mhd2d_frame_points)
 };
 
 struct WorkItem {
@@ -126,11 +127,8 @@ __device__ __forceinline__ void run_item(const BatchInst& I, const WorkItem& wi,
     if (wi.phase == 1) {
         if (ldv(&I.ctl->err) | ldv(&I.ctl->done)) return;
         const long long base = (long long)wi.tile * kCopyChunk;
-        const long long end = base + kCopyChunk < I.wcount + I.bcount ? base + kCopyChunk : I.wcount + I.bcount;
-        for (long long e = base + threadIdx.x; e < end; e += blockDim.x) {
-            if (e < I.wcount) I.w[cur ^ 1][e] = I.w[cur][e];
-            else I.B[cur ^ 1][e - I.wcount] = I.B[cur][e - I.wcount];
-        }
+        const long long end = base + kCopyChunk < I.frame ? base + kCopyChunk : I.frame;
+        mhd2d_copy_frame(I.G, I.FG, I.w[cur], I.w[cur ^ 1], I.B[cur], I.B[cur ^ 1], base, end, threadIdx.x, blockDim.x);
         return;
     }
     const int nbx = I.ntj[wi.phase];

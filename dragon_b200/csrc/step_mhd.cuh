@@ -16,6 +16,8 @@
 // arithmetic (and every failure) is the reference's.
 #pragma once
 
+#include <algorithm>
+
 #include "grid.cuh"
 #include "recon.cuh"
 #include "riemann.cuh"
@@ -405,6 +407,109 @@ __device__ __forceinline__ void mhd2d_update(const Mhd2DArgs& A, const Tile2& T)
     }
 }
 
+// The ghost frame of the 2D MHD step's output buffers: every cell and face the
+// update phase does not write, copied from the inputs so the committed arrays
+// keep the ghosts the prologue filled (the reference commits the interior
+// only, Unsplit.cpp:104-107). The update writes cells [0, nx) x [0, ny),
+// x faces [0, nx] x [0, ny), y faces [0, nx) x [0, ny] and the cell-centred
+// Bz [0, nx) x [0, ny); the frame is the rest of each padded array, about
+// 4 g (n + g) points per array instead of the whole array.
+
+// Point k of the frame of the box [bi0, bi1) x [bj0, bj1) inside the padded
+// range [lo_i, hi_i) x [lo_j, hi_j): the rows above and below the box, then
+// the columns left and right of it. False past the last point.
+__device__ __forceinline__ bool frame_point(long long k, int lo_i, int hi_i, int lo_j, int hi_j, int bi0, int bi1,
+                                            int bj0, int bj1, int& i, int& j) {
+    const long long W = hi_j - lo_j;
+    const long long top = (long long)(bi0 - lo_i) * W;
+    if (k < top) {
+        i = lo_i + (int)(k / W);
+        j = lo_j + (int)(k % W);
+        return true;
+    }
+    k -= top;
+    const long long bot = (long long)(hi_i - bi1) * W;
+    if (k < bot) {
+        i = bi1 + (int)(k / W);
+        j = lo_j + (int)(k % W);
+        return true;
+    }
+    k -= bot;
+    const int sl = bj0 - lo_j, side = sl + (hi_j - bj1);
+    if (side <= 0 || k >= (long long)(bi1 - bi0) * side) return false;
+    i = bi0 + (int)(k / side);
+    const int c = (int)(k % side);
+    j = c < sl ? lo_j + c : bj1 + (c - sl);
+    return true;
+}
+
+__device__ __forceinline__ long long frame_count(int lo_i, int hi_i, int lo_j, int hi_j, int bi0, int bi1, int bj0,
+                                                 int bj1) {
+    return (long long)(hi_i - lo_i) * (hi_j - lo_j) - (long long)(bi1 - bi0) * (bj1 - bj0);
+}
+
+// Frame points of the cells and of the three face-B components, in that order.
+__host__ __device__ __forceinline__ long long mhd2d_frame_points(const Geo& G) {
+    const long long nx = G.n[0], ny = G.n[1], g = G.g;
+    const long long cells = (nx + 2 * g) * (ny + 2 * g) - nx * ny;
+    const long long faces = (nx + 1 + 2 * g) * (ny + 1 + 2 * g);
+    return cells + (faces - (nx + 1) * ny) + (faces - nx * (ny + 1)) + (faces - nx * ny);
+}
+
+// Copies frame points [k0, k1) (of mhd2d_frame_points) with the calling
+// threads: thread tid of nthr.
+__device__ __forceinline__ void mhd2d_copy_frame(const Geo& G, const Geo& FG, const double* __restrict__ w,
+                                                 double* __restrict__ wout, const double* __restrict__ B,
+                                                 double* __restrict__ Bout, long long k0, long long k1, long long tid,
+                                                 long long nthr) {
+    const int nx = G.n[0], ny = G.n[1], g = G.g;
+    const long long nc = frame_count(-g, nx + g, -g, ny + g, 0, nx, 0, ny);
+    const long long nf0 = frame_count(-g, nx + 1 + g, -g, ny + 1 + g, 0, nx + 1, 0, ny);
+    const long long nf1 = frame_count(-g, nx + 1 + g, -g, ny + 1 + g, 0, nx, 0, ny + 1);
+    for (long long k = k0 + tid; k < k1; k += nthr) {
+        int i, j;
+        if (k < nc) {
+            if (!frame_point(k, -g, nx + g, -g, ny + g, 0, nx, 0, ny, i, j)) continue;
+            const long long m = gidx2(G, i, j);
+#pragma unroll
+            for (int f = 0; f < 8; f++) wout[f * G.plane + m] = w[f * G.plane + m];
+            continue;
+        }
+        long long q = k - nc;
+        int comp;
+        bool ok;
+        if (q < nf0) {
+            comp = 0;
+            ok = frame_point(q, -g, nx + 1 + g, -g, ny + 1 + g, 0, nx + 1, 0, ny, i, j);
+        } else if ((q -= nf0) < nf1) {
+            comp = 1;
+            ok = frame_point(q, -g, nx + 1 + g, -g, ny + 1 + g, 0, nx, 0, ny + 1, i, j);
+        } else {
+            q -= nf1;
+            comp = 2;
+            ok = frame_point(q, -g, nx + 1 + g, -g, ny + 1 + g, 0, nx, 0, ny, i, j);
+        }
+        if (!ok) continue;
+        const long long m = comp * FG.plane + gidx2(FG, i, j);
+        Bout[m] = B[m];
+    }
+}
+
+static __global__ void k_mhd2d_copy_frame(Geo G, Geo FG, const double* __restrict__ w, double* __restrict__ wout,
+                                          const double* __restrict__ B, double* __restrict__ Bout) {
+    mhd2d_copy_frame(G, FG, w, wout, B, Bout, 0, mhd2d_frame_points(G), blockIdx.x * (long long)blockDim.x + threadIdx.x,
+                     (long long)gridDim.x * blockDim.x);
+}
+
+// Enqueues the frame copy of a single-grid step.
+inline int launch_mhd2d_copy_frame(const Geo& G, const Geo& FG, const double* w, double* wout, const double* B,
+                                   double* Bout, cudaStream_t st) {
+    const long long n = mhd2d_frame_points(G);
+    const int blocks = (int)std::min<long long>((n + 255) / 256, 148 * 8);
+    k_mhd2d_copy_frame<<<blocks, 256, 0, st>>>(G, FG, w, wout, B, Bout);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
 // Kernels of the single-grid step: one 32 x 8 tile per CTA.
 static __global__ void k_mhd2d_halfstates(Mhd2DArgs A) { mhd2d_halfstates(A, launch_tile()); }
 // The flux kernels carry two CTAs per SM (<= 128 registers): at their natural
@@ -418,9 +523,8 @@ __global__ void __launch_bounds__(256, 2) k_mhd2d_final_flux(Mhd2DArgs A) { mhd2
 static __global__ void k_mhd2d_efinal(Mhd2DArgs A) { mhd2d_efinal(A, launch_tile()); }
 static __global__ void k_mhd2d_update(Mhd2DArgs A) { mhd2d_update(A, launch_tile()); }
 
-// 2D MHD CTU + CT step: the seven kernels in order. Ghost cells and faces of
-// the output buffers are first copied from the inputs (the reference commits
-// the interior only, Unsplit.cpp:104-107).
+// 2D MHD CTU + CT step: the seven kernels in order, after the ghost frame of
+// the output buffers is copied from the inputs (mhd2d_copy_frame).
 template <int SOLVER>
 inline int launch_step2d_mhd_t(const Geo& G, const Geo& FG, const double* w, double* wout, const double* B, double* Bout,
                              const MhdScratch& S, StepCtl* ctl, const StepArgs& sa, cudaStream_t st) {
@@ -428,8 +532,7 @@ inline int launch_step2d_mhd_t(const Geo& G, const Geo& FG, const double* w, dou
     const dim3 blk(kTileJ, kTileI);
     auto grid_for = [&](int ni, int nj) { return dim3((nj + kTileJ - 1) / kTileJ, (ni + kTileI - 1) / kTileI); };
     const int nx = G.n[0], ny = G.n[1];
-    if (cudaMemcpyAsync(wout, w, sizeof(double) * 8 * G.plane, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return 1;
-    if (cudaMemcpyAsync(Bout, B, sizeof(double) * 3 * FG.plane, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return 1;
+    if (launch_mhd2d_copy_frame(G, FG, w, wout, B, Bout, st)) return 1;
     k_mhd2d_halfstates<<<grid_for(nx + 4, ny + 4), blk, 0, st>>>(A);
     k_mhd2d_prelim<SOLVER><<<grid_for(nx + 4, ny + 4), blk, 0, st>>>(A);
     k_mhd2d_e0<<<grid_for(nx + 3, ny + 3), blk, 0, st>>>(A);

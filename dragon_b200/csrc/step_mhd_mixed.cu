@@ -23,8 +23,7 @@ int launch_mx(const Geo& G, const Geo& FG, const double* w, double* wout, const 
     const dim3 blk(kTileJ, kTileI);
     auto grid_for = [&](int ni, int nj) { return dim3((nj + kTileJ - 1) / kTileJ, (ni + kTileI - 1) / kTileI); };
     const int nx = G.n[0], ny = G.n[1];
-    if (cudaMemcpyAsync(wout, w, sizeof(double) * 8 * G.plane, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return 1;
-    if (cudaMemcpyAsync(Bout, B, sizeof(double) * 3 * FG.plane, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return 1;
+    if (launch_mhd2d_copy_frame(G, FG, w, wout, B, Bout, st)) return 1;
     k_mx_halfstates<<<grid_for(nx + 4, ny + 4), blk, 0, st>>>(A);
     k_mx_fluxes<SOLVER, false><<<grid_for(nx + 4, ny + 4), blk, 0, st>>>(A);
     k_mx_edges<false><<<grid_for(nx + 3, ny + 3), blk, 0, st>>>(A);
