@@ -2,7 +2,7 @@
 
 The mixed path runs reconstruction, limiters, the Riemann solves and the CTU
 corrections in FP32 while the state, every pressure recovery, the
-flux-difference accumulation and (MHD) the CT face update stay FP64. Its bar is the north-star one: <= 1e-5 relative L1 per field
+flux-difference accumulation and (MHD) the CT face update stay FP64. Its bar: <= 1e-5 relative L1 per field
 against the FP64 reference after the stated steps."""
 import numpy as np
 import pytest
