@@ -99,6 +99,32 @@ def test_mhd_blast_boundaries(bc):
     same(G.B, R.get_faceB(), f"blast faces {bc}")
 
 
+def test_mhd_blast_ignore_keeps_ghosts():
+    """Ignore on the x faces (Ignore.cpp): those ghost cells and faces are
+    never filled, so every step must carry them over from the state it read
+    (the step writes only the interior; its output buffers take the rest of
+    the input's cells and faces) exactly as the reference, which never
+    touches them."""
+    n = 24
+    g = 3
+    w0, B0, dx = problems.blast_2d_mhd(n, ghosts=g)
+    # ghosts start as copies of the nearest interior cell / face
+    w0 = np.pad(w0[g:g + n, g:g + n], ((g, g), (g, g), (0, 0)), mode="edge")
+    B0 = np.pad(B0[g:g + n + 1, g:g + n + 1], ((g, g), (g, g), (0, 0)), mode="edge")
+    b = dg.Ignore("X") + dg.Periodic("Y")
+    G, R = mhd_pair(w0, B0, n, dx, dx, b, limiter=dg.LIMITER_MC)
+    w_init, B_init = np.array(G.w), np.array(G.B)
+    R.advance(0.02)
+    res = G.advance(0.02)
+    assert res.steps > 1
+    same(G.w, R.get_prim(), "blast cells, ignore x")
+    same(G.B, R.get_faceB(), "blast faces, ignore x")
+    # the x ghost layers are exactly what initialize_B_fields left there
+    np.testing.assert_array_equal(G.w[:g, g:-g], w_init[:g, g:-g])
+    np.testing.assert_array_equal(G.w[-g:, g:-g], w_init[-g:, g:-g])
+    np.testing.assert_array_equal(G.B[:g, g:-g], B_init[:g, g:-g])
+
+
 def test_mhd_1d_hlld_sweep():
     """Brio-Wu-like shock tube through the 1D sweep with HLLD (cell B only)."""
     n = 256
