@@ -264,6 +264,7 @@ int retry_member(dragon_grid* h, int* retries) {
     const int c = C.cur;
     const int stage = (int)(C.err_key >> 56);
     if (stage == ST_CFL_ZERO) return fail(DRAGON_GPU_ECFL, stage_name(stage));
+    if (stage == ST_BARRIER) return fail(DRAGON_GPU_ECUDA, stage_name(stage));
     double t1 = C.t1;
     for (;;) {
         (*retries)++;

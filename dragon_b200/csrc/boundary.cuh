@@ -219,68 +219,35 @@ __device__ inline void bc_faces_axis(const Geo& FG, const int* ncell, double* __
     }
 }
 
-// Per-step prologue, one CTA: step bookkeeping of the previous step, ghost
-// fill, CFL over the ghost ring combined with the interior max the previous
-// step's epilogue produced, and this step's dt (CFL.cpp:188-213).
-// The body runs on one CTA of any size (a multiple of 32 threads); k_prologue
-// launches it alone, the batched step runs it as one work item.
+// Step bookkeeping of the previous step (CFL.cpp:188-213), by one thread:
+// returns non-zero when this step is not taken (failed or finished advance).
+__device__ __forceinline__ int prologue_bookkeeping(StepCtl* ctl, const PrologueArgs& pa) {
+    if (ctl->err) return 1;
+    if (ctl->done) return 1;
+    if (pa.bookkeeping) {
+        if (ctl->have_prev) {
+            ctl->remaining -= ctl->t1;
+            ctl->steps_done += 1;
+        }
+        ctl->have_prev = 1;
+        if (!(ctl->remaining > pa.tol) || (ctl->max_steps > 0 && ctl->steps_done >= ctl->max_steps)) {
+            ctl->done = 1;
+            return 1;
+        }
+    }
+    return 0;
+}
+
+// Max CFL signal speed over the one-cell ghost ring (CFL.cpp:91,110,125:
+// ng = min(1, ghosts)) of a 2D / 3D grid, ring points t0, t0 + stride, ...
 template <bool MHD>
-__device__ __forceinline__ void prologue_body(const Geo& G, const Geo& FG, double* __restrict__ w,
-                                              double* __restrict__ B, const BCEntry* __restrict__ bcs, StepCtl* ctl,
-                                              const PrologueArgs& pa) {
-    __shared__ int s_skip;
-    __shared__ double s_red[32];
-    if (threadIdx.x == 0) {
-        int skip = 0;
-        if (ctl->err) skip = 1;
-        else if (ctl->done) skip = 1;
-        else if (pa.bookkeeping) {
-            if (ctl->have_prev) {
-                ctl->remaining -= ctl->t1;
-                ctl->steps_done += 1;
-            }
-            ctl->have_prev = 1;
-            if (!(ctl->remaining > pa.tol) || (ctl->max_steps > 0 && ctl->steps_done >= ctl->max_steps)) {
-                ctl->done = 1;
-                skip = 1;
-            }
-        }
-        s_skip = skip;
-    }
-    __syncthreads();
-    if (s_skip) return;
-
-    if (pa.apply_bc) {
-        for (int e = pa.bc_first; e < pa.bc_first + pa.nbc; e++) {
-            const BCEntry be = bcs[e];
-            for (int a = 0; a < G.dim; a++) {
-                bc_cells_axis<MHD>(G, w, be, a, threadIdx.x, blockDim.x);
-                __syncthreads();
-            }
-            if constexpr (MHD) {
-                if (G.dim >= 2) {
-                    for (int a = 0; a < G.dim; a++) {
-                        bc_faces_axis(FG, G.n, B, be, a, threadIdx.x, blockDim.x);
-                        __syncthreads();
-                    }
-                }
-            }
-        }
-    }
-
-    if (!pa.compute_dt) return;
-    // CFL over the one-cell ghost ring (CFL.cpp:91,110,125: ng = min(1, ghosts)).
+__device__ __forceinline__ double ring_speed_max(const Geo& G, const double* __restrict__ w, const PrologueArgs& pa,
+                                                 long long t0, long long stride) {
     double m = 0.0;
-    if (G.dim == 1) {
-        if (threadIdx.x < 2) {
-            int i = threadIdx.x == 0 ? -1 : G.n[0];
-            Prim<double> W = load_prim<MHD>(w, G.plane, gidx1(G, i));
-            m = cfl_speed_1d<MHD>(W);
-        }
-    } else if (G.dim == 2) {
+    if (G.dim == 2) {
         const int nx = G.n[0], ny = G.n[1];
         const long long rows = 2LL * (ny + 2), total = rows + 2LL * nx;
-        for (long long r = threadIdx.x; r < total; r += blockDim.x) {
+        for (long long r = t0; r < total; r += stride) {
             int i, j;
             if (r < ny + 2) { i = -1; j = (int)r - 1; }
             else if (r < rows) { i = nx; j = (int)(r - (ny + 2)) - 1; }
@@ -297,7 +264,7 @@ __device__ __forceinline__ void prologue_body(const Geo& G, const Geo& FG, doubl
         const long long ey = ny + 2, ez = nz + 2;
         // ring = two i-slabs, then two j-strips per interior i, then two k-cells per interior (i,j)
         const long long nA = 2 * ey * ez, nB = (long long)nx * 2 * ez, nC = (long long)nx * ny * 2;
-        for (long long r = threadIdx.x; r < nA + nB + nC; r += blockDim.x) {
+        for (long long r = t0; r < nA + nB + nC; r += stride) {
             int i, j, k;
             if (r < nA) {
                 i = (r < ey * ez) ? -1 : nx;
@@ -321,29 +288,160 @@ __device__ __forceinline__ void prologue_body(const Geo& G, const Geo& FG, doubl
             m = speed_max(m, cfl_speed<MHD>(W, pa.cfl, pa.dx, pa.dy, pa.dz));
         }
     }
-    m = block_max(m, s_red);
-    if (threadIdx.x == 0) {
-        double inner = __longlong_as_double((long long)ctl->vmax[pa.slot_in]);
-        double maxs = speed_max(inner, m);
-        ctl->max_speed = maxs;
-        ctl->vmax[pa.slot_out] = 0ull;
-        if (ctl->check_cfl) {
-            if (maxs <= 0) {
-                record_error(ctl, ST_CFL_ZERO, 0);
-            } else {
-                double cfl_dt = (G.dim == 1) ? pa.cfl_coeff * pa.dx / maxs : pa.cfl_coeff / maxs;
-                ctl->t1 = smin(ctl->remaining, cfl_dt);
-            }
+    return m;
+}
+
+// This step's dt from the ring max m and the interior max of the previous
+// step's epilogue (CFL.cpp:98-137, 196), by one thread.
+__device__ __forceinline__ void prologue_set_dt(const Geo& G, StepCtl* ctl, const PrologueArgs& pa, double m) {
+    double inner = __longlong_as_double((long long)ctl->vmax[pa.slot_in]);
+    double maxs = speed_max(inner, m);
+    ctl->max_speed = maxs;
+    ctl->vmax[pa.slot_out] = 0ull;
+    if (ctl->check_cfl) {
+        if (maxs <= 0) {
+            record_error(ctl, ST_CFL_ZERO, 0);
         } else {
-            ctl->t1 = ctl->remaining;
+            double cfl_dt = (G.dim == 1) ? pa.cfl_coeff * pa.dx / maxs : pa.cfl_coeff / maxs;
+            ctl->t1 = smin(ctl->remaining, cfl_dt);
+        }
+    } else {
+        ctl->t1 = ctl->remaining;
+    }
+}
+
+// Per-step prologue, one CTA: step bookkeeping of the previous step, ghost
+// fill, CFL over the ghost ring combined with the interior max the previous
+// step's epilogue produced, and this step's dt (CFL.cpp:188-213).
+// The body runs on one CTA of any size (a multiple of 32 threads); k_prologue
+// launches it alone, the batched step runs it as one work item.
+template <bool MHD>
+__device__ __forceinline__ void prologue_body(const Geo& G, const Geo& FG, double* __restrict__ w,
+                                              double* __restrict__ B, const BCEntry* __restrict__ bcs, StepCtl* ctl,
+                                              const PrologueArgs& pa) {
+    __shared__ int s_skip;
+    __shared__ double s_red[32];
+    if (threadIdx.x == 0) s_skip = prologue_bookkeeping(ctl, pa);
+    __syncthreads();
+    if (s_skip) return;
+
+    if (pa.apply_bc) {
+        for (int e = pa.bc_first; e < pa.bc_first + pa.nbc; e++) {
+            const BCEntry be = bcs[e];
+            for (int a = 0; a < G.dim; a++) {
+                bc_cells_axis<MHD>(G, w, be, a, threadIdx.x, blockDim.x);
+                __syncthreads();
+            }
+            if constexpr (MHD) {
+                if (G.dim >= 2) {
+                    for (int a = 0; a < G.dim; a++) {
+                        bc_faces_axis(FG, G.n, B, be, a, threadIdx.x, blockDim.x);
+                        __syncthreads();
+                    }
+                }
+            }
         }
     }
+
+    if (!pa.compute_dt) return;
+    double m = 0.0;
+    if (G.dim == 1) {
+        if (threadIdx.x < 2) {
+            int i = threadIdx.x == 0 ? -1 : G.n[0];
+            Prim<double> W = load_prim<MHD>(w, G.plane, gidx1(G, i));
+            m = cfl_speed_1d<MHD>(W);
+        }
+    } else {
+        m = ring_speed_max<MHD>(G, w, pa, threadIdx.x, blockDim.x);
+    }
+    m = block_max(m, s_red);
+    if (threadIdx.x == 0) prologue_set_dt(G, ctl, pa, m);
 }
 
 template <bool MHD>
 __global__ void __launch_bounds__(1024) k_prologue(Geo G, Geo FG, double* __restrict__ w, double* __restrict__ B,
                                                    const BCEntry* __restrict__ bcs, StepCtl* ctl, PrologueArgs pa) {
     prologue_body<MHD>(G, FG, w, B, bcs, ctl, pa);
+}
+
+// Grid-wide barrier of a cooperative launch (every CTA resident). Bounded: a
+// wait that gives up records ST_BARRIER and returns false.
+constexpr long long kGridBarrierPolls = 1LL << 22;  // >= 32 ns each
+__device__ __forceinline__ bool grid_barrier(StepCtl* ctl) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* gen = &ctl->bar_gen;
+        const unsigned g0 = *gen;
+        __threadfence();
+        int ok = 1;
+        if (atomicAdd(&ctl->bar_arrive, 1u) == gridDim.x - 1) {
+            atomicExch(&ctl->bar_arrive, 0u);
+            __threadfence();
+            atomicAdd(&ctl->bar_gen, 1u);
+        } else {
+            long long polls = 0;
+            while (*gen == g0) {
+                if (++polls > kGridBarrierPolls) {
+                    ok = 0;
+                    record_error(ctl, ST_BARRIER, 0);
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// The prologue of a 2D / 3D grid as one cooperative launch: bookkeeping (CTA
+// 0), then every ghost-fill pass over the whole grid in the reference's order
+// (entry by entry, cells axis by axis, then faces axis by axis), then the
+// ring CFL max (a block max per CTA, an atomic max across them) and dt (CTA
+// 0), with a grid barrier between the stages. The same work as the one-CTA
+// prologue_body, spread over the grid.
+template <bool MHD>
+__global__ void __launch_bounds__(256) k_prologue_coop(Geo G, Geo FG, double* __restrict__ w, double* __restrict__ B,
+                                                      const BCEntry* __restrict__ bcs, StepCtl* ctl, PrologueArgs pa) {
+    __shared__ int s_skip;
+    __shared__ double s_red[32];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ctl->ring_bits = 0ull;
+        prologue_bookkeeping(ctl, pa);
+    }
+    if (!grid_barrier(ctl)) return;
+    if (threadIdx.x == 0) s_skip = *(const volatile int*)&ctl->err | *(const volatile int*)&ctl->done;
+    __syncthreads();
+    if (s_skip) return;
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nt = (long long)gridDim.x * blockDim.x;
+    if (pa.apply_bc) {
+        for (int e = pa.bc_first; e < pa.bc_first + pa.nbc; e++) {
+            const BCEntry be = bcs[e];
+            for (int a = 0; a < G.dim; a++) {
+                bc_cells_axis<MHD>(G, w, be, a, tid, nt);
+                if (!grid_barrier(ctl)) return;
+            }
+            if constexpr (MHD) {
+                if (G.dim >= 2) {
+                    for (int a = 0; a < G.dim; a++) {
+                        bc_faces_axis(FG, G.n, B, be, a, tid, nt);
+                        if (!grid_barrier(ctl)) return;
+                    }
+                }
+            }
+        }
+    }
+    if (!pa.compute_dt) return;
+    double m = ring_speed_max<MHD>(G, w, pa, tid, nt);
+    m = block_max(m, s_red);
+    if (threadIdx.x == 0) atomic_max_speed(&ctl->ring_bits, m);
+    if (!grid_barrier(ctl)) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        prologue_set_dt(G, ctl, pa, __longlong_as_double((long long)*(volatile unsigned long long*)&ctl->ring_bits));
 }
 
 // One ghost-fill pass (entry, axis; cells or faces) spread over a whole grid,

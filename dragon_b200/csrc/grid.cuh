@@ -55,6 +55,10 @@ struct StepCtl {
     // statistics (summed over all face solves of committed and failed steps)
     unsigned long long pivots_exact, hlld_to_hlle, newton_iters, exact_calls, trrs, muscl_first_order;
     unsigned long long cap_hits, guess_rejects, judge_reruns;
+    // grid barrier of the cooperative prologue (arrivals, generation) and its
+    // ghost-ring max CFL speed (bits of a non-negative double)
+    unsigned bar_arrive, bar_gen;
+    unsigned long long ring_bits;
     // interior max CFL speed (bits of a non-negative double): slots 0/1 ping-pong
     // with the state buffers, slot 2 is scratch for cfl_time. Kept last: the
     // host rewrites everything before it when a new advance starts.
@@ -68,6 +72,7 @@ enum ErrStage : int {
     ST_NAN = 3,           // non-finite conservative state in applyFluxes (Unsplit.cpp:267,284)
     ST_UNPHYSICAL = 4,    // unphysical committed state (Unsplit.cpp:97,192; Splitting.cpp:109)
     ST_CFL_ZERO = 5,      // max signal speed zero (CFL.cpp:102,117,134)
+    ST_BARRIER = 6,       // a grid barrier of the cooperative prologue gave up waiting
 };
 
 __device__ __forceinline__ void record_error(StepCtl* ctl, int stage, long long cell) {

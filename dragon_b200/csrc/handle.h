@@ -79,6 +79,8 @@ struct dragon_grid {
     dgpu::MlpNet* mlp_dev = nullptr;
     dragon_newton_stats ntot{};
     AdvanceState adv{};
+    // CTAs of the cooperative prologue that fit on the device (hydro, MHD); 0: not yet known, -1: none
+    int coop_cap[2] = {0, 0};
 };
 
 namespace dgpu_rt {

@@ -278,13 +278,6 @@ int launch_prologue(dragon_grid* h, int c, int bookkeeping, int apply_bc, int co
         CK(cudaGetLastError());
         return 0;
     }
-    // 2D / 3D: bookkeeping on one CTA, every ghost-fill pass over a whole grid,
-    // then the ring CFL and dt on one CTA (the ghost layers of a large grid are
-    // far too much work for one CTA)
-    PrologueArgs head = pa;
-    head.apply_bc = 0;
-    head.compute_dt = 0;
-    one_cta(head);
     long long ext_max = 1;  // largest transverse section of a pass, padded
     for (int a = 0; a < h->dim; a++) {
         long long sec = 1;
@@ -294,6 +287,39 @@ int launch_prologue(dragon_grid* h, int c, int bookkeeping, int apply_bc, int co
     }
     const long long items = 2 * ext_max * h->g;
     const int blocks = (int)std::max<long long>(1, std::min<long long>((items + 255) / 256, 148 * 8));
+    // 2D / 3D: one cooperative launch (bookkeeping, every ghost-fill pass over
+    // the whole grid, the ring CFL and dt, grid barriers between them) where the
+    // device can hold its CTAs at once
+    int& cap = h->coop_cap[h->mhd ? 1 : 0];
+    const void* coop = h->mhd ? (const void*)k_prologue_coop<true> : (const void*)k_prologue_coop<false>;
+    if (cap == 0) {
+        int dev = 0, sms = 0, occ = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, coop, 256, 0));
+        int coop_ok = 0;
+        CK(cudaDeviceGetAttribute(&coop_ok, cudaDevAttrCooperativeLaunch, dev));
+        cap = (coop_ok && occ > 0) ? occ * sms : -1;
+    }
+    if (cap > 0) {
+        Geo g0 = h->cg, g1 = h->fg;
+        double* wp = W;
+        double* bp = h->B[c];
+        const BCEntry* ep = h->dbcs;
+        StepCtl* cp = h->ctl;
+        PrologueArgs ap = pa;
+        void* args[] = {&g0, &g1, &wp, &bp, &ep, &cp, &ap};
+        CK(cudaLaunchCooperativeKernel(coop, std::min(blocks, cap), 256, args, 0, h->stream));
+        h->launches++;
+        return 0;
+    }
+    // no cooperative launch: bookkeeping on one CTA, every ghost-fill pass over
+    // a whole grid, then the ring CFL and dt on one CTA (the ghost layers of a
+    // large grid are far too much work for one CTA)
+    PrologueArgs head = pa;
+    head.apply_bc = 0;
+    head.compute_dt = 0;
+    one_cta(head);
     for (int e = bc_first; e < bc_first + bc_count; e++) {
         for (int a = 0; a < h->dim; a++) {
             if (h->mhd) k_bc_pass<true><<<blocks, 256, 0, h->stream>>>(h->cg, h->fg, W, h->B[c], h->dbcs, h->ctl, e, a, 0);
@@ -438,6 +464,7 @@ const char* stage_name(int s) {
         case ST_NAN: return "NaN state would be produced";
         case ST_UNPHYSICAL: return "Unphysical state would be produced";
         case ST_CFL_ZERO: return "CFL timestep failed: max signal speed is zero";
+        case ST_BARRIER: return "ghost fill failed: a grid barrier gave up waiting";
         default: return "step failed";
     }
 }
@@ -511,6 +538,12 @@ int advance_finish(dragon_grid* h, dragon_advance_stats* st) {
                 if (st) st->failure.code = DRAGON_GPU_ECFL;
                 if (h->split_mode) h->sweep_step += ks;
                 return fail(DRAGON_GPU_ECFL, stage_name(stage));
+            }
+            if (stage == ST_BARRIER) {  // the ghosts may be incomplete: no retry on them
+                if (st) st->failure.code = DRAGON_GPU_ECUDA;
+                if (h->split_mode) h->sweep_step += ks;
+                h->imax_valid = false;
+                return fail(DRAGON_GPU_ECUDA, stage_name(stage));
             }
             // CFL.cpp:198-208: halve t1 and retry the same step on the same ghosts.
             double t1 = C.t1;
