@@ -481,15 +481,28 @@ static int enqueue_batch(dragon_grid* h) {
     int rc;
     for (int b = 0; b < nb; b++) {
         const int c = A.cur0 ^ (int)((A.k + b) & 1);
-        // with a step budget, the prologue after the last step only accounts it
-        // (bookkeeping alone: no ghost fill, no CFL time)
-        const bool account_only = A.max_steps > 0 && A.k + b >= A.max_steps;
-        if ((rc = launch_prologue(h, c, 1, account_only ? 0 : 1, account_only ? 0 : 1, c, c ^ 1))) return rc;
-        if (account_only) continue;
+        // with a step budget, the slot after the last step only accounts it;
+        // advance_finish does that on the host (account_last_step)
+        if (A.max_steps > 0 && A.k + b >= A.max_steps) continue;
+        if ((rc = launch_prologue(h, c, 1, 1, 1, c, c ^ 1))) return rc;
         if ((rc = launch_any_step(h, c, A.k + b))) return rc;
     }
     A.k += nb;
     return 0;
+}
+
+// The bookkeeping of the prologue that would follow a step budget's last
+// step (prologue_bookkeeping), done on the host mirror once that step has run:
+// one launch fewer per budgeted advance. The device copy of the control block
+// is not read again before the next advance rewrites it.
+static bool account_last_step(dragon_grid* h, StepCtl& C) {
+    if (C.have_prev) {
+        C.remaining -= C.t1;
+        C.steps_done += 1;
+    }
+    C.have_prev = 1;
+    if (!(C.remaining > h->cfg.timestep_tol) || (C.max_steps > 0 && C.steps_done >= C.max_steps)) C.done = 1;
+    return C.done != 0;
 }
 
 int advance_begin(dragon_grid* h, double remaining, int max_steps, int check_cfl) {
@@ -573,6 +586,8 @@ int advance_finish(dragon_grid* h, dragon_advance_stats* st) {
             if ((rc = enqueue_batch(h))) return rc;
             continue;
         }
+        if (!C.done && A.max_steps > 0 && A.k > A.max_steps && !account_last_step(h, C))
+            return fail(DRAGON_GPU_ESTEP, "step budget consumed but the advance did not finish");
         if (C.done) {
             h->cur = cur0 ^ (int)(C.steps_done & 1);
             h->imax_valid = true;
