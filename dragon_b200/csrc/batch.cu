@@ -142,7 +142,7 @@ BatchInst make_inst(dragon_grid* h, int tile, int group, bool mixed) {
         return I;
     }
     const int nx = h->n[0], ny = h->n[1];
-    I.frame = mhd2d_frame_points(h->cg);
+    I.frame = mhd2d_frame_points(h->cg.n[0], h->cg.n[1], h->cg.g);
     I.last_phase = 8;
     I.ntiles[1] = (int)std::max<long long>(1, (I.frame + kCopyChunk - 1) / kCopyChunk);
     I.ntj[1] = 1;

@@ -18,6 +18,7 @@
 
 #include <algorithm>
 
+#include "frame.cuh"
 #include "grid.cuh"
 #include "recon.cuh"
 #include "riemann.cuh"
@@ -415,47 +416,6 @@ __device__ __forceinline__ void mhd2d_update(const Mhd2DArgs& A, const Tile2& T)
 // Bz [0, nx) x [0, ny); the frame is the rest of each padded array, about
 // 4 g (n + g) points per array instead of the whole array.
 
-// Point k of the frame of the box [bi0, bi1) x [bj0, bj1) inside the padded
-// range [lo_i, hi_i) x [lo_j, hi_j): the rows above and below the box, then
-// the columns left and right of it. False past the last point.
-__device__ __forceinline__ bool frame_point(long long k, int lo_i, int hi_i, int lo_j, int hi_j, int bi0, int bi1,
-                                            int bj0, int bj1, int& i, int& j) {
-    const long long W = hi_j - lo_j;
-    const long long top = (long long)(bi0 - lo_i) * W;
-    if (k < top) {
-        i = lo_i + (int)(k / W);
-        j = lo_j + (int)(k % W);
-        return true;
-    }
-    k -= top;
-    const long long bot = (long long)(hi_i - bi1) * W;
-    if (k < bot) {
-        i = bi1 + (int)(k / W);
-        j = lo_j + (int)(k % W);
-        return true;
-    }
-    k -= bot;
-    const int sl = bj0 - lo_j, side = sl + (hi_j - bj1);
-    if (side <= 0 || k >= (long long)(bi1 - bi0) * side) return false;
-    i = bi0 + (int)(k / side);
-    const int c = (int)(k % side);
-    j = c < sl ? lo_j + c : bj1 + (c - sl);
-    return true;
-}
-
-__device__ __forceinline__ long long frame_count(int lo_i, int hi_i, int lo_j, int hi_j, int bi0, int bi1, int bj0,
-                                                 int bj1) {
-    return (long long)(hi_i - lo_i) * (hi_j - lo_j) - (long long)(bi1 - bi0) * (bj1 - bj0);
-}
-
-// Frame points of the cells and of the three face-B components, in that order.
-__host__ __device__ __forceinline__ long long mhd2d_frame_points(const Geo& G) {
-    const long long nx = G.n[0], ny = G.n[1], g = G.g;
-    const long long cells = (nx + 2 * g) * (ny + 2 * g) - nx * ny;
-    const long long faces = (nx + 1 + 2 * g) * (ny + 1 + 2 * g);
-    return cells + (faces - (nx + 1) * ny) + (faces - nx * (ny + 1)) + (faces - nx * ny);
-}
-
 // Copies frame points [k0, k1) (of mhd2d_frame_points) with the calling
 // threads: thread tid of nthr.
 __device__ __forceinline__ void mhd2d_copy_frame(const Geo& G, const Geo& FG, const double* __restrict__ w,
@@ -497,14 +457,14 @@ __device__ __forceinline__ void mhd2d_copy_frame(const Geo& G, const Geo& FG, co
 
 static __global__ void k_mhd2d_copy_frame(Geo G, Geo FG, const double* __restrict__ w, double* __restrict__ wout,
                                           const double* __restrict__ B, double* __restrict__ Bout) {
-    mhd2d_copy_frame(G, FG, w, wout, B, Bout, 0, mhd2d_frame_points(G), blockIdx.x * (long long)blockDim.x + threadIdx.x,
-                     (long long)gridDim.x * blockDim.x);
+    mhd2d_copy_frame(G, FG, w, wout, B, Bout, 0, mhd2d_frame_points(G.n[0], G.n[1], G.g),
+                     blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
 }
 
 // Enqueues the frame copy of a single-grid step.
 inline int launch_mhd2d_copy_frame(const Geo& G, const Geo& FG, const double* w, double* wout, const double* B,
                                    double* Bout, cudaStream_t st) {
-    const long long n = mhd2d_frame_points(G);
+    const long long n = mhd2d_frame_points(G.n[0], G.n[1], G.g);
     const int blocks = (int)std::min<long long>((n + 255) / 256, 148 * 8);
     k_mhd2d_copy_frame<<<blocks, 256, 0, st>>>(G, FG, w, wout, B, Bout);
     return cudaGetLastError() == cudaSuccess ? 0 : 1;

@@ -18,7 +18,8 @@ def build_hostcheck(variant: str) -> str:
     """Builds tests/hostcheck/libhostcheck_{hydro,mhd}.so (CPU build of the device math)."""
     out = os.path.join(HOSTCHECK, f"libhostcheck_{variant}.so")
     src = os.path.join(HOSTCHECK, "hostcheck.cpp")
-    deps = [src] + [os.path.join(ROOT, "dragon_b200", "csrc", f) for f in ("fluid.cuh", "recon.cuh", "riemann.cuh")]
+    deps = [src] + [os.path.join(ROOT, "dragon_b200", "csrc", f)
+                    for f in ("fluid.cuh", "recon.cuh", "riemann.cuh", "frame.cuh")]
     if not os.path.exists(out) or any(os.path.getmtime(d) > os.path.getmtime(out) for d in deps):
         cmd = ["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-o", out, src]
         if variant == "mhd":

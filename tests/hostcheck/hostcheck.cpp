@@ -4,6 +4,7 @@
 // the CPU tests check operand order against the reference bit for bit before
 // any GPU run. Not part of the product: nothing outside tests/ loads it.
 #include "../../dragon_b200/csrc/fluid.cuh"
+#include "../../dragon_b200/csrc/frame.cuh"
 #include "../../dragon_b200/csrc/recon.cuh"
 #include "../../dragon_b200/csrc/riemann.cuh"
 
@@ -70,6 +71,13 @@ void hc_exact_flux_guess(const double* l, const double* r, int mode, int max_ite
 }
 #endif
 int hc_nfields(void) { return NF; }
+// Ghost-frame enumeration of the 2D MHD step (frame.cuh): point k of the frame
+// of box b (bi0, bi1, bj0, bj1) inside range r (lo_i, hi_i, lo_j, hi_j).
+int hc_frame_point(long long k, const int* r, const int* b, int* ij) {
+    return frame_point(k, r[0], r[1], r[2], r[3], b[0], b[1], b[2], b[3], ij[0], ij[1]) ? 1 : 0;
+}
+long long hc_frame_count(const int* r, const int* b) { return frame_count(r[0], r[1], r[2], r[3], b[0], b[1], b[2], b[3]); }
+long long hc_mhd2d_frame_points(long long nx, long long ny, long long g) { return mhd2d_frame_points(nx, ny, g); }
 void hc_prim_to_cons(const double* w, double* u) { Cout(to_cons<M>(P(w)), u); }
 void hc_cons_to_prim(const double* u, double* w) { Pout(to_prim<M>(C(u)), w); }
 void hc_prim_flux(const double* w, double* f) { Cout(prim_flux<M>(P(w)), f); }
