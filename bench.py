@@ -325,7 +325,9 @@ def run_reference(args):
         return
     base = {"metric": METRIC, "unit": "cell-updates/s", "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": WORKLOAD, "grid": [N, N], "parallelism": "host threads"}}
+            "data": "synthetic (seeded KH shear layer, numpy PCG64 seed 1234)",
+            "config": {"workload": WORKLOAD, "grid": [N, N], "solver": "HLLC", "limiter": "vanLeer", "precision": "fp64",
+                       "parallelism": "host threads (DistGrid2D children)"}}
     cb, why = reference_baseline(args.steps, args.warmup)
     if cb is None:
         base["unavailable"] = why
