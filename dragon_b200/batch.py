@@ -5,7 +5,10 @@ Grid::advance, DRAGON/Hydro/CFL/CFL.cpp:151-213). A Batch holds grid objects of
 uneven sizes - 1D hydro and 2D MHD - each with its own configuration,
 boundaries, CFL dt and retries, and advances them all with one persistent
 kernel per step over a device work queue, replayed from a CUDA graph. Each
-member ends in exactly the state its own advance_steps would give.
+FP64 member ends in exactly the state its own advance_steps would give. The
+members share one precision; in a mixed FP32/FP64 batch the 1D members end
+exactly where their own mixed advance ends and the 2D MHD members to FP32
+rounding of it.
 """
 from __future__ import annotations
 
