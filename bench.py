@@ -29,7 +29,14 @@ fused update). Metric: cell-updates/s (interior cells x steps / time).
              persistent work-queue kernel, against the same grids one by one,
              in mixed FP32/FP64 (with its L1 per field from FP64) and FP64;
   mhd        2D MHD Orszag-Tang 1024^2, FP64 and mixed, with the mixed path's
-             L1 per field and max |div B| of both.
+             L1 per field and max |div B| of both;
+  stated_length  the mixed path against the FP64 path at the stated lengths of
+             the two 2D configurations: the shear layer 1024^2 for 2000 steps
+             and Orszag-Tang 1024^2 to t = 0.5 (relative L1 per field).
+
+stdout carries one JSON line: the contract keys and a compact "summary" of
+the sections above, last so a tail of the line keeps it; the full sections
+go to stderr as one JSON line prefixed "detail: ".
 
 ``--impl reference`` times only the reference on the host cores and prints its
 own line. Multi-GPU (torchrun): every rank advances its own 1024^2 grid
@@ -55,6 +62,36 @@ N = 1024  # grid extent per axis (--grid overrides it, e.g. for profiling captur
 CELL_BYTES = 80  # 5 FP64 primitive fields read + written per cell update
 METRIC = "cell-updates/s (2D unsplit CTU hydro, FP64)"
 WORKLOAD = "kelvin_helmholtz_2d_1024sq_hllc_vanleer_cfl0.3_periodic"
+L2_RULE = "84 MB double-buffered state < 126 MB L2: the device arm writes 256 MB before every timed step"
+
+
+def config_line():
+    """The workload both arms report (same keys and values)."""
+    return {"workload": WORKLOAD, "grid": [N, N], "solver": "HLLC", "limiter": "vanLeer", "precision": "fp64",
+            "l2": L2_RULE}
+
+
+def sig(x, digits=4):
+    """x with every float rounded to `digits` significant digits (lists and
+    dicts recursively): the compact summary of the bench line."""
+    if isinstance(x, float):
+        return float(f"{x:.{digits}g}") if math.isfinite(x) else x
+    if isinstance(x, dict):
+        return {k: sig(v, digits) for k, v in x.items()}
+    if isinstance(x, (list, tuple)):
+        return [sig(v, digits) for v in x]
+    return x
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 E2E_INFLIGHT = 8  # grids whose upload / step / download overlap on separate streams (4: 1.00e9, 6: 1.07e9, 8: 1.08e9)
@@ -314,9 +351,11 @@ def reference_baseline(steps: int, warmup: int, budget_s: float | None = None):
             break
     el = time.perf_counter() - t0
     R.close()
+    side = math.ceil(math.sqrt(cores))  # DistGrid2D's children: ceil(sqrt(core_count))^2 (DistGrid.cpp:63-64)
     return {"value": N * N * done / el, "unit": "cell-updates/s", "cores": cores, "kind": "reference",
-            "sample": f"{done} full 1024x1024 steps of the reference DistGrid2D (core_count={cores}), "
-                      f"{el:.1f} s wall"}, None
+            "cpu_model": cpu_model(), "core_count": cores, "threads_spawned": side * side,
+            "sample": f"{done} full {N}x{N} steps of the reference DistGrid2D (core_count={cores}, "
+                      f"{side * side} child threads), {el:.1f} s wall"}, None
 
 
 def run_reference(args):
@@ -326,8 +365,7 @@ def run_reference(args):
     base = {"metric": METRIC, "unit": "cell-updates/s", "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded KH shear layer, numpy PCG64 seed 1234)",
-            "config": {"workload": WORKLOAD, "grid": [N, N], "solver": "HLLC", "limiter": "vanLeer", "precision": "fp64",
-                       "parallelism": "host threads (DistGrid2D children)"}}
+            "parallelism": "host threads (DistGrid2D children)", "config": config_line()}
     cb, why = reference_baseline(args.steps, args.warmup)
     if cb is None:
         base["unavailable"] = why
@@ -340,12 +378,17 @@ def run_reference(args):
     print(json.dumps(base))
 
 
-def learned_guess_report(train_runs=4, train_n=96, train_steps=15, n=128, p_in=1000.0, steps=10):
-    """The learned star-pressure guess on a 3D blast: a network trained on the
-    GPU from seeded blast runs (inner pressure log-uniform in [10, 1e4]), then
-    an unseen blast run with the reference's mean guess, the analytic guess
-    and the learned guess, cap lifted so every solve reaches the tolerance,
-    plus the reference's own setting (mean guess, cap 6)."""
+def learned_guess_report(n=256, p_in=10.0, steps=10):
+    """The learned star-pressure guess on the 3D blast configuration (n^3,
+    p_in = 10): a network trained on the GPU from the configuration's training
+    runs (learned.c4_training_set: seeded 128^3 blasts, inner pressure
+    log-uniform in [10, 1e4], ~1e7 converged solves), then the blast run with
+    the reference's mean guess, the analytic guess and the learned guess, cap
+    lifted so every solve reaches the tolerance, plus the reference's own
+    setting (mean guess, cap 6). The "perfect" arms start Newton from the
+    converged star pressure of an uncounted first solve, exactly or with a
+    relative error of 1e-9, 1e-6 or 1e-3: the iterations any guess of that
+    accuracy needs, i.e. the ceiling of the reduction a guess can give."""
     import torch
 
     import dragon_b200 as dg
@@ -353,19 +396,23 @@ def learned_guess_report(train_runs=4, train_n=96, train_steps=15, n=128, p_in=1
 
     t0 = time.perf_counter()
     net = learned.Network(seed=2024)
-    info = learned.collect_blast_samples(net, runs=train_runs, n=train_n, steps=train_steps, seed=2024, stride=8)
+    info = learned.c4_training_set(net)
     fit = learned.fit(net, steps=6000, batch=16384, lr=3e-3)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
-    out = {"train": {"runs": train_runs, "grid": train_n, "steps": train_steps, "samples": info["samples"],
-                     "rmse_ln_pstar": fit["rmse_log"], "gate": fit["gate"], "seconds": train_s},
+    out = {"train": {k: info[k] for k in ("runs", "n", "steps", "stride", "solves", "samples", "saturated_runs")},
            "workload": f"3D blast {n}^3, p_in {p_in:g}, MC, exact solver, {steps} steps"}
+    out["train"].update({"rmse_ln_pstar": fit["rmse_log"], "gate": fit["gate"], "seconds": train_s})
     ref = None
-    for name, guess, cap in (("mean_cap64", dg.GUESS_MEAN, 64), ("reference_mean_cap6", dg.GUESS_MEAN, 6),
-                             ("analytic_cap64", dg.GUESS_ANALYTIC, 64), ("learned_cap64", dg.GUESS_LEARNED, 64)):
+    arms = [("mean_cap64", dg.GUESS_MEAN, 64, 0), ("reference_mean_cap6", dg.GUESS_MEAN, 6, 0),
+            ("analytic_cap64", dg.GUESS_ANALYTIC, 64, 0), ("learned_cap64", dg.GUESS_LEARNED, 64, 0),
+            ("perfect_cap64", dg.GUESS_PERFECT, 64, 0), ("perfect_err1e-9_cap64", dg.GUESS_PERFECT, 64, 9),
+            ("perfect_err1e-6_cap64", dg.GUESS_PERFECT, 64, 6), ("perfect_err1e-3_cap64", dg.GUESS_PERFECT, 64, 3)]
+    for name, guess, cap, err in arms:
         w, d = problems.blast_3d(n, ghosts=2, p_in=p_in)
         G = dg.Grid3D(n, n, n, d, d, d, ghosts=2, config=dg.Config(
-            riemann=dg.RIEMANN_EXACT, limiter=dg.LIMITER_MC, exact_max_iters=cap, exact_guess=guess))
+            riemann=dg.RIEMANN_EXACT, limiter=dg.LIMITER_MC, exact_max_iters=cap, exact_guess=guess,
+            perfect_guess_err_exp=err))
         G.w[...] = w
         if guess == dg.GUESS_LEARNED:
             G.set_network(net)
@@ -389,6 +436,8 @@ def learned_guess_report(train_runs=4, train_n=96, train_steps=15, n=128, p_in=1
     m, l_ = out["mean_cap64"]["newton_iters_per_solve"], out["learned_cap64"]["newton_iters_per_solve"]
     out["iteration_reduction_vs_mean"] = m / l_
     out["iteration_reduction_vs_analytic"] = out["analytic_cap64"]["newton_iters_per_solve"] / l_
+    out["ceiling_reduction_vs_mean"] = {k[len("perfect_"):-len("_cap64")] or "exact": m / out[k]["newton_iters_per_solve"]
+                                        for k in out if k.startswith("perfect")}
     net.close()
     return out
 
@@ -443,6 +492,63 @@ def mhd_report(n=1024, steps=20, warmup=3):
     out["mixed"]["rel_l1_vs_fp64_per_field"] = [float(x) for x in l1]
     out["mixed"]["rel_l1_fields"] = ["rho", "p", "vx", "vy", "vz", "Bx", "By", "Bz"]
     out["mixed"]["rel_l1_face_B_vs_fp64"] = [float(x) for x in lb]
+    return out
+
+
+def stated_length_report(n=1024, kh_steps=2000, ot_time=0.5):
+    """The mixed path against the FP64 path (bit-identical to the reference) at
+    the stated lengths of the two 2D configurations: the shear layer for
+    kh_steps steps and Orszag-Tang to t = ot_time, both n^2, each grid pair
+    from the same initial state; relative L1 per field of the interiors, the
+    step counts and the device-loop wall time of each path."""
+    import torch
+
+    import dragon_b200 as dg
+    from dragon_b200 import problems
+
+    out = {}
+    w0, dx, dy = problems.kelvin_helmholtz_2d(n, ghosts=2, seed=1234)
+    st = {}
+    for name, prec in (("fp64", dg.PREC_FP64), ("mixed", dg.PREC_MIXED)):
+        G = dg.Grid2D(n, n, dx, dy, ghosts=2, config=dg.Config(riemann=dg.RIEMANN_HLLC, limiter=dg.LIMITER_VANLEER,
+                                                               precision=prec))
+        G.w[...] = w0
+        G.boundary = dg.Periodic()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = G.advance_steps(kh_steps)
+        st[name] = (G.w.copy(), time.perf_counter() - t0, r.time_advanced)
+        G.close()
+    l1 = problems.rel_l1(st["mixed"][0][2:-2, 2:-2], st["fp64"][0][2:-2, 2:-2])
+    out["shear_layer"] = {"grid": n, "steps": kh_steps, "t_fp64": st["fp64"][2], "t_mixed": st["mixed"][2],
+                          "rel_l1_vs_fp64": dict(zip(["rho", "p", "vx", "vy", "vz"], (float(x) for x in l1))),
+                          "wall_s_fp64": st["fp64"][1], "wall_s_mixed": st["mixed"][1]}
+    w0, B0, dx, dy = problems.orszag_tang_2d(n, ghosts=3)
+    st = {}
+    for name, prec in (("fp64", dg.PREC_FP64), ("mixed", dg.PREC_MIXED)):
+        G = dg.Grid2D(n, n, dx, dy, ghosts=3, config=dg.Config(mhd=True, riemann=dg.RIEMANN_HLLX, precision=prec))
+        G.w[...] = w0
+        G.B[...] = B0
+        G.boundary = dg.Periodic()
+        G.initialize_B_fields()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = G.advance(ot_time)
+        Bf = G.B.copy()
+        g = 3
+        d = (Bf[g + 1:g + n + 1, g:g + n, 0] - Bf[g:g + n, g:g + n, 0]) + \
+            (Bf[g:g + n, g + 1:g + n + 1, 1] - Bf[g:g + n, g:g + n, 1])
+        st[name] = (G.w.copy(), Bf, time.perf_counter() - t0, r.steps, float(np.abs(d).max()))
+        G.close()
+    g = 3
+    l1 = problems.rel_l1(st["mixed"][0][g:-g, g:-g], st["fp64"][0][g:-g, g:-g])
+    lb = problems.rel_l1(st["mixed"][1][g:-g, g:-g, :2], st["fp64"][1][g:-g, g:-g, :2])
+    out["orszag_tang"] = {"grid": n, "t": ot_time, "steps_fp64": st["fp64"][3], "steps_mixed": st["mixed"][3],
+                          "rel_l1_vs_fp64": dict(zip(["rho", "p", "vx", "vy", "vz", "Bx", "By", "Bz"],
+                                                     (float(x) for x in l1))),
+                          "rel_l1_face_B_vs_fp64": [float(x) for x in lb],
+                          "max_abs_divB_dx": {"fp64": st["fp64"][4], "mixed": st["mixed"][4]},
+                          "wall_s_fp64": st["fp64"][2], "wall_s_mixed": st["mixed"][2]}
     return out
 
 
@@ -543,6 +649,39 @@ def batch_report(steps=500, one_by_one_steps=50):
                                          "retries", "tuning")}}
     out["mixed_vs_fp64"] = mixed["value"] / fp64["value"]
     return out
+
+
+def summary_of(d):
+    """The headline numbers of each detailed section, rounded (the bench line's
+    last key, so a tail of the line keeps it)."""
+    out = {}
+    if "mixed" in d:
+        m = d["mixed"]
+        out["mixed"] = {"value": m["value"], "speedup_vs_fp64": m["speedup_vs_fp64"],
+                        "kernel_ms": m["kernel_ms_avg"], "hbm_frac": m["roofline_hbm_frac"],
+                        "max_rel_l1_vs_fp64": max(m["rel_l1_vs_fp64_per_field"]),
+                        "steps_compared": m["steps_compared"]}
+    if "stated_length" in d:
+        k, o = d["stated_length"]["shear_layer"], d["stated_length"]["orszag_tang"]
+        out["mixed_at_stated_length"] = {
+            "shear_layer_1024_2000_steps": k["rel_l1_vs_fp64"],
+            "orszag_tang_1024_t0.5": dict(o["rel_l1_vs_fp64"], steps=o["steps_fp64"],
+                                          divB_dx=max(o["max_abs_divB_dx"].values()))}
+    if "mhd" in d:
+        m = d["mhd"]
+        out["mhd_orszag_tang_1024"] = {"fp64_value": m["fp64"]["value"], "mixed_value": m["mixed"]["value"],
+                                       "mixed_speedup": m["mixed"]["speedup_vs_fp64"]}
+    if "learned_guess" in d:
+        g = d["learned_guess"]
+        out["learned_guess"] = {k: g[k] for k in g if k.startswith(("iteration_reduction", "ceiling_reduction"))}
+        out["learned_guess"]["train_samples"] = g["train"]["samples"]
+        out["learned_guess"]["iters_per_solve"] = {k: g[k]["newton_iters_per_solve"] for k in g
+                                                   if isinstance(g[k], dict) and "newton_iters_per_solve" in g[k]}
+    if "batch" in d:
+        b = d["batch"]
+        out["batch_c5"] = {"mixed_value": b["value"], "fp64_value": b["fp64"]["value"],
+                           "vs_one_by_one": b["speedup_vs_one_by_one"], "mixed_vs_fp64": b["mixed_vs_fp64"]}
+    return sig(out, 4)
 
 
 def run_gpu(args):
@@ -698,9 +837,8 @@ def run_gpu(args):
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if not args.mixed else "f32/f64",
             "data": "synthetic (seeded KH shear layer, numpy PCG64 seed 1234 + rank)",
-            "config": {"workload": WORKLOAD, "grid": [N, N], "solver": "HLLC", "limiter": "vanLeer",
-                       "precision": "mixed" if args.mixed else "fp64", "l2": "flushed before every timed step",
-                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
+            "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+            "config": dict(config_line(), precision="mixed" if args.mixed else "fp64"),
             "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": bytes_step,
                     "d2h_bytes_per_step": bytes_step, "steps": e2e_steps * len(e2e_grids),
                     "grids_in_flight": len(e2e_grids), "one_grid_value": e2e_serial_value,
@@ -714,18 +852,26 @@ def run_gpu(args):
             "clocks": clocks,
             "wall_s_timed": t_wall,
         }
+        detail = {}
         if mixed is not None:
-            line["mixed"] = mixed
+            detail["mixed"] = mixed
         if not args.no_learned:
-            line["learned_guess"] = learned_guess_report()
+            detail["learned_guess"] = learned_guess_report()
         if not args.no_batch:
-            line["batch"] = batch_report()
+            detail["batch"] = batch_report()
         if not args.no_mhd:
-            line["mhd"] = mhd_report()
+            detail["mhd"] = mhd_report()
+        if not args.no_stated_length:
+            detail["stated_length"] = stated_length_report()
         if not args.no_cpu_baseline:
             cb, why = reference_baseline(1000, 0, budget_s=args.cpu_budget)
             line["cpu_baseline"] = cb if cb else {"unavailable": why}
-        print(json.dumps(line))
+        line["e2e"].pop("copy_bound", None)
+        line["e2e"]["copy_bound_value"] = link["value"]
+        detail["e2e_copy_bound"] = link
+        line["summary"] = summary_of(detail)
+        print("detail: " + json.dumps(detail), file=sys.stderr, flush=True)
+        print(json.dumps(sig(line, 6)), flush=True)
     G.close()
     if ws > 1:
         dist.destroy_process_group()
@@ -743,6 +889,8 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned star-pressure guess report")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched uneven-instance report")
     ap.add_argument("--no-mhd", action="store_true", help="skip the 2D MHD (Orszag-Tang) report")
+    ap.add_argument("--no-stated-length", action="store_true",
+                    help="skip the mixed-vs-FP64 comparison at the configurations' stated lengths")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--e2e-inflight", type=int, default=E2E_INFLIGHT,
                     help="grids whose end-to-end steps overlap on separate streams")

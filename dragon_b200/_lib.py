@@ -30,7 +30,8 @@ class DragonConfig(ctypes.Structure):
         ("timestep_tol", ctypes.c_double),
         ("precision", ctypes.c_int),
         ("exact_guess", ctypes.c_int),
-        ("reserved", ctypes.c_int * 6),
+        ("perfect_guess_err_exp", ctypes.c_int),
+        ("reserved", ctypes.c_int * 5),
     ]
 
 
@@ -151,6 +152,7 @@ SIGNATURES = {
     ),
     "dragon_gpu_launch_count": (ctypes.c_ulonglong, [ctypes.c_void_p]),
     "dragon_gpu_profile_enable": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "dragon_gpu_debug_set": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "dragon_gpu_profile_read": (
         ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong),
                        ctypes.c_int]),

@@ -132,6 +132,7 @@ BatchInst make_inst(dragon_grid* h, int tile, int group, bool mixed) {
     pa.compute_dt = 1;
     pa.nbc = h->nbc;
     pa.bc_first = 0;
+    pa.stall_cta = -1;
     I.ntiles[0] = mixed ? 0 : 1;  // a mixed batch runs its prologues in k_batch_prologue
     I.ntj[0] = 1;
     I.group = group < 1 ? 1 : group;

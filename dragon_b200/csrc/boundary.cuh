@@ -38,6 +38,7 @@ struct PrologueArgs {
     int compute_dt;     // compute t1 from the CFL limit
     int nbc;            // entries to apply
     int bc_first;       // first entry to apply
+    int stall_cta;      // test hook: this CTA of k_prologue_coop returns before its first barrier (-1: none)
 };
 
 // ---------------------------------------------------------------------------
@@ -365,7 +366,10 @@ __global__ void __launch_bounds__(1024) k_prologue(Geo G, Geo FG, double* __rest
 }
 
 // Grid-wide barrier of a cooperative launch (every CTA resident). Bounded: a
-// wait that gives up records ST_BARRIER and returns false.
+// wait that gives up records ST_BARRIER and returns false. A waiting CTA also
+// gives up as soon as another CTA has recorded a failure (the only failure the
+// prologue records before its last barrier is a barrier that gave up), so one
+// missing CTA costs one wait limit, not one per remaining barrier.
 constexpr long long kGridBarrierPolls = 1LL << 22;  // >= 32 ns each
 __device__ __forceinline__ bool grid_barrier(StepCtl* ctl) {
     __shared__ int s_ok;
@@ -382,6 +386,10 @@ __device__ __forceinline__ bool grid_barrier(StepCtl* ctl) {
         } else {
             long long polls = 0;
             while (*gen == g0) {
+                if (*(const volatile int*)&ctl->err) {
+                    ok = 0;
+                    break;
+                }
                 if (++polls > kGridBarrierPolls) {
                     ok = 0;
                     record_error(ctl, ST_BARRIER, 0);
@@ -408,6 +416,13 @@ __global__ void __launch_bounds__(256) k_prologue_coop(Geo G, Geo FG, double* __
                                                       const BCEntry* __restrict__ bcs, StepCtl* ctl, PrologueArgs pa) {
     __shared__ int s_skip;
     __shared__ double s_red[32];
+    // A failure recorded by an earlier launch of this advance (a flux, state or
+    // barrier failure of the batch the host has not read yet): every CTA
+    // returns before the first barrier. Nothing in this launch writes err
+    // before that barrier (bookkeeping only writes done), so all CTAs agree.
+    if (threadIdx.x == 0) s_skip = *(const volatile int*)&ctl->err | (int)(blockIdx.x == pa.stall_cta);
+    __syncthreads();
+    if (s_skip) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         ctl->ring_bits = 0ull;
         prologue_bookkeeping(ctl, pa);

@@ -199,12 +199,13 @@ struct StepArgs {
     int slot_out;        // vmax slot the epilogue accumulates into
     int forced;          // retry: use ctl->t1 even if err was set earlier in this batch
     int exact_guess;     // GuessMode of the exact solver
+    double guess_err;    // GUESS_PERFECT's relative error of the start
     NewtonLog nlog;      // converged-solve sample log (rows null: off)
     const MlpNet* mlp;   // learned guess network (GUESS_LEARNED)
 };
 
 __host__ __device__ __forceinline__ ExactOpts exact_opts(const StepArgs& sa) {
-    return ExactOpts{sa.exact_max_iters, sa.exact_tol, sa.exact_guess, sa.nlog};
+    return ExactOpts{sa.exact_max_iters, sa.exact_tol, sa.exact_guess, sa.nlog, sa.guess_err};
 }
 
 }  // namespace dgpu

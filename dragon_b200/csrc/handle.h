@@ -81,6 +81,11 @@ struct dragon_grid {
     AdvanceState adv{};
     // CTAs of the cooperative prologue that fit on the device (hydro, MHD); 0: not yet known, -1: none
     int coop_cap[2] = {0, 0};
+    // test hooks (dragon_gpu_debug_set): CTA of the cooperative prologue that
+    // returns before its first grid barrier (-1: none); take the prologue path
+    // of devices without cooperative launch
+    int dbg_stall_cta = -1;
+    bool dbg_no_coop = false;
 };
 
 namespace dgpu_rt {

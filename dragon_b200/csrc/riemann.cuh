@@ -31,8 +31,11 @@ struct FaceStats {
 // reference's (pL + pR) / 2 (Exact.cpp:47); GUESS_ANALYTIC is the adaptive
 // PVRS / two-rarefaction / two-shock choice; GUESS_LEARNED takes the network's
 // value, with the analytic guess as fallback when that value is unusable and
-// as judge when the iteration from it hits the cap.
-enum GuessMode : int { GUESS_MEAN = 0, GUESS_ANALYTIC = 1, GUESS_LEARNED = 2 };
+// as judge when the iteration from it hits the cap. GUESS_PERFECT is a
+// measurement arm, not a solver option: the start is the converged star
+// pressure of a first solve that is not counted, times (1 +- guess_err), so
+// its iteration count is the floor a guess of that accuracy can reach.
+enum GuessMode : int { GUESS_MEAN = 0, GUESS_ANALYTIC = 1, GUESS_LEARNED = 2, GUESS_PERFECT = 3 };
 
 // Converged Newton solves recorded as training samples for the learned guess:
 // kNewtonLogCols doubles per row (face-normal frame).
@@ -49,6 +52,7 @@ struct ExactOpts {
     double tol;        // ExactRiemann_Tolerance (Config.h:43)
     int guess;         // GuessMode
     NewtonLog log;
+    double guess_err;  // GUESS_PERFECT: relative error given to the converged star pressure (0: none)
 };
 
 // HLL::roeAvg (HLL.cpp:21-37)
@@ -245,6 +249,8 @@ __device__ __forceinline__ void newton_log_push(const NewtonLog& lg, double rl, 
 }
 #endif
 
+constexpr int kPerfectGuessCap = 200;  // iterations of GUESS_PERFECT's uncounted first solve
+
 // Riemann::exact_StarP (Exact.cpp:71-84): Newton from pGuess, step clamp
 // 0.8 p, stop on relative change <= tol or after max_iters iterations.
 // *converged tells whether the tolerance (not the cap) ended the iteration.
@@ -349,6 +355,15 @@ DHD ExactSolution<R> exact_solve(const Prim<R>& L, const Prim<R>& Rt, ExactOpts 
     R pGuess, judge = R(0);
     if (o.guess == GUESS_MEAN) {
         pGuess = (L.p + Rt.p) / R(2);
+    } else if (o.guess == GUESS_PERFECT) {
+        ExactOpts q = o;
+        q.max_iters = kPerfectGuessCap;
+        q.log.rows = nullptr;
+        bool c0;
+        const R mean = (L.p + Rt.p) / R(2);
+        const R p0 = exact_star_p(L, Rt, mean, q, nullptr, &c0);
+        const R e = R(o.guess_err);
+        pGuess = (c0 && p0 > R(0) && sfinite(p0)) ? p0 * (R(1) + (L.p >= Rt.p ? e : -e)) : mean;
     } else if (o.guess != GUESS_LEARNED || !learned) {
         pGuess = analytic_guess(L, Rt);
     } else if (learned->guess > R(0) && sfinite(learned->guess)) {

@@ -172,6 +172,7 @@ StepArgs step_args(const dragon_grid* h, int slot_out) {
     a.slot_out = slot_out;
     a.forced = 0;
     a.exact_guess = h->cfg.exact_guess;
+    a.guess_err = h->cfg.perfect_guess_err_exp > 0 ? std::pow(10.0, -h->cfg.perfect_guess_err_exp) : 0.0;
     a.nlog = NewtonLog{h->nlog_rows, h->nlog_count, h->nlog_cap, h->nlog_stride};
     a.mlp = h->mlp_dev;
     return a;
@@ -268,6 +269,7 @@ int launch_prologue(dragon_grid* h, int c, int bookkeeping, int apply_bc, int co
     pa.compute_dt = compute_dt;
     pa.nbc = bc_count;
     pa.bc_first = bc_first;
+    pa.stall_cta = h->dbg_stall_cta;
     auto one_cta = [&](const PrologueArgs& a) {
         if (h->mhd) k_prologue<true><<<1, 1024, 0, h->stream>>>(h->cg, h->fg, W, h->B[c], h->dbcs, h->ctl, a);
         else k_prologue<false><<<1, 1024, 0, h->stream>>>(h->cg, h->fg, W, h->B[c], h->dbcs, h->ctl, a);
@@ -301,7 +303,7 @@ int launch_prologue(dragon_grid* h, int c, int bookkeeping, int apply_bc, int co
         CK(cudaDeviceGetAttribute(&coop_ok, cudaDevAttrCooperativeLaunch, dev));
         cap = (coop_ok && occ > 0) ? occ * sms : -1;
     }
-    if (cap > 0) {
+    if (cap > 0 && !h->dbg_no_coop) {
         Geo g0 = h->cg, g1 = h->fg;
         double* wp = W;
         double* bp = h->B[c];
@@ -658,9 +660,9 @@ int dragon_gpu_grid_create(int dim, int nx, int ny, int nz, double dx, double dy
     h->g = ghosts > gmin ? ghosts : gmin;
     if (h->mhd && dim == 1) h->g = ghosts > 3 ? ghosts : 3;
     h->solver = solver_id(h->cfg);
-    if (h->cfg.exact_guess < GUESS_MEAN || h->cfg.exact_guess > GUESS_LEARNED) {
+    if (h->cfg.exact_guess < GUESS_MEAN || h->cfg.exact_guess > GUESS_PERFECT) {
         delete h;
-        return fail(DRAGON_GPU_EINVAL, "exact_guess must be 0 (mean), 1 (analytic) or 2 (learned)");
+        return fail(DRAGON_GPU_EINVAL, "exact_guess must be 0 (mean), 1 (analytic), 2 (learned) or 3 (perfect)");
     }
     if (h->cfg.exact_guess == GUESS_LEARNED && !(dim == 3 && !h->mhd)) {
         delete h;
@@ -1085,6 +1087,15 @@ int dragon_gpu_device_state(dragon_grid* h, double** prim, long long* plane, lon
 }
 
 unsigned long long dragon_gpu_launch_count(const dragon_grid* h) { return h ? h->launches : 0; }
+
+int dragon_gpu_debug_set(dragon_grid* h, int key, int value) {
+    if (!h) return fail(DRAGON_GPU_EINVAL, "null handle");
+    switch (key) {
+        case DRAGON_GPU_DEBUG_STALL_CTA: h->dbg_stall_cta = value < 0 ? -1 : value; return 0;
+        case DRAGON_GPU_DEBUG_NO_COOP: h->dbg_no_coop = value != 0; return 0;
+        default: return fail(DRAGON_GPU_EINVAL, "unknown debug key");
+    }
+}
 
 int dragon_gpu_profile_enable(dragon_grid* h, int on) {
     if (!h) return fail(DRAGON_GPU_EINVAL, "null handle");

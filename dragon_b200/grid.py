@@ -28,7 +28,7 @@ LIMITER_MINMOD, LIMITER_MC, LIMITER_VANLEER, LIMITER_SUPERBEE, LIMITER_VANALBADA
 CFL_MAX, CFL_ADD = 0, 1
 CT_CONSV_TOTAL_E, CT_CONSV_THERMAL, CT_CONSV_BETA_GATED = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
-GUESS_MEAN, GUESS_ANALYTIC, GUESS_LEARNED = 0, 1, 2
+GUESS_MEAN, GUESS_ANALYTIC, GUESS_LEARNED, GUESS_PERFECT = 0, 1, 2, 3
 
 
 @dataclass
@@ -46,6 +46,7 @@ class Config:
     timestep_tol: float = 1e-14
     precision: int = PREC_FP64
     exact_guess: int = GUESS_MEAN
+    perfect_guess_err_exp: int = 0
 
     def to_c(self) -> _lib.DragonConfig:
         c = _lib.DragonConfig()
@@ -60,6 +61,7 @@ class Config:
         c.timestep_tol = self.timestep_tol
         c.precision = self.precision
         c.exact_guess = self.exact_guess
+        c.perfect_guess_err_exp = self.perfect_guess_err_exp
         return c
 
 

@@ -55,8 +55,11 @@ typedef struct dragon_config {
     int precision;        /* 0: FP64 throughout (bit-faithful), 1: mixed FP32/FP64 (1D hydro, 2D) */
     int exact_guess;      /* start of the exact solver's Newton iteration: 0 the reference's
                              (pL + pR) / 2 (Exact.cpp:47), 1 adaptive PVRS / two-rarefaction /
-                             two-shock, 2 learned (dragon_learned.h; 3D grids) */
-    int reserved[6];
+                             two-shock, 2 learned (dragon_learned.h; 3D grids), 3 a measurement
+                             arm: the converged star pressure of an uncounted first solve */
+    int perfect_guess_err_exp; /* exact_guess 3: the start is that pressure times (1 +- 10^-e)
+                             for e > 0 (+ where pL >= pR), exactly it for e <= 0 */
+    int reserved[5];
 } dragon_config;
 
 /* Fills the reference's shipped defaults for the given physics mode. */
@@ -197,6 +200,16 @@ unsigned long long dragon_gpu_launch_count(const dragon_grid* g);
  * measurement hook for the roofline). */
 int dragon_gpu_profile_enable(dragon_grid* g, int on);
 int dragon_gpu_profile_read(dragon_grid* g, double* ms_total, long long* launches, int reset);
+
+/* Test hooks (no reference counterpart). DRAGON_GPU_DEBUG_STALL_CTA: CTA
+ * `value` of every following cooperative ghost-fill launch (2D / 3D grids)
+ * returns before its first grid barrier, so the others' bounded barrier wait
+ * runs out and the advance fails with DRAGON_GPU_ECUDA; value < 0 turns it
+ * off. DRAGON_GPU_DEBUG_NO_COOP: value != 0 makes the ghost fill take the
+ * path of devices without cooperative launch (one launch per pass). */
+#define DRAGON_GPU_DEBUG_STALL_CTA 1
+#define DRAGON_GPU_DEBUG_NO_COOP 2
+int dragon_gpu_debug_set(dragon_grid* g, int key, int value);
 
 /* CFL time step of a state the caller already holds on the device, without
  * allocating anything (no counterpart in the reference: it serves callers

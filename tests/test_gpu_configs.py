@@ -1,0 +1,184 @@
+"""The stated configurations at their stated size and length, FP64 device path
+against the DRAGON reference itself (oracle/_ref), and the mixed path against
+the pinned FP64 path at the same lengths.
+
+* Shear layer (2D CTU hydro, HLLC, van Leer, periodic, CFL 0.3): 1024^2 for
+  200 steps against the reference's DistGrid2D on every host core, and 256^2
+  for the configuration's 2000 steps; same dt list, state bit for bit.
+* Orszag-Tang (2D MHD, HLLD, MC, CTU + CT, BETA_GATED, periodic) to t = 0.5 at
+  256^2: same dt list, cells and face B bit for bit, max |div B| at roundoff.
+* 3D blast (exact solver, MC, outflow) at 256^3 for 3 steps against the
+  reference's DistGrid3D: 1e-12 relative L1 per field (CUDA's pow against
+  glibc's) and the same dt list to 1e-12.
+* Mixed FP32/FP64 against FP64 at the full stated lengths: the shear layer at
+  1024^2 for 2000 steps and Orszag-Tang at 1024^2 to t = 0.5, relative L1 per
+  field (Kelvin-Helmholtz/Problem2D.cpp:13-60, Orszag-Tang/Problem2D.cpp:13-45
+  set these problems up in the reference).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import cuda_ok
+
+pytestmark = pytest.mark.gpu
+
+import dragon_b200 as dg  # noqa: E402
+from dragon_b200 import problems  # noqa: E402
+
+TOL_L1 = 1e-12
+TOL_MIXED = 1e-5
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _need_gpu():
+    if not cuda_ok():
+        pytest.fail("CUDA device required for -m gpu tests")
+
+
+def reference(variant="hydro"):
+    from oracle import refgrid
+    if not refgrid.available(variant):
+        pytest.skip("reference library not built")
+    return refgrid
+
+
+def same(a, b, what):
+    bad = np.argwhere(a != b)
+    assert bad.size == 0, f"{what}: {len(bad)} mismatches, first at {bad[:3].tolist()}"
+
+
+def div_b_max(Bf, n, g):
+    d = (Bf[g + 1:g + n + 1, g:g + n, 0] - Bf[g:g + n, g:g + n, 0]) + \
+        (Bf[g:g + n, g + 1:g + n + 1, 1] - Bf[g:g + n, g:g + n, 1])
+    return float(np.abs(d).max())
+
+
+def kh_device(n, precision=dg.PREC_FP64, seed=1234):
+    w0, dx, dy = problems.kelvin_helmholtz_2d(n, ghosts=2, seed=seed)
+    G = dg.Grid2D(n, n, dx, dy, ghosts=2, config=dg.Config(riemann=dg.RIEMANN_HLLC, limiter=dg.LIMITER_VANLEER,
+                                                           precision=precision))
+    G.w[...] = w0
+    G.boundary = dg.Periodic()
+    return G, w0, dx, dy
+
+
+def kh_reference_dist(n, w0, dx, dy):
+    ref = reference("hydro")
+    R = ref.RefGrid(2, (n, n), (dx, dy), ghosts=2, dist=True, riemann=dg.RIEMANN_HLLC, limiter=dg.LIMITER_VANLEER,
+                    cfl=dg.CFL_ADD, core_count=os.cpu_count() or 1)
+    R.set_prim(w0)
+    R.set_boundary([(dg.boundary.PERIODIC, 63, 1, None)])
+    return R
+
+
+@pytest.mark.parametrize("n,steps", [(1024, 200), (256, 2000)])
+def test_shear_layer_bitwise_vs_reference_distgrid(n, steps):
+    G, w0, dx, dy = kh_device(n)
+    R = kh_reference_dist(n, w0, dx, dy)
+    ref_dts = [R.step_cfl() for _ in range(steps)]
+    dts = []
+    for _ in range(steps):
+        res = G.advance_steps(1)
+        assert res.steps == 1 and res.retries == 0
+        dts.append(res.last_dt)
+    assert dts == ref_dts
+    same(G.w, R.get_prim(), f"shear layer {n}^2 after {steps} steps")
+    R.close()
+
+
+def ot_device(n, precision=dg.PREC_FP64):
+    w0, B0, dx, dy = problems.orszag_tang_2d(n, ghosts=3)
+    G = dg.Grid2D(n, n, dx, dy, ghosts=3, config=dg.Config(mhd=True, riemann=dg.RIEMANN_HLLX, limiter=dg.LIMITER_MC,
+                                                           precision=precision))
+    G.w[...] = w0
+    G.B[...] = B0
+    G.boundary = dg.Periodic()
+    G.initialize_B_fields()
+    return G, w0, B0, dx, dy
+
+
+def test_orszag_tang_to_t05_bitwise_vs_reference_distgrid():
+    n, T = 256, 0.5
+    ref = reference("mhd")
+    G, w0, B0, dx, dy = ot_device(n)
+    H = ot_device(n)[0]
+    R = ref.RefGrid(2, (n, n), (dx, dy), ghosts=3, mhd=True, dist=True, riemann=dg.RIEMANN_HLLX,
+                    limiter=dg.LIMITER_MC, cfl=dg.CFL_ADD, core_count=os.cpu_count() or 1)
+    R.set_prim(w0)
+    R.set_faceB(B0)
+    R.set_boundary([(dg.boundary.PERIODIC, 63, 1, None)])
+    R.initialize_B_fields()
+    # the reference's advance_unsplit loop (CFL.cpp:188-213) step by step, logging dt
+    ref_dts, rem = [], T
+    while rem > 1e-14:
+        R.apply_boundary()
+        t1 = min(rem, R.cfl_time())
+        R.unsplit_step(t1)
+        ref_dts.append(t1)
+        rem -= t1
+    # the device: the same loop through its own ghost fill, CFL and step ...
+    dts, rem = [], T
+    while rem > 1e-14:
+        G.apply_boundary()
+        t1 = min(rem, G.cfl_time())
+        G.unsplit_step(t1)
+        dts.append(t1)
+        rem -= t1
+    assert dts == ref_dts
+    same(G.w, R.get_prim(), "Orszag-Tang cells at t = 0.5")
+    same(G.B, R.get_faceB(), "Orszag-Tang face B at t = 0.5")
+    # ... and its device advance loop in one call
+    res = H.advance(T)
+    assert res.steps == len(ref_dts) and res.retries == 0 and res.last_dt == ref_dts[-1]
+    same(H.w, R.get_prim(), "Orszag-Tang cells, device advance")
+    same(H.B, R.get_faceB(), "Orszag-Tang face B, device advance")
+    assert div_b_max(H.B, n, 3) < 1e-13
+    R.close()
+
+
+def test_blast_3d_256_exact_vs_reference_distgrid():
+    n, steps = 256, 3
+    ref = reference("hydro")
+    w, d = problems.blast_3d(n, ghosts=2, p_in=10.0)
+    R = ref.RefGrid(3, (n, n, n), (d, d, d), ghosts=2, dist=True, riemann=dg.RIEMANN_EXACT, limiter=dg.LIMITER_MC,
+                    cfl=dg.CFL_ADD, core_count=os.cpu_count() or 1)
+    R.set_prim(w)
+    R.set_boundary([])
+    ref_dts = [R.step_cfl() for _ in range(steps)]
+    ref_w = R.get_prim()
+    R.close()
+    G = dg.Grid3D(n, n, n, d, d, d, ghosts=2, config=dg.Config(riemann=dg.RIEMANN_EXACT, limiter=dg.LIMITER_MC))
+    G.w[...] = w
+    dts = [G.advance_steps(1).last_dt for _ in range(steps)]
+    assert np.allclose(dts, ref_dts, rtol=1e-12, atol=0), (dts, ref_dts)
+    l1 = problems.rel_l1(G.w, ref_w)
+    assert np.all(l1 <= TOL_L1), l1
+
+
+def test_mixed_shear_layer_1024_2000_steps_vs_fp64():
+    n, steps = 1024, 2000
+    F = kh_device(n)[0]
+    M = kh_device(n, dg.PREC_MIXED)[0]
+    F.advance_steps(steps)
+    M.advance_steps(steps)
+    g = 2
+    l1 = problems.rel_l1(M.w[g:-g, g:-g], F.w[g:-g, g:-g])
+    assert np.all(l1 <= TOL_MIXED), dict(zip(["rho", "p", "vx", "vy", "vz"], l1))
+    assert np.any(M.w != F.w)  # really the FP32 path
+
+
+def test_mixed_orszag_tang_1024_to_t05_vs_fp64():
+    n, T = 1024, 0.5
+    F = ot_device(n)[0]
+    M = ot_device(n, dg.PREC_MIXED)[0]
+    F.advance(T)
+    M.advance(T)
+    g = 3
+    l1 = problems.rel_l1(M.w[g:-g, g:-g], F.w[g:-g, g:-g])
+    assert np.all(l1 <= TOL_MIXED), dict(zip(["rho", "p", "vx", "vy", "vz", "Bx", "By", "Bz"], l1))
+    lb = problems.rel_l1(M.B[g:-g, g:-g, :2], F.B[g:-g, g:-g, :2])
+    assert np.all(lb <= TOL_MIXED), lb
+    assert div_b_max(M.B, n, g) < 1e-13
+    assert np.any(M.w != F.w)
