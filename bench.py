@@ -552,6 +552,47 @@ def stated_length_report(n=1024, kh_steps=2000, ot_time=0.5):
     return out
 
 
+def custom_bc_report(n=1024, steps=20, warmup=3):
+    """A user GhostFill element (an inflow jet on X-, the reference's Jet
+    pattern) on the n^2 shear layer against the same grid with built-in
+    elements only: wall time per CFL step of advance_steps. The user element
+    runs on the host; only the slabs along its face cross the host link."""
+    import torch
+
+    import dragon_b200 as dg
+    from dragon_b200 import problems
+
+    class Jet(dg.GhostFill):
+        def __init__(self, dy, g):
+            super().__init__("X-", True)
+            self.dy, self.g = dy, g
+
+        def apply(self, grid):
+            w, g = grid.w, self.g
+            ys = (np.arange(w.shape[1]) - g + 0.5) * self.dy
+            jet = np.abs(ys - 0.5) < 0.1
+            for gl in range(1, g + 1):
+                w[g - gl] = w[g]
+                w[g - gl, jet] = (2.0, 3.0, 1.5, 0.0, 0.0)
+
+    w0, dx, dy = problems.kelvin_helmholtz_2d(n, ghosts=2, seed=1234)
+    out = {"workload": f"shear layer {n}^2, X- inflow jet (user element) + Outflow X+ + Periodic Y"}
+    for name, bl in (("builtin", dg.Outflow("X") + dg.Periodic("Y")),
+                     ("user_element", dg.Periodic("Y") + Jet(dy, 2))):
+        G = dg.Grid2D(n, n, dx, dy, ghosts=2, config=dg.Config(riemann=dg.RIEMANN_HLLC, limiter=dg.LIMITER_VANLEER))
+        G.w[...] = w0
+        G.boundary = bl
+        G.advance_steps(warmup)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        G.advance_steps(steps)
+        torch.cuda.synchronize()
+        out[name + "_ms_per_step"] = (time.perf_counter() - t0) / steps * 1e3
+        G.close()
+    out["ratio"] = out["user_element_ms_per_step"] / out["builtin_ms_per_step"]
+    return out
+
+
 def _batch_run(precision, steps, one_by_one_steps):
     """One precision of the batched uneven-instance workload: the batch
     (autotuned, then timed over `steps` steps) and the same grids advanced one
@@ -677,6 +718,8 @@ def summary_of(d):
         out["learned_guess"]["train_samples"] = g["train"]["samples"]
         out["learned_guess"]["iters_per_solve"] = {k: g[k]["newton_iters_per_solve"] for k in g
                                                    if isinstance(g[k], dict) and "newton_iters_per_solve" in g[k]}
+    if "custom_bc" in d:
+        out["user_ghostfill_step_vs_builtin"] = d["custom_bc"]["ratio"]
     if "batch" in d:
         b = d["batch"]
         out["batch_c5"] = {"mixed_value": b["value"], "fp64_value": b["fp64"]["value"],
@@ -863,6 +906,8 @@ def run_gpu(args):
             detail["mhd"] = mhd_report()
         if not args.no_stated_length:
             detail["stated_length"] = stated_length_report()
+        if not args.no_custom_bc:
+            detail["custom_bc"] = custom_bc_report()
         if not args.no_cpu_baseline:
             cb, why = reference_baseline(1000, 0, budget_s=args.cpu_budget)
             line["cpu_baseline"] = cb if cb else {"unavailable": why}
@@ -889,6 +934,7 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned star-pressure guess report")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched uneven-instance report")
     ap.add_argument("--no-mhd", action="store_true", help="skip the 2D MHD (Orszag-Tang) report")
+    ap.add_argument("--no-custom-bc", action="store_true", help="skip the user-GhostFill step cost")
     ap.add_argument("--no-stated-length", action="store_true",
                     help="skip the mixed-vs-FP64 comparison at the configurations' stated lengths")
     ap.add_argument("--cpu-budget", type=float, default=15.0)

@@ -68,13 +68,20 @@ class GhostFill:
     def state(self) -> Sequence[float]:
         return ()
 
+    # Interior layers next to its faces a user element reads (None: the ghost
+    # width). Only these and the ghost layers of its faces cross the host link.
+    reach = None
+
     def apply(self, grid) -> None:
         """GhostFill::apply(Grid&) (GhostFill.hpp:16-30). A user element
         subclasses GhostFill and overrides this to fill grid's ghost cells on
         the host (grid.w / grid.B, or grid[i, j] with ghost coordinates), like
         the reference's Jet (Jets.hpp:12-39). Grids then run such lists on the
-        host-driven slow path: the built-in elements stay on the device, the
-        state crosses to the host around each user element."""
+        host-driven path: the built-in elements stay on the device, and around
+        each user element only the slabs along its faces cross to the host and
+        back: its ghost layers and `reach` interior layers next to them, over
+        the whole transverse extent (corners included). apply must read and
+        write inside those slabs."""
         raise NotImplementedError(f"{type(self).__name__} is a built-in element applied on the device")
 
     @property

@@ -73,6 +73,7 @@ enum ErrStage : int {
     ST_UNPHYSICAL = 4,    // unphysical committed state (Unsplit.cpp:97,192; Splitting.cpp:109)
     ST_CFL_ZERO = 5,      // max signal speed zero (CFL.cpp:102,117,134)
     ST_BARRIER = 6,       // a grid barrier of the cooperative prologue gave up waiting
+    ST_TILE_LOAD = 7,     // a tile load into shared memory did not complete within its wait limit
 };
 
 __device__ __forceinline__ void record_error(StepCtl* ctl, int stage, long long cell) {

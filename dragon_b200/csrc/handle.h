@@ -2,6 +2,7 @@
 // batched step (batch.cu) shares with the single-grid runtime (runtime.cu).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <utility>
@@ -86,6 +87,10 @@ struct dragon_grid {
     // of devices without cooperative launch
     int dbg_stall_cta = -1;
     bool dbg_no_coop = false;
+    // TMA tensor maps of the two state buffers for the fused 2D hydro kernels
+    // (FP64, mixed), encoded on first use
+    CUtensorMap tmap[2][2];
+    bool tmap_ok[2][2] = {{false, false}, {false, false}};
 };
 
 namespace dgpu_rt {

@@ -2,6 +2,7 @@
 // family so the library builds in parallel. Each returns 0 on a clean launch.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "grid.cuh"
@@ -18,10 +19,15 @@ int launch_step1d(bool mhd, int solver, const Geo& G, const double* win, double*
 // Mixed FP32/FP64 1D hydro sweep (step1d_mixed.cu).
 int launch_step1d_mixed(int solver, const Geo& G, const double* win, double* wout, StepCtl* ctl, const StepArgs& sa,
                         cudaStream_t st);
+// The fused 2D hydro steps load each tile with one TMA copy through `map`, a
+// tensor map of the input buffer with the box step2d_tile_box gives (columns,
+// rows, fields) for the FP64 (mixed = 0) or the mixed kernel.
+constexpr int kMx2dTI = 16;
+int step2d_tile_box(int mixed, int box[3]);
 int launch_step2d_hydro(int solver, const Geo& G, const double* win, double* wout, StepCtl* ctl, const StepArgs& sa,
-                        cudaStream_t st);
+                        const CUtensorMap* map, cudaStream_t st);
 int launch_step2d_hydro_mixed(int solver, const Geo& G, const double* win, double* wout, StepCtl* ctl,
-                              const StepArgs& sa, cudaStream_t st);
+                              const StepArgs& sa, const CUtensorMap* map, cudaStream_t st);
 int launch_step2d_mhd(int solver, const Geo& G, const Geo& FG, const double* w, double* wout, const double* B,
                       double* Bout, const MhdScratch& S, StepCtl* ctl, const StepArgs& sa, cudaStream_t st);
 int launch_step2d_mhd_mixed(int solver, const Geo& G, const Geo& FG, const double* w, double* wout, const double* B,

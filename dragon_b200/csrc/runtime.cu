@@ -10,11 +10,13 @@
 // is still intact; the host then halves dt and retries exactly like the
 // reference's catch block (CFL.cpp:194-209).
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -203,6 +205,44 @@ void collect_profile(dragon_grid* h) {
     h->ev_pending.clear();
 }
 
+// cuTensorMapEncodeTiled from the driver, looked up once.
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// The tensor map of state buffer b for the fused 2D hydro kernel (mixed or
+// FP64): the five field planes as a 3D FP64 tensor (padded columns, padded
+// rows, fields) with the kernel's tile box; encoded on first use, the buffers
+// live as long as the handle.
+static int state_tile_map(dragon_grid* h, int mixed, int b, const CUtensorMap** out) {
+    if (!h->tmap_ok[mixed][b]) {
+        auto encode = tensor_map_encoder();
+        if (!encode) return fail(DRAGON_GPU_ECUDA, "cuTensorMapEncodeTiled is not available");
+        int box[3];
+        step2d_tile_box(mixed, box);
+        const cuuint64_t dims[3] = {(cuuint64_t)h->cg.ext[1], (cuuint64_t)h->cg.ext[0], 5};
+        const cuuint64_t strides[2] = {(cuuint64_t)h->cg.pitch * sizeof(double), (cuuint64_t)h->cg.plane * sizeof(double)};
+        const cuuint32_t boxd[3] = {(cuuint32_t)box[0], (cuuint32_t)box[1], (cuuint32_t)box[2]};
+        const cuuint32_t elem[3] = {1, 1, 1};
+        const CUresult r = encode(&h->tmap[mixed][b], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, h->w[b], dims, strides, boxd,
+                                  elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return fail(DRAGON_GPU_ECUDA, "cuTensorMapEncodeTiled failed for the state tile");
+        h->tmap_ok[mixed][b] = true;
+    }
+    *out = &h->tmap[mixed][b];
+    return 0;
+}
+
 int launch_step(dragon_grid* h, int c) {
     const StepArgs sa = step_args(h, c ^ 1);
     if (sa.exact_guess == GUESS_LEARNED && h->solver == RS_EXACT && !sa.mlp)
@@ -232,11 +272,14 @@ int launch_step(dragon_grid* h, int c) {
             rc = launch_step2d_mhd(h->solver, h->cg, h->fg, h->w[c], h->w[c ^ 1], h->B[c], h->B[c ^ 1], h->mhd_s,
                                    h->ctl, sa, h->stream);
         }
-        if (h->dim == 2) nk = kMhd2DKernels;
+        // 2D: the ghost-frame copy, then seven phase kernels (FP64) or the fused kernel (mixed)
+        if (h->dim == 2) nk = 1 + (h->cfg.precision == 1 ? 1 : kMhd2DKernels);
     } else if (h->dim == 2) {
-        rc = (h->cfg.precision == 1)
-                 ? launch_step2d_hydro_mixed(h->solver, h->cg, h->w[c], h->w[c ^ 1], h->ctl, sa, h->stream)
-                 : launch_step2d_hydro(h->solver, h->cg, h->w[c], h->w[c ^ 1], h->ctl, sa, h->stream);
+        const int mixed = h->cfg.precision == 1 ? 1 : 0;
+        const CUtensorMap* map = nullptr;
+        if ((rc = state_tile_map(h, mixed, c, &map))) return rc;
+        rc = mixed ? launch_step2d_hydro_mixed(h->solver, h->cg, h->w[c], h->w[c ^ 1], h->ctl, sa, map, h->stream)
+                   : launch_step2d_hydro(h->solver, h->cg, h->w[c], h->w[c ^ 1], h->ctl, sa, map, h->stream);
     } else {
         rc = launch_step3d_hydro(h->solver, h->cg, h->w[c], h->w[c ^ 1], h->h3_s, h->ctl, sa, h->stream);
         nk = kHydro3DKernels;
@@ -467,6 +510,7 @@ const char* stage_name(int s) {
         case ST_UNPHYSICAL: return "Unphysical state would be produced";
         case ST_CFL_ZERO: return "CFL timestep failed: max signal speed is zero";
         case ST_BARRIER: return "ghost fill failed: a grid barrier gave up waiting";
+        case ST_TILE_LOAD: return "step failed: a tile load did not complete";
         default: return "step failed";
     }
 }
@@ -554,7 +598,7 @@ int advance_finish(dragon_grid* h, dragon_advance_stats* st) {
                 if (h->split_mode) h->sweep_step += ks;
                 return fail(DRAGON_GPU_ECFL, stage_name(stage));
             }
-            if (stage == ST_BARRIER) {  // the ghosts may be incomplete: no retry on them
+            if (stage == ST_BARRIER || stage == ST_TILE_LOAD) {  // not a physics failure: no retry
                 if (st) st->failure.code = DRAGON_GPU_ECUDA;
                 if (h->split_mode) h->sweep_step += ks;
                 h->imax_valid = false;

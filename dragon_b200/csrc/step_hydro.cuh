@@ -12,15 +12,17 @@
 #include "grid.cuh"
 #include "recon.cuh"
 #include "riemann.cuh"
+#include "tma.cuh"
 
 namespace dgpu {
 
 template <int TI, int TJ>
 struct Smem2DH {
     static constexpr int HI = TI + 2, HJ = TJ + 2;
+    static constexpr int WC = TJ + 6;  // tile columns as loaded: the halo, plus one for an odd first column
     double hs[4][5][HI][HJ];  // xL, xR, yL, yR half states (primitive)
     union U {
-        double w[5][TI + 4][TJ + 4];
+        double w[5][TI + 4][WC];  // w[f][a][b + off]: tile row a, column b, off the load's column offset
         struct F {
             double fx[5][TI + 1][TJ + 2];
             double fy[5][TI + 2][TJ + 1];
@@ -28,7 +30,13 @@ struct Smem2DH {
     } u;
     double red[32];
     unsigned long long stat[7];
+    uint64_t bar;
 };
+
+// First padded column of a tile's TMA box (even, so the box starts 16-byte
+// aligned) and the offset of the tile's own first column inside the box.
+__device__ __forceinline__ int tile_col0(int j0, int g) { return (j0 - 2 + g) & ~1; }
+__device__ __forceinline__ int tile_off(int j0, int g) { return (j0 - 2 + g) & 1; }
 
 enum { HS_XL = 0, HS_XR = 1, HS_YL = 2, HS_YR = 3 };
 
@@ -87,8 +95,9 @@ __device__ __forceinline__ void copy_ghosts_2d(const Geo& G, const double* __res
 
 template <int SOLVER, int TI, int TJ, int NT>
 __global__ void __launch_bounds__(NT, 2)
-k_step2d_hydro(Geo G, const double* __restrict__ win, double* __restrict__ wout, StepCtl* ctl, StepArgs sa) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+k_step2d_hydro(Geo G, const double* __restrict__ win, double* __restrict__ wout, StepCtl* ctl, StepArgs sa,
+               const __grid_constant__ CUtensorMap tile_map) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     Smem2DH<TI, TJ>& S = *reinterpret_cast<Smem2DH<TI, TJ>*>(smem_raw);
     __shared__ int s_skip;
     if (cta_should_skip(ctl, &s_skip)) return;
@@ -104,18 +113,14 @@ k_step2d_hydro(Geo G, const double* __restrict__ win, double* __restrict__ wout,
     int first_order = 0;
     if (threadIdx.x < 7) S.stat[threadIdx.x] = 0;
 
-    // P0: tile + two-cell halo of the primitive state
-    constexpr int WI = TI + 4, WJ = TJ + 4;
-    for (int t = threadIdx.x; t < WI * WJ; t += NT) {
-        const int a = t / WJ, b = t % WJ;
-        const int i = i0 - 2 + a, j = j0 - 2 + b;
-        if (i >= -g && i < nx + g && j >= -g && j < ny + g) {
-            const long long m = gidx2(G, i, j);
-#pragma unroll
-            for (int f = 0; f < 5; f++) S.u.w[f][a][b] = win[f * PL + m];
-        }
-    }
-    __syncthreads();
+    // P0: tile + two-cell halo of the primitive state, one TMA copy of the five
+    // planes (padded rows i0-2+g .., columns from the even column at or
+    // before j0-2+g); cells past the padded array read zeros and are not used
+    static_assert(sizeof(double) * 4 * 5 * (TI + 2) * (TJ + 2) % 128 == 0, "the tile must start 128-byte aligned");
+    const int off = tile_off(j0, g);
+    if (!load_state_tile(&S.u.w[0][0][0], &tile_map, tile_col0(j0, g), i0 - 2 + g,
+                         (unsigned)sizeof(S.u.w), &S.bar, ctl))
+        return;
 
     // P1: MUSCL-Hancock half states in x and y for cells [-1, TI] x [-1, TJ]
     // (computeHalfStates_X/Y, Unsplit.cpp:292-342)
@@ -126,6 +131,7 @@ k_step2d_hydro(Geo G, const double* __restrict__ win, double* __restrict__ wout,
         if (!(i >= -1 && i <= nx && j >= -1 && j <= ny)) continue;
         auto W = [&](int aa, int bb) {
             Prim<double> r;
+            bb += off;
             r.rho = S.u.w[0][aa][bb]; r.p = S.u.w[1][aa][bb];
             r.vx = S.u.w[2][aa][bb]; r.vy = S.u.w[3][aa][bb]; r.vz = S.u.w[4][aa][bb];
             r.Bx = r.By = r.Bz = 0;

@@ -1,47 +1,56 @@
-// Single-grid mixed FP32/FP64 2D MHD step: the seven phase bodies of
-// step_mhd_mixed.cuh, one 32 x 8 tile per CTA. Compiled with FMA contraction
+// Single-grid mixed FP32/FP64 2D MHD step: the fused one-kernel step of
+// step_mhd_fused.cuh (the batched step runs the seven phase bodies of
+// step_mhd_mixed.cuh as work items instead). Compiled with FMA contraction
 // and fast single-precision division / square root.
+#include <algorithm>
+
 #include "launchers.h"
-#include "step_mhd_mixed.cuh"
+#include "step_mhd_fused.cuh"
 
 namespace dgpu {
 
 namespace {
 
-__global__ void k_mx_halfstates(Mhd2DMixedArgs A) { mx_halfstates(A, launch_tile()); }
-template <int SOLVER, bool FINAL>
-__global__ void __launch_bounds__(256, 3) k_mx_fluxes(Mhd2DMixedArgs A) { mx_fluxes<SOLVER, FINAL>(A, launch_tile()); }
-template <bool FINAL>
-__global__ void k_mx_edges(Mhd2DMixedArgs A) { mx_edges<FINAL>(A, launch_tile()); }
-__global__ void k_mx_half(Mhd2DMixedArgs A) { mx_half(A, launch_tile()); }
-__global__ void k_mx_update(Mhd2DMixedArgs A) { mx_update(A, launch_tile()); }
+// Strips of kFuseTJ columns marching kFuseR rows per iteration, kFuseNT threads.
+constexpr int kFuseTJ = 32, kFuseR = 4, kFuseNT = 128;
 
+// One fused launch: a strip of columns per blockIdx.x, a segment of rows per
+// blockIdx.y. Segments are sized so the CTAs fill the device's resident
+// slots about once (each segment costs one ring-filling iteration extra).
 template <int SOLVER>
-int launch_mx(const Geo& G, const Geo& FG, const double* w, double* wout, const double* B, double* Bout,
-              const MhdScratchF& S, StepCtl* ctl, const StepArgs& sa, cudaStream_t st) {
-    Mhd2DMixedArgs A{G, FG, w, wout, B, Bout, S, ctl, sa};
-    const dim3 blk(kTileJ, kTileI);
-    auto grid_for = [&](int ni, int nj) { return dim3((nj + kTileJ - 1) / kTileJ, (ni + kTileI - 1) / kTileI); };
+int launch_fused(const Geo& G, const Geo& FG, const double* w, double* wout, const double* B, double* Bout,
+                 StepCtl* ctl, const StepArgs& sa, cudaStream_t st) {
+    auto kern = k_mhd2d_fused_mixed<SOLVER, kFuseTJ, kFuseR, kFuseNT>;
+    const size_t smem = sizeof(FusedMhdSmem<kFuseTJ, kFuseR>);
+    static int slots = 0;
+    if (slots == 0) {
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 1;
+        int dev = 0, sms = 0, occ = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kFuseNT, smem) != cudaSuccess || occ < 1)
+            return 1;
+        slots = occ * sms;
+    }
     const int nx = G.n[0], ny = G.n[1];
+    const int strips = (ny + kFuseTJ - 1) / kFuseTJ;
+    const int segs_wanted = std::max(1, slots / strips);
+    int seg = (nx + segs_wanted - 1) / segs_wanted;
+    seg = std::max(4 * kFuseR, (seg + kFuseR - 1) / kFuseR * kFuseR);
+    const dim3 grid(strips, (nx + seg - 1) / seg);
     if (launch_mhd2d_copy_frame(G, FG, w, wout, B, Bout, st)) return 1;
-    k_mx_halfstates<<<grid_for(nx + 4, ny + 4), blk, 0, st>>>(A);
-    k_mx_fluxes<SOLVER, false><<<grid_for(nx + 4, ny + 4), blk, 0, st>>>(A);
-    k_mx_edges<false><<<grid_for(nx + 3, ny + 3), blk, 0, st>>>(A);
-    k_mx_half<<<grid_for(nx + 2, ny + 2), blk, 0, st>>>(A);
-    k_mx_fluxes<SOLVER, true><<<grid_for(nx + 2, ny + 2), blk, 0, st>>>(A);
-    k_mx_edges<true><<<grid_for(nx + 1, ny + 1), blk, 0, st>>>(A);
-    k_mx_update<<<grid_for(nx, ny), blk, 0, st>>>(A);
+    kern<<<grid, kFuseNT, smem, st>>>(G, FG, w, wout, B, Bout, ctl, sa, seg);
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 
 }  // namespace
 
 int launch_step2d_mhd_mixed(int solver, const Geo& G, const Geo& FG, const double* w, double* wout, const double* B,
-                            double* Bout, const MhdScratchF& S, StepCtl* ctl, const StepArgs& sa, cudaStream_t st) {
+                            double* Bout, const MhdScratchF&, StepCtl* ctl, const StepArgs& sa, cudaStream_t st) {
     switch (solver) {
-        case RS_HLL: return launch_mx<RS_HLL>(G, FG, w, wout, B, Bout, S, ctl, sa, st);
-        case RS_HLLE: return launch_mx<RS_HLLE>(G, FG, w, wout, B, Bout, S, ctl, sa, st);
-        default: return launch_mx<RS_HLLD>(G, FG, w, wout, B, Bout, S, ctl, sa, st);
+        case RS_HLL: return launch_fused<RS_HLL>(G, FG, w, wout, B, Bout, ctl, sa, st);
+        case RS_HLLE: return launch_fused<RS_HLLE>(G, FG, w, wout, B, Bout, ctl, sa, st);
+        default: return launch_fused<RS_HLLD>(G, FG, w, wout, B, Bout, ctl, sa, st);
     }
 }
 

@@ -33,6 +33,7 @@ struct SmemMixed {
     } u;
     double red[32];
     unsigned long long stat[6];
+    uint64_t bar;
 };
 
 template <int TI, int TJ>
@@ -71,8 +72,9 @@ __device__ __forceinline__ double block_min(double v, double* scratch) {
 // faster than two CTAs at 110 registers on a 2048^2 shear layer, same results.
 template <int SOLVER, int TI, int TJ, int NT>
 __global__ void __launch_bounds__(NT, 3)
-k_step2d_hydro_mixed(Geo G, const double* __restrict__ win, double* __restrict__ wout, StepCtl* ctl, StepArgs sa) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+k_step2d_hydro_mixed(Geo G, const double* __restrict__ win, double* __restrict__ wout, StepCtl* ctl, StepArgs sa,
+                     const __grid_constant__ CUtensorMap tile_map) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     SmemMixed<TI, TJ>& S = *reinterpret_cast<SmemMixed<TI, TJ>*>(smem_raw);
     __shared__ int s_skip;
     if (cta_should_skip(ctl, &s_skip)) return;
@@ -88,15 +90,26 @@ k_step2d_hydro_mixed(Geo G, const double* __restrict__ win, double* __restrict__
     int first_order = 0;
     if (threadIdx.x < 6) S.stat[threadIdx.x] = 0;
 
-    constexpr int WI = TI + 4, WJ = TJ + 4;
+    constexpr int WI = TI + 4, WJ = TJ + 4, WC = TJ + 6;
+    // the FP64 tile (five planes, padded rows i0-2+g .., columns from the even
+    // column at or before j0-2+g) arrives by one TMA copy into a staging area
+    // that the half states overwrite later
+    static_assert(sizeof(double) * 5 * WI * WC <= sizeof(S.hs), "the FP64 tile must fit in the half-state area");
+    double* stg = reinterpret_cast<double*>(&S.hs[0][0][0][0]);
+    const int off = (j0 - 2 + g) & 1;
+    if (!load_state_tile(stg, &tile_map, (j0 - 2 + g) & ~1, i0 - 2 + g, (unsigned)(sizeof(double) * 5 * WI * WC),
+                         &S.bar, ctl))
+        return;
+    auto T = [&](int f, int a, int b) { return stg[(f * WI + a) * WC + b + off]; };
     // pressure reference of the tile (mixed.cuh, pressure offset): the smallest
     // pressure it loads, with HLLC; zero (absolute pressures) otherwise
     double pref = 0.0;
     if constexpr (SOLVER == RS_HLLC) {
         double pmin = INFINITY;
         for (int t = threadIdx.x; t < WI * WJ; t += NT) {
-            const int i = i0 - 2 + t / WJ, j = j0 - 2 + t % WJ;
-            if (i >= -g && i < nx + g && j >= -g && j < ny + g) pmin = fmin(pmin, win[PL + gidx2(G, i, j)]);
+            const int a = t / WJ, b = t % WJ;
+            const int i = i0 - 2 + a, j = j0 - 2 + b;
+            if (i >= -g && i < nx + g && j >= -g && j < ny + g) pmin = fmin(pmin, T(1, a, b));
         }
         pref = block_min(pmin, S.red);
         if (!(pref > 0.0 && pref < INFINITY)) pref = 0.0;
@@ -106,10 +119,9 @@ k_step2d_hydro_mixed(Geo G, const double* __restrict__ win, double* __restrict__
         const int a = t / WJ, b = t % WJ;
         const int i = i0 - 2 + a, j = j0 - 2 + b;
         if (i >= -g && i < nx + g && j >= -g && j < ny + g) {
-            const long long m = gidx2(G, i, j);
 #pragma unroll
-            for (int f = 0; f < 5; f++) S.u.w[f][a][b] = (float)win[f * PL + m];
-            S.u.w[1][a][b] = (float)(win[PL + m] - pref);
+            for (int f = 0; f < 5; f++) S.u.w[f][a][b] = (float)T(f, a, b);
+            S.u.w[1][a][b] = (float)(T(1, a, b) - pref);
         }
     }
     __syncthreads();
@@ -255,11 +267,11 @@ k_step2d_hydro_mixed(Geo G, const double* __restrict__ win, double* __restrict__
     }
 }
 
-constexpr int kMxTI = 16, kMxTJ = 32, kMxNT = 256;
+constexpr int kMxTI = kMx2dTI, kMxTJ = 32, kMxNT = 256;
 
 template <int SOLVER>
 static int launch_mixed_t(const Geo& G, const double* win, double* wout, StepCtl* ctl, const StepArgs& sa,
-                          cudaStream_t st) {
+                          const CUtensorMap* map, cudaStream_t st) {
     auto kern = k_step2d_hydro_mixed<SOLVER, kMxTI, kMxTJ, kMxNT>;
     const size_t smem = sizeof(SmemMixed<kMxTI, kMxTJ>);
     static bool attr = false;
@@ -268,18 +280,18 @@ static int launch_mixed_t(const Geo& G, const double* win, double* wout, StepCtl
         attr = true;
     }
     dim3 grid((G.n[1] + kMxTJ - 1) / kMxTJ, (G.n[0] + kMxTI - 1) / kMxTI);
-    kern<<<grid, kMxNT, smem, st>>>(G, win, wout, ctl, sa);
+    kern<<<grid, kMxNT, smem, st>>>(G, win, wout, ctl, sa, *map);
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 
 int launch_step2d_hydro_mixed(int solver, const Geo& G, const double* win, double* wout, StepCtl* ctl,
-                              const StepArgs& sa, cudaStream_t st) {
+                              const StepArgs& sa, const CUtensorMap* map, cudaStream_t st) {
     switch (solver) {
-        case RS_HLLC: return launch_mixed_t<RS_HLLC>(G, win, wout, ctl, sa, st);
-        case RS_HLL: return launch_mixed_t<RS_HLL>(G, win, wout, ctl, sa, st);
-        case RS_HLLE: return launch_mixed_t<RS_HLLE>(G, win, wout, ctl, sa, st);
-        case RS_ROE: return launch_mixed_t<RS_ROE>(G, win, wout, ctl, sa, st);
-        default: return launch_mixed_t<RS_EXACT>(G, win, wout, ctl, sa, st);
+        case RS_HLLC: return launch_mixed_t<RS_HLLC>(G, win, wout, ctl, sa, map, st);
+        case RS_HLL: return launch_mixed_t<RS_HLL>(G, win, wout, ctl, sa, map, st);
+        case RS_HLLE: return launch_mixed_t<RS_HLLE>(G, win, wout, ctl, sa, map, st);
+        case RS_ROE: return launch_mixed_t<RS_ROE>(G, win, wout, ctl, sa, map, st);
+        default: return launch_mixed_t<RS_EXACT>(G, win, wout, ctl, sa, map, st);
     }
 }
 

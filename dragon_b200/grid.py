@@ -93,6 +93,38 @@ def _result(st: _lib.AdvanceStats) -> AdvanceResult:
                          st.newton_iters, st.exact_calls, st.trrs, st.muscl_first_order)
 
 
+class _SlabView:
+    """The grid as a user GhostFill element sees it on the ghost-slab path
+    (_GridBase._apply_custom): w, B, grid[i, j] and the geometry read and
+    write the host mirror directly, which is current only in the slabs along
+    the element's faces. Everything else is the grid's."""
+
+    def __init__(self, grid):
+        object.__setattr__(self, "_grid", grid)
+
+    @property
+    def w(self) -> np.ndarray:
+        return self._grid._w
+
+    @property
+    def B(self) -> np.ndarray:
+        if self._grid._B is None:
+            raise AttributeError("grid has no face-centred B")
+        return self._grid._B
+
+    def _B_(self):
+        return self.B
+
+    def __getitem__(self, idx):
+        return self._grid._w[self._grid._index(idx)]
+
+    def __setitem__(self, idx, value):
+        self._grid._w[self._grid._index(idx)] = np.asarray(value, dtype=np.float64)[: self._grid.nfields]
+
+    def __getattr__(self, name):
+        return getattr(self._grid, name)
+
+
 class _GridBase:
     dim = 0
 
@@ -231,7 +263,8 @@ class _GridBase:
     def _apply_boundary_host(self):
         """BoundaryList::apply (BoundaryList.hpp:79-93) with user elements: the
         device applies the runs of built-in entries (the implicit Outflow first),
-        each user element's apply(grid) runs on the host between them."""
+        each user element's apply(grid) runs on the host between them, on the
+        slabs along its faces only (_apply_custom)."""
         els = list(self._boundary)
         off = int(self._lib.dragon_gpu_boundary_entries(self._h)) - len(els)
         start = 0  # first device entry not yet applied
@@ -244,8 +277,74 @@ class _GridBase:
                 _lib.check(self._lib.dragon_gpu_apply_boundary_range(self._h, start, stop - start))
                 self._device_ran()
             if e is not None:
-                e.apply(self)
+                self._apply_custom(e)
             start = off + k + 1
+
+    def _custom_slabs(self, e):
+        """The layers a user element sees, per face of its mask: its ghost
+        layers and the `reach` interior layers next to them (GhostFill.reach,
+        default the ghost width), over the whole padded transverse extent.
+        Returns (axis, first, layers) in interior coordinates, or None when the
+        slabs would cover an axis end to end."""
+        g = self.ghosts
+        r = self.ghosts if e.reach is None else int(e.reach)
+        faces = e.get_faces()
+        out = []
+        for a in range(self.dim):
+            n = self.n[a]
+            neg, pos = faces & (1 << (2 * a)), faces & (1 << (2 * a + 1))
+            if (neg or pos) and (bool(neg) + bool(pos)) * (g + r) >= n + 2 * g - 1:
+                return None
+            if neg:
+                out.append((a, -g, g + r))
+            if pos:
+                out.append((a, n - r, g + r))
+        return out
+
+    def _slab_copy(self, axis, first, layers, faces, down):
+        """Copies layers [first, first + layers) along `axis` (cells, or face B
+        with faces = 1) between the device state and the host mirror, over the
+        padded transverse extent: down = True device to host."""
+        g = self.ghosts
+        arr = self._B if faces else self._w
+        count = ctypes.c_longlong()
+        _lib.check(self._lib.dragon_gpu_halo_size(self._h, axis, layers, faces, 1, ctypes.byref(count)))
+        nf = arr.shape[-1]
+        trans = [arr.shape[b] for b in range(self.dim) if b != axis]
+        sl = [slice(None)] * self.dim
+        sl[axis] = slice(first + g, first + g + layers)
+        sl = tuple(sl)
+        if down:
+            buf = np.empty(count.value)
+            _lib.check(self._lib.dragon_gpu_halo_pack(self._h, axis, first, layers, faces, 1, self._ptr(buf), 0))
+            # buffer order: field, layer, transverse axes (last fastest)
+            arr[sl] = np.moveaxis(np.moveaxis(buf.reshape(nf, layers, *trans), 0, -1), 0, axis)
+        else:
+            buf = np.ascontiguousarray(np.moveaxis(np.moveaxis(arr[sl], axis, 0), -1, 0))
+            _lib.check(self._lib.dragon_gpu_halo_unpack(self._h, axis, first, layers, faces, 1, self._ptr(buf), 0))
+
+    def _apply_custom(self, e):
+        """One user element on the host. When the device holds the newer state,
+        only the slabs along the element's faces cross the host link: they are
+        copied into the host mirror, the element's apply runs on a view of the
+        mirror that triggers no transfer, and the same slabs go back (cells,
+        and face B for MHD grids). Slabs that would span a whole axis fall
+        back to apply on the grid itself (a full round trip)."""
+        slabs = self._custom_slabs(e)
+        if slabs is None:
+            e.apply(self)
+            return
+        self._to_device()
+        if self._dev_dirty:
+            for a, first, layers in slabs:
+                self._slab_copy(a, first, layers, 0, True)
+                if self._B is not None:
+                    self._slab_copy(a, first, layers + 1, 1, True)
+        e.apply(_SlabView(self))
+        for a, first, layers in slabs:
+            self._slab_copy(a, first, layers, 0, False)
+            if self._B is not None:
+                self._slab_copy(a, first, layers + 1, 1, False)
 
     def _advance_host(self, dt: float, check_cfl: bool, split: bool) -> AdvanceResult:
         """Grid::advance_unsplit / advance_split (CFL.cpp:160-213) driven from

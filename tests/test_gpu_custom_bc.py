@@ -1,7 +1,9 @@
 """User GhostFill elements (the reference's Jet pattern, Jets.hpp:12-39) on the
 host-driven path: built-in elements stay on the device, the user's apply(grid)
-runs on the host between them in list order. Checked bit for bit against the
-oracle driven through the same sequence (ghost fill, user fill, CFL dt, step)."""
+runs on the host between them in list order, and only the slabs along the
+element's faces cross the host link. Checked bit for bit against the oracle
+driven through the same sequence (ghost fill, user fill, CFL dt, step), and
+against a full round trip of the state."""
 import numpy as np
 import pytest
 
@@ -98,3 +100,58 @@ def test_custom_between_builtins_keeps_list_order():
     assert len(calls) == 1
     # Periodic X comes last: it overwrites the marker's X- ghosts
     np.testing.assert_array_equal(G.w[0:2, 2:-2, 0], G.w[n:n + 2, 2:-2, 0])
+
+
+class FixedInflow(dg.GhostFill):
+    """A user element that writes a fixed state into every ghost cell (and,
+    on MHD grids, every ghost face) of its faces, reading the first interior
+    layer for the transverse velocity like an inflow that carries the shear."""
+
+    def __init__(self, faces, state, reach=None):
+        super().__init__(faces, True)
+        self.st = np.asarray(state, dtype=np.float64)
+        if reach is not None:
+            self.reach = reach
+
+    def apply(self, grid):
+        g = grid.ghosts
+        w = grid.w
+        w[:g] = self.st[: w.shape[-1]]
+        w[:g, :, 3] = w[g, :, 3]          # the first interior layer's vy
+        if grid.config.mhd:
+            grid.B[:g, :, 1] = 0.25       # transverse face field in the ghost faces
+
+
+@pytest.mark.parametrize("mhd", [False, True])
+def test_ghost_slab_path_equals_full_round_trip(mhd):
+    """The ghost-slab path (only the element's slabs cross the host link)
+    gives the same state bit for bit as a full round trip of the state
+    (forced by a reach that spans the axis)."""
+    n = 96
+    if mhd:
+        w0, B0, dx, dy = problems.orszag_tang_2d(n, ghosts=3)
+        st = [0.3, 0.2, 0.5, 0.0, 0.0, 0.2, 0.1, 0.0]
+        cfg = dg.Config(mhd=True, riemann=dg.RIEMANN_HLLX)
+    else:
+        w0, dx, dy = problems.kelvin_helmholtz_2d(n, ghosts=2, seed=13)
+        B0 = None
+        st = [2.0, 3.0, 1.5, 0.0, 0.0]
+        cfg = dg.Config(riemann=dg.RIEMANN_HLLC, limiter=dg.LIMITER_VANLEER)
+    out = []
+    for reach in (None, 10 * n):
+        G = dg.Grid2D(n, n, dx, dy, ghosts=3 if mhd else 2, config=cfg)
+        G.w[...] = w0
+        if mhd:
+            G.B[...] = B0
+        G.boundary = dg.Periodic("Y") + FixedInflow("X-", st, reach)
+        if mhd:
+            G.initialize_B_fields()
+        el = list(G.boundary)[-1]
+        assert (G._custom_slabs(el) is None) == (reach is not None)
+        res = G.advance_steps(6)
+        assert res.steps == 6
+        out.append((G.w.copy(), G.B.copy() if mhd else None))
+        G.close()
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    if mhd:
+        np.testing.assert_array_equal(out[0][1], out[1][1])
