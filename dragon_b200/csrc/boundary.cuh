@@ -228,6 +228,7 @@ __device__ __forceinline__ int prologue_bookkeeping(StepCtl* ctl, const Prologue
     if (pa.bookkeeping) {
         if (ctl->have_prev) {
             ctl->remaining -= ctl->t1;
+            ctl->elapsed += ctl->t1;
             ctl->steps_done += 1;
         }
         ctl->have_prev = 1;

@@ -43,6 +43,7 @@ struct StepCtl {
     double remaining;              // interval left in the current advance (CFL.cpp:188-213)
     double t1;                     // dt of the current step
     double max_speed;              // max CFL signal speed seen by the last prologue
+    double elapsed;                // sum of the committed steps' dt in this advance
     unsigned long long err_key;    // min over failures of (stage << 56 | linear cell index); ~0 = none
     int err;                       // non-zero once any failure was seen this batch
     int done;                      // advance finished (interval consumed or step budget reached)

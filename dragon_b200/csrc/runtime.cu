@@ -544,6 +544,7 @@ static int enqueue_batch(dragon_grid* h) {
 static bool account_last_step(dragon_grid* h, StepCtl& C) {
     if (C.have_prev) {
         C.remaining -= C.t1;
+        C.elapsed += C.t1;
         C.steps_done += 1;
     }
     C.have_prev = 1;
@@ -643,7 +644,9 @@ int advance_finish(dragon_grid* h, dragon_advance_stats* st) {
                 st->steps = C.steps_done;
                 st->retries = A.retries;
                 st->last_dt = C.t1;
-                st->time_advanced = (A.remaining - C.remaining);
+                // the interval consumed (Grid::advance's own bookkeeping), or for a
+                // step budget without an interval the sum of the steps' dt
+                st->time_advanced = std::isfinite(A.remaining) ? (A.remaining - C.remaining) : C.elapsed;
             }
             return 0;
         }

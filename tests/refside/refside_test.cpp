@@ -211,8 +211,8 @@ int run_blast3d_mhd() {
         X->boundary.apply(*X);
         X->initialize_B_fields();
     }
-    R.advance(0.004);
-    G.advance(0.004);
+    R.advance(0.01);
+    G.advance(0.01);
     const int g = R.getGhosts();
     const long bad = mismatches(G.cells(), R.cells(), (long)(n + 2 * g) * (n + 2 * g) * (n + 2 * g)) +
                      mismatches(G.faces(), R.faces(), (long)(n + 1 + 2 * g) * (n + 1 + 2 * g) * (n + 1 + 2 * g));
