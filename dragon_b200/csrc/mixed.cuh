@@ -16,10 +16,59 @@
 
 namespace dgpu {
 
-// FP64 energy of an FP32 primitive state (PrimitiveState::energy in FP64).
+// The FP64 arithmetic of the mixed path is not held to bit parity, so it
+// divides by neither gamma - 1 nor a density: it multiplies by the constant
+// 1 / (gamma - 1) and by the density's correctly rounded reciprocal
+// (__drcp_rn), which costs fewer FP64 instructions than an IEEE division.
+constexpr double kInvGm1 = 1.0 / kGm1;
+
+// FP64 energy of a primitive state (PrimitiveState::energy in FP64).
+template <bool MHD, class R>
+__device__ __forceinline__ double energy64_of(const Prim<R>& w) {
+    const double rho = w.rho, vx = w.vx, vy = w.vy, vz = w.vz;
+    double E = (double)w.p * kInvGm1 + (0.5 * rho) * (vx * vx + vy * vy + vz * vz);
+    if constexpr (MHD) {
+        const double bx = w.Bx, by = w.By, bz = w.Bz;
+        E += (bx * bx + by * by + bz * bz) * k1_8pi;
+    }
+    return E;
+}
 template <bool MHD>
 __device__ __forceinline__ double energy64(const Prim<float>& w) {
-    return energy<MHD>(cvt<double>(w));
+    return energy64_of<MHD>(w);
+}
+
+// ConservativeState <-> PrimitiveState in FP64 for the mixed path's committed
+// state (same formulas as to_cons / to_prim, divisions replaced as above).
+template <bool MHD>
+__device__ __forceinline__ Cons<double> to_cons64(const Prim<double>& w) {
+    Cons<double> u;
+    u.rho = w.rho;
+    u.mx = w.vx * w.rho;
+    u.my = w.vy * w.rho;
+    u.mz = w.vz * w.rho;
+    u.E = energy64_of<MHD>(w);
+    if constexpr (MHD) { u.Bx = w.Bx; u.By = w.By; u.Bz = w.Bz; }
+    else { u.Bx = u.By = u.Bz = 0; }
+    return u;
+}
+template <bool MHD>
+__device__ __forceinline__ Prim<double> to_prim64(const Cons<double>& u) {
+    const double inv = __drcp_rn(u.rho);
+    Prim<double> w;
+    w.rho = u.rho;
+    w.vx = u.mx * inv;
+    w.vy = u.my * inv;
+    w.vz = u.mz * inv;
+    double Eth = u.E - (u.mx * u.mx + u.my * u.my + u.mz * u.mz) * (0.5 * inv);
+    if constexpr (MHD) {
+        Eth -= (u.Bx * u.Bx + u.By * u.By + u.Bz * u.Bz) * k1_8pi;
+        w.Bx = u.Bx; w.By = u.By; w.Bz = u.Bz;
+    } else {
+        w.Bx = w.By = w.Bz = 0;
+    }
+    w.p = kGm1 * Eth;
+    return w;
 }
 
 // Primitive state from FP32 momenta / density and an FP64 total energy,
@@ -32,7 +81,7 @@ __device__ __forceinline__ Prim<float> prim_from(const Cons<float>& u, double E6
     w.vy = u.my / u.rho;
     w.vz = u.mz / u.rho;
     const double rho = u.rho, mx = u.mx, my = u.my, mz = u.mz;
-    double Eth = E64 - (mx * mx + my * my + mz * mz) / (2.0 * rho);
+    double Eth = E64 - (mx * mx + my * my + mz * mz) * (0.5 * __drcp_rn(rho));
     if constexpr (MHD) {
         const double bx = u.Bx, by = u.By, bz = u.Bz;
         Eth -= (bx * bx + by * by + bz * bz) * k1_8pi;
@@ -155,7 +204,7 @@ __device__ __forceinline__ Prim<float> abs_p(Prim<float> w, float ref_f) {
 __device__ __forceinline__ double energy64_off(const Prim<float>& w, double ref) {
     Prim<double> d = cvt<double>(w);
     d.p = ref + d.p;
-    return energy<false>(d);
+    return energy64_of<false>(d);
 }
 
 // Offset primitive state from FP32 momenta / density and an FP64 total energy;
@@ -167,7 +216,7 @@ __device__ __forceinline__ Prim<float> prim_from_off(const Cons<float>& u, doubl
     w.vy = u.my / u.rho;
     w.vz = u.mz / u.rho;
     const double rho = u.rho, mx = u.mx, my = u.my, mz = u.mz;
-    const double p = kGm1 * (E64 - (mx * mx + my * my + mz * mz) / (2.0 * rho));
+    const double p = kGm1 * (E64 - (mx * mx + my * my + mz * mz) * (0.5 * __drcp_rn(rho)));
     w.p = (float)(p - ref);
     w.Bx = w.By = w.Bz = 0.f;
     if (phys)

@@ -123,15 +123,15 @@ __device__ __forceinline__ void step1d_tile_mx(const Geo& G, const double* __res
         const Prim<double> w0 = load_prim<false>(win, PL, p);
         Prim<double> nw = w0;
         if (p >= 1 && p <= np - 2) {
-            Cons<double> U = to_cons<false>(w0);
+            Cons<double> U = to_cons64<false>(w0);
             double* u5[5] = {&U.rho, &U.E, &U.mx, &U.my, &U.mz};
 #pragma unroll
             for (int f = 0; f < 5; f++) *u5[f] += ((double)sF[f][q] - (double)sF[f][q + 1]) * dt_dx;
-            nw = to_prim<false>(U);
+            nw = to_prim64<false>(U);
             // the FP64 sweep applies the last interior face's flux difference
             // to this cell a second time with both sides that face (a zero
             // difference): a conservative round trip
-            if (p == np - 2) nw = to_prim<false>(to_cons<false>(nw));
+            if (p == np - 2) nw = to_prim64<false>(to_cons64<false>(nw));
         }
         const int c = p - G.g;
         if (c >= 0 && c < G.n[0]) {

@@ -281,12 +281,12 @@ __global__ void __launch_bounds__(NT) k_mhd2d_fused_mixed(Geo G, Geo FG, const d
                 const Cons<double> px0 = fm_get8(S.px[ring<S_t::K1>(i)], ch), px1 = fm_get8(S.px[ring<S_t::K1>(i + 1)], ch);
                 const Cons<double> py0 = fm_get8(S.py[ring<S_t::K1>(i)], cy), py1 = fm_get8(S.py[ring<S_t::K1>(i)], cy + 1);
                 {
-                    Cons<double> U = to_cons<true>(W);
+                    Cons<double> U = to_cons64<true>(W);
                     U = c_add<true>(U, c_mul<true>(c_sub<true>(px0, px1), hdx));
                     U = c_add<true>(U, c_mul<true>(c_sub<true>(py0, py1), hdy));
                     if (!is_finite<true>(U)) record_error(ctl, ST_NAN, m);
-                    Prim<double> wh = to_prim<true>(U);
-                    wh = body_field(wh, (bxh0 + bxh1) * 0.5, (byh0 + byh1) * 0.5, bzh, sa.ct_energy);
+                    Prim<double> wh = to_prim64<true>(U);
+                    wh = body_field64(wh, (bxh0 + bxh1) * 0.5, (byh0 + byh1) * 0.5, bzh, sa.ct_energy);
                     fm_put3(S.eh[ring<S_t::K1>(i)], c, body_e(wh));
                 }
                 const double dBx = (bx1 - bx0) * dt_dx, dBy = (by1 - by0) * dt_dy;
@@ -375,13 +375,13 @@ __global__ void __launch_bounds__(NT) k_mhd2d_fused_mixed(Geo G, Geo FG, const d
                 const double by1 = B[FP + gF(i, j + 1)] - -(e11.z - e01.z) * dt_dx;
                 const double bz = B[2 * FP + mf] - ((e10.y - e00.y) * dt_dx - (e01.x - e00.x) * dt_dy);
                 const int cx = j - j0 - S_t::OC;
-                Cons<double> U = to_cons<true>(load_prim<true>(w, P, mc));
+                Cons<double> U = to_cons64<true>(load_prim<true>(w, P, mc));
                 U = c_add<true>(U, c_mul<true>(c_sub<true>(fm_get8(S.fx[ring<S_t::K1>(i)], cx),
                                                            fm_get8(S.fx[ring<S_t::K1>(i + 1)], cx)), dt_dx));
                 U = c_add<true>(U, c_mul<true>(c_sub<true>(fm_get8(S.fy[ring<S_t::K1>(i)], c),
                                                            fm_get8(S.fy[ring<S_t::K1>(i)], c + 1)), dt_dy));
                 if (!is_finite<true>(U)) record_error(ctl, ST_NAN, mc);
-                Prim<double> nw = body_field(to_prim<true>(U), (bx0 + bx1) * 0.5, (by0 + by1) * 0.5, bz, sa.ct_energy);
+                Prim<double> nw = body_field64(to_prim64<true>(U), (bx0 + bx1) * 0.5, (by0 + by1) * 0.5, bz, sa.ct_energy);
                 if (!is_physical<true>(nw)) record_error(ctl, ST_UNPHYSICAL, mc);
                 store_prim<true>(wout, P, mc, nw);
                 Bout[mf] = bx0;

@@ -37,6 +37,17 @@ struct Mhd2DMixedArgs {
     StepArgs sa;
 };
 
+// computeBodyField (B_fields.cpp:70-79) with the mixed path's FP64 conversions.
+__device__ __forceinline__ Prim<double> body_field64(Prim<double> w, double bx, double by, double bz, int mode) {
+    if (!protect_thermal(w, mode)) {
+        Cons<double> U = to_cons64<true>(w);
+        U.Bx = bx; U.By = by; U.Bz = bz;
+        return to_prim64<true>(U);
+    }
+    w.Bx = bx; w.By = by; w.Bz = bz;
+    return w;
+}
+
 __device__ __forceinline__ void st_prim8f(float* a, long long P, long long m, const Prim<float>& w) {
     a[m] = w.rho; a[P + m] = w.p; a[2 * P + m] = w.vx; a[3 * P + m] = w.vy; a[4 * P + m] = w.vz;
     a[5 * P + m] = w.Bx; a[6 * P + m] = w.By; a[7 * P + m] = w.Bz;
@@ -187,12 +198,12 @@ __device__ __forceinline__ void mx_half(const Mhd2DMixedArgs& A, const Tile2& T)
     const Cons<double> px0 = ld_cons8d(A.S.fx, SP, m), px1 = ld_cons8d(A.S.fx, SP, gidx2(F, i + 1, j));
     const Cons<double> py0 = ld_cons8d(A.S.fy, SP, m), py1 = ld_cons8d(A.S.fy, SP, gidx2(F, i, j + 1));
     {
-        Cons<double> U = to_cons<true>(W);
+        Cons<double> U = to_cons64<true>(W);
         U = c_add<true>(U, c_mul<true>(c_sub<true>(px0, px1), hdx));
         U = c_add<true>(U, c_mul<true>(c_sub<true>(py0, py1), hdy));
         if (!is_finite<true>(U)) record_error(A.ctl, ST_NAN, m);
-        Prim<double> wh = to_prim<true>(U);
-        wh = body_field(wh, (bxh0 + bxh1) * 0.5, (byh0 + byh1) * 0.5, bzh, A.sa.ct_energy);
+        Prim<double> wh = to_prim64<true>(U);
+        wh = body_field64(wh, (bxh0 + bxh1) * 0.5, (byh0 + byh1) * 0.5, bzh, A.sa.ct_energy);
         st_v3f(A.S.eh, SP, m, body_e(wh));
     }
     const double dBx = (A.B[gidx2(F, i + 1, j)] - A.B[gidx2(F, i, j)]) * dt_dx;
@@ -248,11 +259,11 @@ __device__ __forceinline__ void mx_update(const Mhd2DMixedArgs& A, const Tile2& 
         const double by1 = A.B[FP + gidx2(F, i, j + 1)] - -(e11.z - e01.z) * dt_dx;
         const double bz = A.B[2 * FP + gidx2(F, i, j)] - ((e10.y - e00.y) * dt_dx - (e01.x - e00.x) * dt_dy);
         const long long mc = gidx2(G, i, j), mf = gidx2(F, i, j);
-        Cons<double> U = to_cons<true>(load_prim<true>(A.w, P, mc));
+        Cons<double> U = to_cons64<true>(load_prim<true>(A.w, P, mc));
         U = c_add<true>(U, c_mul<true>(c_sub<true>(ld_cons8d(A.S.fx, SP, mf), ld_cons8d(A.S.fx, SP, gidx2(F, i + 1, j))), dt_dx));
         U = c_add<true>(U, c_mul<true>(c_sub<true>(ld_cons8d(A.S.fy, SP, mf), ld_cons8d(A.S.fy, SP, gidx2(F, i, j + 1))), dt_dy));
         if (!is_finite<true>(U)) record_error(A.ctl, ST_NAN, mc);
-        Prim<double> nw = body_field(to_prim<true>(U), (bx0 + bx1) * 0.5, (by0 + by1) * 0.5, bz, A.sa.ct_energy);
+        Prim<double> nw = body_field64(to_prim64<true>(U), (bx0 + bx1) * 0.5, (by0 + by1) * 0.5, bz, A.sa.ct_energy);
         if (!is_physical<true>(nw)) record_error(A.ctl, ST_UNPHYSICAL, mc);
         store_prim<true>(A.wout, P, mc, nw);
         A.Bout[mf] = bx0;

@@ -241,14 +241,14 @@ k_step2d_hydro_mixed(Geo G, const double* __restrict__ win, double* __restrict__
         const int i = i0 + a, j = j0 + b;
         if (!(i < nx && j < ny)) continue;
         const long long m = gidx2(G, i, j);
-        Cons<double> U = to_cons<false>(load_prim<false>(win, PL, m));
+        Cons<double> U = to_cons64<false>(load_prim<false>(win, PL, m));
         double* u5[5] = {&U.rho, &U.E, &U.mx, &U.my, &U.mz};
 #pragma unroll
         for (int f = 0; f < 5; f++) {
             *u5[f] += ((double)S.u.f.fx[f][a][b + 1] - (double)S.u.f.fx[f][a + 1][b + 1]) * dt_dx;
             *u5[f] += ((double)S.u.f.fy[f][a + 1][b] - (double)S.u.f.fy[f][a + 1][b + 1]) * dt_dy;
         }
-        const Prim<double> nw = to_prim<false>(U);
+        const Prim<double> nw = to_prim64<false>(U);
         if (!is_finite<false>(U)) record_error(ctl, ST_NAN, (long long)(i + g) * (ny + 2 * g) + (j + g));
         else if (!is_physical<false>(nw)) record_error(ctl, ST_UNPHYSICAL, (long long)(i + g) * (ny + 2 * g) + (j + g));
         store_prim<false>(wout, PL, m, nw);

@@ -190,3 +190,28 @@ def test_learned_needs_a_network_and_a_3d_grid():
     G.w[...] = w
     with pytest.raises(dg.grid._lib.DragonGPUError):
         G.advance_steps(1)
+
+
+@pytest.mark.parametrize("err_exp,max_iters_per_solve", [(0, 1.0), (6, 2.0)])
+def test_perfect_guess_arm_is_the_iteration_floor(err_exp, max_iters_per_solve):
+    """The measurement arm GUESS_PERFECT starts Newton from the converged star
+    pressure of an uncounted first solve: every counted solve then converges
+    in one iteration (two when the start carries a 1e-6 relative error), and
+    the states equal the reference mean-guess solve's to 1e-12."""
+    n, steps = 32, 4
+    out = {}
+    for name, guess, e in (("mean", dg.GUESS_MEAN, 0), ("perfect", dg.GUESS_PERFECT, err_exp)):
+        w, d = problems.blast_3d(n, ghosts=2, p_in=100.0)
+        G = dg.Grid3D(n, n, n, d, d, d, ghosts=2, config=dg.Config(
+            riemann=dg.RIEMANN_EXACT, limiter=dg.LIMITER_MC, exact_max_iters=64, exact_guess=guess,
+            perfect_guess_err_exp=e))
+        G.w[...] = w
+        G.advance_steps(steps)
+        out[name] = (G.w.copy(), G.newton_stats())
+        G.close()
+    st = out["perfect"][1]
+    assert st["exact_calls"] > 1000 and st["cap_hits"] == 0
+    assert st["newton_iters"] <= max_iters_per_solve * st["exact_calls"]
+    assert out["mean"][1]["newton_iters"] > 1.5 * st["exact_calls"]
+    l1 = problems.rel_l1(out["perfect"][0], out["mean"][0])
+    assert np.all(l1 <= 1e-12), l1
