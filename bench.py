@@ -40,7 +40,10 @@ go to stderr as one JSON line prefixed "detail: ".
 
 ``--impl reference`` times only the reference on the host cores and prints its
 own line. Multi-GPU (torchrun): every rank advances its own 1024^2 grid
-(replicas, weak scaling), timing is the max over ranks.
+(replicas, weak scaling; the headline), timing is the max over ranks; then one
+4096^2 grid sharded across the ranks in x slabs (DistGrid2D: halo exchange,
+CFL all-reduce, all-or-nothing commit over NCCL) is timed the same way
+("dist", strong scaling).
 """
 from __future__ import annotations
 
@@ -692,6 +695,43 @@ def batch_report(steps=500, one_by_one_steps=50):
     return out
 
 
+def dist_report(ws, dev, n=4096, steps=10, warmup=2):
+    """Strong scaling of one sharded grid (multi-GPU runs only): an n^2 shear
+    layer cut into ws x slabs (DistGrid2D over NCCL: per step the slabs' ghost
+    fill, x-halo exchange, CFL all-reduce MIN, step and all-or-nothing
+    commit), `steps` CFL steps timed with CUDA events on each slab's stream,
+    max over ranks."""
+    import torch
+    import torch.distributed as dist
+
+    import dragon_b200 as dg
+    from dragon_b200 import problems
+    from dragon_b200.dist import DistGrid2D
+
+    w0, dx, dy = problems.kelvin_helmholtz_2d(n, ghosts=2, seed=1234)
+    G = DistGrid2D(n, n, dx, dy, ghosts=2, config=dg.Config(riemann=dg.RIEMANN_HLLC, limiter=dg.LIMITER_VANLEER))
+    G.boundary = dg.Periodic()
+    G.scatter(w0)
+    del w0
+    G.advance_steps(warmup)
+    slab = G.local.grid
+    stream = torch.cuda.ExternalStream(slab._lib.dragon_gpu_stream(slab._h), device=dev)
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    G.advance_steps(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t = torch.tensor([e0.elapsed_time(e1)], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = t.item()
+    slab.close()
+    return {"workload": f"shear layer {n}^2 in {ws} x slabs (DistGrid2D, NCCL), HLLC, van Leer, periodic",
+            "steps": steps, "ms_per_step": ms / steps, "value": n * n * steps / (ms / 1e3), "unit": "cell-updates/s",
+            "scaling": "strong"}
+
+
 def summary_of(d):
     """The headline numbers of each detailed section, rounded (the bench line's
     last key, so a tail of the line keeps it)."""
@@ -720,6 +760,8 @@ def summary_of(d):
                                                    if isinstance(g[k], dict) and "newton_iters_per_solve" in g[k]}
     if "custom_bc" in d:
         out["user_ghostfill_step_vs_builtin"] = d["custom_bc"]["ratio"]
+    if "dist" in d:
+        out["distgrid_4096_strong"] = {"value": d["dist"]["value"], "ms_per_step": d["dist"]["ms_per_step"]}
     if "batch" in d:
         b = d["batch"]
         out["batch_c5"] = {"mixed_value": b["value"], "fp64_value": b["fp64"]["value"],
@@ -868,6 +910,7 @@ def run_gpu(args):
     e2e_serial_value = ws * N * N * e2e_steps / (e2e_serial_ms / 1e3)
     bytes_step = G.w.nbytes
     link = copy_bound(dev, bytes_step, N * N)
+    dist_sec = dist_report(ws, dev) if ws > 1 and not args.no_dist else None
 
     if rank == 0:
         peak, peak_kind = measured_peaks()
@@ -914,6 +957,8 @@ def run_gpu(args):
         line["e2e"].pop("copy_bound", None)
         line["e2e"]["copy_bound_value"] = link["value"]
         detail["e2e_copy_bound"] = link
+        if dist_sec is not None:
+            detail["dist"] = dist_sec
         line["summary"] = summary_of(detail)
         print("detail: " + json.dumps(detail), file=sys.stderr, flush=True)
         print(json.dumps(sig(line, 6)), flush=True)
@@ -935,6 +980,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched uneven-instance report")
     ap.add_argument("--no-mhd", action="store_true", help="skip the 2D MHD (Orszag-Tang) report")
     ap.add_argument("--no-custom-bc", action="store_true", help="skip the user-GhostFill step cost")
+    ap.add_argument("--no-dist", action="store_true", help="multi-GPU runs: skip the sharded 4096^2 grid")
     ap.add_argument("--no-stated-length", action="store_true",
                     help="skip the mixed-vs-FP64 comparison at the configurations' stated lengths")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
