@@ -93,6 +93,45 @@ def _result(st: _lib.AdvanceStats) -> AdvanceResult:
                          st.newton_iters, st.exact_calls, st.trrs, st.muscl_first_order)
 
 
+def custom_slabs(n, g, faces, reach=None):
+    """(axis, first, layers) per face in the mask `faces` of a grid with
+    interior extents n and g ghosts: the face's g ghost layers and `reach`
+    interior layers next to them (None: g). None when the slabs of an axis
+    would cover it end to end (a full round trip is then as cheap)."""
+    r = g if reach is None else int(reach)
+    out = []
+    for a, na in enumerate(n):
+        neg, pos = faces & (1 << (2 * a)), faces & (1 << (2 * a + 1))
+        if (neg or pos) and (bool(neg) + bool(pos)) * (g + r) >= na + 2 * g - 1:
+            return None
+        if neg:
+            out.append((a, -g, g + r))
+        if pos:
+            out.append((a, na - r, g + r))
+    return out
+
+
+def _slab_index(dim, axis, first, layers, g):
+    sl = [slice(None)] * dim
+    sl[axis] = slice(first + g, first + g + layers)
+    return tuple(sl)
+
+
+def slab_to_buffer(arr, dim, axis, first, layers, g):
+    """Layers [first, first + layers) along `axis` of a padded host array (last
+    axis: fields) in the order of dragon_gpu_halo_pack's buffer with corners:
+    field, layer, then the transverse axes over their padded extent (last
+    fastest)."""
+    return np.ascontiguousarray(np.moveaxis(np.moveaxis(arr[_slab_index(dim, axis, first, layers, g)], axis, 0), -1, 0))
+
+
+def buffer_to_slab(buf, arr, dim, axis, first, layers, g):
+    """The inverse of slab_to_buffer: writes a halo buffer into those layers of arr."""
+    nf = arr.shape[-1]
+    trans = [arr.shape[b] for b in range(dim) if b != axis]
+    arr[_slab_index(dim, axis, first, layers, g)] = np.moveaxis(np.moveaxis(buf.reshape(nf, layers, *trans), 0, -1), 0, axis)
+
+
 class _SlabView:
     """The grid as a user GhostFill element sees it on the ghost-slab path
     (_GridBase._apply_custom): w, B, grid[i, j] and the geometry read and
@@ -286,41 +325,21 @@ class _GridBase:
         default the ghost width), over the whole padded transverse extent.
         Returns (axis, first, layers) in interior coordinates, or None when the
         slabs would cover an axis end to end."""
-        g = self.ghosts
-        r = self.ghosts if e.reach is None else int(e.reach)
-        faces = e.get_faces()
-        out = []
-        for a in range(self.dim):
-            n = self.n[a]
-            neg, pos = faces & (1 << (2 * a)), faces & (1 << (2 * a + 1))
-            if (neg or pos) and (bool(neg) + bool(pos)) * (g + r) >= n + 2 * g - 1:
-                return None
-            if neg:
-                out.append((a, -g, g + r))
-            if pos:
-                out.append((a, n - r, g + r))
-        return out
+        return custom_slabs(self.n, self.ghosts, e.get_faces(), e.reach)
 
     def _slab_copy(self, axis, first, layers, faces, down):
         """Copies layers [first, first + layers) along `axis` (cells, or face B
         with faces = 1) between the device state and the host mirror, over the
         padded transverse extent: down = True device to host."""
-        g = self.ghosts
         arr = self._B if faces else self._w
         count = ctypes.c_longlong()
         _lib.check(self._lib.dragon_gpu_halo_size(self._h, axis, layers, faces, 1, ctypes.byref(count)))
-        nf = arr.shape[-1]
-        trans = [arr.shape[b] for b in range(self.dim) if b != axis]
-        sl = [slice(None)] * self.dim
-        sl[axis] = slice(first + g, first + g + layers)
-        sl = tuple(sl)
         if down:
             buf = np.empty(count.value)
             _lib.check(self._lib.dragon_gpu_halo_pack(self._h, axis, first, layers, faces, 1, self._ptr(buf), 0))
-            # buffer order: field, layer, transverse axes (last fastest)
-            arr[sl] = np.moveaxis(np.moveaxis(buf.reshape(nf, layers, *trans), 0, -1), 0, axis)
+            buffer_to_slab(buf, arr, self.dim, axis, first, layers, self.ghosts)
         else:
-            buf = np.ascontiguousarray(np.moveaxis(np.moveaxis(arr[sl], axis, 0), -1, 0))
+            buf = slab_to_buffer(arr, self.dim, axis, first, layers, self.ghosts)
             _lib.check(self._lib.dragon_gpu_halo_unpack(self._h, axis, first, layers, faces, 1, self._ptr(buf), 0))
 
     def _apply_custom(self, e):
