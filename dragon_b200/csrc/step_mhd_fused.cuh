@@ -136,7 +136,7 @@ template <int R>
 constexpr int kFill = R * ((6 + R - 1) / R);
 
 template <int SOLVER, int TJ, int R, int NT>
-__global__ void __launch_bounds__(NT) k_mhd2d_fused_mixed(Geo G, Geo FG, const double* __restrict__ w,
+__global__ void __launch_bounds__(NT, 2) k_mhd2d_fused_mixed(Geo G, Geo FG, const double* __restrict__ w,
                                                           double* __restrict__ wout, const double* __restrict__ B,
                                                           double* __restrict__ Bout, StepCtl* ctl, StepArgs sa,
                                                           int seg_rows) {
@@ -186,12 +186,14 @@ __global__ void __launch_bounds__(NT) k_mhd2d_fused_mixed(Geo G, Geo FG, const d
             }
         }
         __syncthreads();
-        // ---- S1: half states
+        // ---- S1: half states, one item per (cell, direction): x items first
         {
             const RowSpan rs = span_of<R>(a, se, 2, sb - 2);
-            const int n = (rs.hi - rs.lo) * S_t::CH;
-            for (int t = threadIdx.x; t < n; t += NT) {
-                const int i = rs.lo + t / S_t::CH, c = t % S_t::CH, j = j0 + S_t::OH + c;
+            const int nc = (rs.hi - rs.lo) * S_t::CH;
+            for (int t = threadIdx.x; t < 2 * nc; t += NT) {
+                const bool yd = t >= nc;
+                const int q = yd ? t - nc : t;
+                const int i = rs.lo + q / S_t::CH, c = q % S_t::CH, j = j0 + S_t::OH + c;
                 if (j < ch_lo || j >= ch_hi) continue;
                 const int cw = c + S_t::OH - S_t::OW;
                 auto W = [&](int ii, int cc) {
@@ -202,42 +204,47 @@ __global__ void __launch_bounds__(NT) k_mhd2d_fused_mixed(Geo G, Geo FG, const d
                 const double bx0 = B[gF(i, j)], bx1 = B[gF(i + 1, j)];
                 const double by0 = B[FP + gF(i, j)], by1 = B[FP + gF(i, j + 1)];
                 const float dBx = (float)((bx1 - bx0) * dt_dx), dBy = (float)((by1 - by0) * dt_dy);
-                const Prim<float> wc = W(i, cw);
+                Prim<float> l = yd ? W(i, cw - 1) : W(i - 1, cw), wc = W(i, cw), r = yd ? W(i, cw + 1) : W(i + 1, cw);
+                if (yd) { swap_xy(l); swap_xy(wc); swap_xy(r); }
                 Prim<float> L, Rr;
-                fo += !muscl_mixed<true>(sa.limiter, W(i - 1, cw), L, wc, Rr, W(i + 1, cw), fdx, dBx, dBy, 0.f);
-                L.Bx = (float)bx0;
-                Rr.Bx = (float)bx1;
-                fm_put_hs(S, i, 0, c, L);
-                fm_put_hs(S, i, 1, c, Rr);
-                Prim<float> yl = W(i, cw - 1), yc = wc, yr = W(i, cw + 1);
-                swap_xy(yl); swap_xy(yc); swap_xy(yr);
-                fo += !muscl_mixed<true>(sa.limiter, yl, L, yc, Rr, yr, fdy, dBy, dBx, 0.f);
-                swap_xy(L); swap_xy(Rr);
-                L.By = (float)by0;
-                Rr.By = (float)by1;
-                fm_put_hs(S, i, 2, c, L);
-                fm_put_hs(S, i, 3, c, Rr);
+                // y: the swapped source terms, dB.y from the x faces and dB.x from the y faces
+                fo += !muscl_mixed<true>(sa.limiter, l, L, wc, Rr, r, yd ? fdy : fdx, yd ? dBy : dBx, yd ? dBx : dBy, 0.f);
+                if (yd) {
+                    swap_xy(L); swap_xy(Rr);
+                    L.By = (float)by0;
+                    Rr.By = (float)by1;
+                } else {
+                    L.Bx = (float)bx0;
+                    Rr.Bx = (float)bx1;
+                }
+                fm_put_hs(S, i, yd ? 2 : 0, c, L);
+                fm_put_hs(S, i, yd ? 3 : 1, c, Rr);
             }
         }
         __syncthreads();
-        // ---- S2: predictor fluxes, x faces (rows from sb-1) then y faces (rows from sb-2)
+        // ---- S2: predictor fluxes, x faces (rows from sb-1) then y faces (rows
+        // from sb-2), one Riemann code path: y faces solve on swapped states
         {
             const RowSpan rx = span_of<R>(a, se, 2, sb - 1), ry = span_of<R>(a, se, 2, sb - 2);
             const int nxf = (rx.hi - rx.lo) * S_t::CH, nyf = (ry.hi - ry.lo) * S_t::CY;
             for (int t = threadIdx.x; t < nxf + nyf; t += NT) {
+                const bool yd = t >= nxf;
+                const int q = yd ? t - nxf : t;
+                const int C = yd ? S_t::CY : S_t::CH;
+                const int i = (yd ? ry.lo : rx.lo) + q / C, c = q % C;
+                const int j = j0 + (yd ? S_t::OY : S_t::OH) + c;
+                if (yd ? (j < cy_lo || j >= cy_hi) : (j < ch_lo || j >= ch_hi)) continue;
+                const int ch = j - j0 - S_t::OH;  // half-state column of cell j
+                Prim<float> L = yd ? fm_hs(S, i, 3, ch - 1) : fm_hs(S, i - 1, 1, ch);
+                Prim<float> Rr = yd ? fm_hs(S, i, 2, ch) : fm_hs(S, i, 0, ch);
+                if (yd) { swap_xy(L); swap_xy(Rr); }
                 Cons<float> Fl;
-                if (t < nxf) {
-                    const int i = rx.lo + t / S_t::CH, c = t % S_t::CH, j = j0 + S_t::OH + c;
-                    if (j < ch_lo || j >= ch_hi) continue;
-                    face_flux_mixed<true, SOLVER, 0>(fm_hs(S, i - 1, 1, c), fm_hs(S, i, 0, c), fdx, eo, Fl, &st);
-                    fm_put8(S.px[ring<S_t::K1>(i)], c, Fl);
-                } else {
-                    const int q = t - nxf;
-                    const int i = ry.lo + q / S_t::CY, c = q % S_t::CY, j = j0 + S_t::OY + c;
-                    if (j < cy_lo || j >= cy_hi) continue;
-                    const int ch = c + S_t::OY - S_t::OH;  // half-state column of cell j
-                    face_flux_mixed<true, SOLVER, 1>(fm_hs(S, i, 3, ch - 1), fm_hs(S, i, 2, ch), fdy, eo, Fl, &st);
+                face_flux_mixed<true, SOLVER, 0>(L, Rr, yd ? fdy : fdx, eo, Fl, &st);
+                if (yd) {
+                    swap_xy(Fl);
                     fm_put8(S.py[ring<S_t::K1>(i)], c, Fl);
+                } else {
+                    fm_put8(S.px[ring<S_t::K1>(i)], c, Fl);
                 }
             }
         }
@@ -260,12 +267,16 @@ __global__ void __launch_bounds__(NT) k_mhd2d_fused_mixed(Geo G, Geo FG, const d
             }
         }
         __syncthreads();
-        // ---- S4: half step and CTU corrections (mx_half of step_mhd_mixed.cuh)
+        // ---- S4: half step and CTU corrections (mx_half of step_mhd_mixed.cuh),
+        // three items per cell: the x half states' correction, the y half
+        // states' correction (one code path on selected operands), the
+        // half-step cell's body E
         {
             const RowSpan rs = span_of<R>(a, se, 1, sb - 1);
-            const int n = (rs.hi - rs.lo) * S_t::CC;
-            for (int t = threadIdx.x; t < n; t += NT) {
-                const int i = rs.lo + t / S_t::CC, c = t % S_t::CC, j = j0 + S_t::OC + c;
+            const int nc = (rs.hi - rs.lo) * S_t::CC;
+            for (int t = threadIdx.x; t < 3 * nc; t += NT) {
+                const int kind = t / nc, q = t - kind * nc;
+                const int i = rs.lo + q / S_t::CC, c = q % S_t::CC, j = j0 + S_t::OC + c;
                 if (j < cc_lo || j >= cc_hi) continue;
                 const int cy = j - j0 - S_t::OY, ch = j - j0 - S_t::OH;
                 auto E0 = [&](int ii, int cc) { return fm_get3(S.e0[ring<S_t::K1>(ii)], cc); };
@@ -276,11 +287,12 @@ __global__ void __launch_bounds__(NT) k_mhd2d_fused_mixed(Geo G, Geo FG, const d
                 const double bxh1 = bx1 - (e11.z - e10.z) * hdy;
                 const double byh0 = by0 - -(e10.z - e00.z) * hdx;
                 const double byh1 = by1 - -(e11.z - e01.z) * hdx;
-                const double bzh = B[2 * FP + m] - ((e10.y - e00.y) * hdx - (e01.x - e00.x) * hdy);
-                const Prim<double> W = load_prim<true>(w, P, gidx2(G, i, j));
-                const Cons<double> px0 = fm_get8(S.px[ring<S_t::K1>(i)], ch), px1 = fm_get8(S.px[ring<S_t::K1>(i + 1)], ch);
-                const Cons<double> py0 = fm_get8(S.py[ring<S_t::K1>(i)], cy), py1 = fm_get8(S.py[ring<S_t::K1>(i)], cy + 1);
-                {
+                const long long mc = gidx2(G, i, j);
+                if (kind == 2) {
+                    const double bzh = B[2 * FP + m] - ((e10.y - e00.y) * hdx - (e01.x - e00.x) * hdy);
+                    const Prim<double> W = load_prim<true>(w, P, mc);
+                    const Cons<double> px0 = fm_get8(S.px[ring<S_t::K1>(i)], ch), px1 = fm_get8(S.px[ring<S_t::K1>(i + 1)], ch);
+                    const Cons<double> py0 = fm_get8(S.py[ring<S_t::K1>(i)], cy), py1 = fm_get8(S.py[ring<S_t::K1>(i)], cy + 1);
                     Cons<double> U = to_cons64<true>(W);
                     U = c_add<true>(U, c_mul<true>(c_sub<true>(px0, px1), hdx));
                     U = c_add<true>(U, c_mul<true>(c_sub<true>(py0, py1), hdy));
@@ -288,55 +300,54 @@ __global__ void __launch_bounds__(NT) k_mhd2d_fused_mixed(Geo G, Geo FG, const d
                     Prim<double> wh = to_prim64<true>(U);
                     wh = body_field64(wh, (bxh0 + bxh1) * 0.5, (byh0 + byh1) * 0.5, bzh, sa.ct_energy);
                     fm_put3(S.eh[ring<S_t::K1>(i)], c, body_e(wh));
+                    continue;
                 }
+                const bool yd = kind == 1;
+                const double Wvz = w[4 * P + mc], WBz = w[7 * P + mc];
                 const double dBx = (bx1 - bx0) * dt_dx, dBy = (by1 - by0) * dt_dy;
-                auto correct = [&](int k, const Cons<double>& corr, int comp, double bl, double br) {
-                    const Prim<float> hl = fm_hs(S, i, k, ch), hr = fm_hs(S, i, k + 1, ch);
-                    const Cons<float> cf = cvt<float>(corr);
-                    Cons<float> ul = c_add<true>(to_cons<true>(hl), cf), ur = c_add<true>(to_cons<true>(hr), cf);
-                    if (comp == 0) { ul.Bx = (float)bl; ur.Bx = (float)br; }
-                    else { ul.By = (float)bl; ur.By = (float)br; }
-                    fm_put_hs(S, i, k, ch, prim_from<true>(ul, energy64<true>(hl) + corr.E));
-                    fm_put_hs(S, i, k + 1, ch, prim_from<true>(ur, energy64<true>(hr) + corr.E));
-                };
-                {
-                    Cons<double> corr = c_mul<true>(c_mul<true>(c_sub<true>(py0, py1), 0.5), dt_dy);
-                    corr.Bx = corr.By = corr.Bz = 0;
-                    const double lim_z = lim_minmod(-dBy, dBx);
-                    corr.E += k1_8pi * (W.Bz * W.vz * lim_z);
-                    corr.Bz = 0.5 * dt_dy * (e01.x - e00.x) + 0.5 * W.vz * lim_z;
-                    correct(0, corr, 0, bxh0, bxh1);
-                }
-                {
-                    Cons<double> corr = c_mul<true>(c_mul<true>(c_sub<true>(px0, px1), 0.5), dt_dx);
-                    corr.Bx = corr.By = corr.Bz = 0;
-                    const double lim_z = lim_minmod(-dBx, dBy);
-                    corr.E += k1_8pi * (W.Bz * W.vz * lim_z);
-                    corr.Bz = -0.5 * dt_dx * (e10.y - e00.y) + 0.5 * W.vz * lim_z;
-                    correct(2, corr, 1, byh0, byh1);
-                }
+                // x half states: the y fluxes' difference; y half states: the x fluxes'
+                const Cons<double> p0 = yd ? fm_get8(S.px[ring<S_t::K1>(i)], ch) : fm_get8(S.py[ring<S_t::K1>(i)], cy);
+                const Cons<double> p1 = yd ? fm_get8(S.px[ring<S_t::K1>(i + 1)], ch) : fm_get8(S.py[ring<S_t::K1>(i)], cy + 1);
+                Cons<double> corr = c_mul<true>(c_mul<true>(c_sub<true>(p0, p1), 0.5), yd ? dt_dx : dt_dy);
+                corr.Bx = corr.By = corr.Bz = 0;
+                const double lim_z = yd ? lim_minmod(-dBx, dBy) : lim_minmod(-dBy, dBx);
+                corr.E += k1_8pi * (WBz * Wvz * lim_z);
+                corr.Bz = yd ? -0.5 * dt_dx * (e10.y - e00.y) + 0.5 * Wvz * lim_z
+                             : 0.5 * dt_dy * (e01.x - e00.x) + 0.5 * Wvz * lim_z;
+                const int k = yd ? 2 : 0;
+                const Prim<float> hl = fm_hs(S, i, k, ch), hr = fm_hs(S, i, k + 1, ch);
+                const Cons<float> cf = cvt<float>(corr);
+                Cons<float> ul = c_add<true>(to_cons<true>(hl), cf), ur = c_add<true>(to_cons<true>(hr), cf);
+                if (yd) { ul.By = (float)byh0; ur.By = (float)byh1; }
+                else { ul.Bx = (float)bxh0; ur.Bx = (float)bxh1; }
+                fm_put_hs(S, i, k, ch, prim_from<true>(ul, energy64<true>(hl) + corr.E));
+                fm_put_hs(S, i, k + 1, ch, prim_from<true>(ur, energy64<true>(hr) + corr.E));
             }
         }
         __syncthreads();
-        // ---- S5: final fluxes, x faces (rows from sb) then y faces (rows from sb-1)
+        // ---- S5: final fluxes, x faces (rows from sb) then y faces (rows from
+        // sb-1), one Riemann code path as in S2
         {
             const RowSpan rx = span_of<R>(a, se, 1, sb), ry = span_of<R>(a, se, 1, sb - 1);
             const int nxf = (rx.hi - rx.lo) * S_t::CC, nyf = (ry.hi - ry.lo) * S_t::CF;
             for (int t = threadIdx.x; t < nxf + nyf; t += NT) {
+                const bool yd = t >= nxf;
+                const int q = yd ? t - nxf : t;
+                const int C = yd ? S_t::CF : S_t::CC;
+                const int i = (yd ? ry.lo : rx.lo) + q / C, c = q % C;
+                const int j = j0 + (yd ? S_t::OF : S_t::OC) + c;
+                if (yd ? (j < cf_lo || j >= cf_hi) : (j < cc_lo || j >= cc_hi)) continue;
+                const int ch = j - j0 - S_t::OH;
+                Prim<float> L = yd ? fm_hs(S, i, 3, ch - 1) : fm_hs(S, i - 1, 1, ch);
+                Prim<float> Rr = yd ? fm_hs(S, i, 2, ch) : fm_hs(S, i, 0, ch);
+                if (yd) { swap_xy(L); swap_xy(Rr); }
                 Cons<float> Fl;
-                if (t < nxf) {
-                    const int i = rx.lo + t / S_t::CC, c = t % S_t::CC, j = j0 + S_t::OC + c;
-                    if (j < cc_lo || j >= cc_hi) continue;
-                    const int ch = j - j0 - S_t::OH;
-                    face_flux_mixed<true, SOLVER, 0>(fm_hs(S, i - 1, 1, ch), fm_hs(S, i, 0, ch), fdx, eo, Fl, &st);
-                    fm_put8(S.fx[ring<S_t::K1>(i)], c, Fl);
-                } else {
-                    const int q = t - nxf;
-                    const int i = ry.lo + q / S_t::CF, c = q % S_t::CF, j = j0 + S_t::OF + c;
-                    if (j < cf_lo || j >= cf_hi) continue;
-                    const int ch = j - j0 - S_t::OH;
-                    face_flux_mixed<true, SOLVER, 1>(fm_hs(S, i, 3, ch - 1), fm_hs(S, i, 2, ch), fdy, eo, Fl, &st);
+                face_flux_mixed<true, SOLVER, 0>(L, Rr, yd ? fdy : fdx, eo, Fl, &st);
+                if (yd) {
+                    swap_xy(Fl);
                     fm_put8(S.fy[ring<S_t::K1>(i)], c, Fl);
+                } else {
+                    fm_put8(S.fx[ring<S_t::K1>(i)], c, Fl);
                 }
             }
         }

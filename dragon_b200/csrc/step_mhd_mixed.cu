@@ -12,7 +12,7 @@ namespace dgpu {
 namespace {
 
 // Strips of kFuseTJ columns marching kFuseR rows per iteration, kFuseNT threads.
-constexpr int kFuseTJ = 32, kFuseR = 4, kFuseNT = 128;
+constexpr int kFuseTJ = 32, kFuseR = 8, kFuseNT = 256;
 
 // One fused launch: a strip of columns per blockIdx.x, a segment of rows per
 // blockIdx.y. Segments are sized so the CTAs fill the device's resident
