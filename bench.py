@@ -390,8 +390,10 @@ def learned_guess_report(n=256, p_in=10.0, steps=10):
     lifted so every solve reaches the tolerance, plus the reference's own
     setting (mean guess, cap 6). The "perfect" arms start Newton from the
     converged star pressure of an uncounted first solve, exactly or with a
-    relative error of 1e-9, 1e-6 or 1e-3: the iterations any guess of that
-    accuracy needs, i.e. the ceiling of the reduction a guess can give."""
+    relative error of 1e-9, 1e-6 or 1e-3, or from the mean guess on faces
+    where that needs no more iterations: the fewest iterations any guess of
+    that accuracy with a fallback to the mean can reach, i.e. the ceiling of
+    the reduction such a guess can give."""
     import torch
 
     import dragon_b200 as dg

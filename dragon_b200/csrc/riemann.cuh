@@ -33,8 +33,10 @@ struct FaceStats {
 // value, with the analytic guess as fallback when that value is unusable and
 // as judge when the iteration from it hits the cap. GUESS_PERFECT is a
 // measurement arm, not a solver option: the start is the converged star
-// pressure of a first solve that is not counted, times (1 +- guess_err), so
-// its iteration count is the floor a guess of that accuracy can reach.
+// pressure of a first solve that is not counted, times (1 +- guess_err), or
+// the reference's mean where that takes no more iterations, so its
+// iteration count is the floor any guess of that accuracy with a fallback to
+// the mean can reach.
 enum GuessMode : int { GUESS_MEAN = 0, GUESS_ANALYTIC = 1, GUESS_LEARNED = 2, GUESS_PERFECT = 3 };
 
 // Converged Newton solves recorded as training samples for the learned guess:
@@ -255,7 +257,8 @@ constexpr int kPerfectGuessCap = 200;  // iterations of GUESS_PERFECT's uncounte
 // 0.8 p, stop on relative change <= tol or after max_iters iterations.
 // *converged tells whether the tolerance (not the cap) ended the iteration.
 template <class R>
-DHD R exact_star_p(const Prim<R>& L, const Prim<R>& Rt, R pGuess, ExactOpts o, FaceStats* st, bool* converged) {
+DHD R exact_star_p(const Prim<R>& L, const Prim<R>& Rt, R pGuess, ExactOpts o, FaceStats* st, bool* converged,
+                   int* iterations = nullptr) {
     R pStar = pGuess, CHA = R(1);
     int iters = o.max_iters;
     int n = 0;
@@ -277,6 +280,7 @@ DHD R exact_star_p(const Prim<R>& L, const Prim<R>& Rt, R pGuess, ExactOpts o, F
         newton_log_push(o.log, L.rho, L.vx, L.p, Rt.rho, Rt.vx, Rt.p, pStar, n);
 #endif
     *converged = conv;
+    if (iterations) *iterations = n;
     return pStar;
 }
 
@@ -356,14 +360,23 @@ DHD ExactSolution<R> exact_solve(const Prim<R>& L, const Prim<R>& Rt, ExactOpts 
     if (o.guess == GUESS_MEAN) {
         pGuess = (L.p + Rt.p) / R(2);
     } else if (o.guess == GUESS_PERFECT) {
+        // uncounted dry runs: the converged star pressure, the iterations from
+        // it with the given relative error and from the mean guess; the counted
+        // solve starts from whichever needs fewer (a gate that knows the answer)
         ExactOpts q = o;
         q.max_iters = kPerfectGuessCap;
         q.log.rows = nullptr;
-        bool c0;
+        bool c0, c1, c2;
+        int n_mean = 0, n_err = 0;
         const R mean = (L.p + Rt.p) / R(2);
         const R p0 = exact_star_p(L, Rt, mean, q, nullptr, &c0);
         const R e = R(o.guess_err);
-        pGuess = (c0 && p0 > R(0) && sfinite(p0)) ? p0 * (R(1) + (L.p >= Rt.p ? e : -e)) : mean;
+        const R pe = (c0 && p0 > R(0) && sfinite(p0)) ? p0 * (R(1) + (L.p >= Rt.p ? e : -e)) : mean;
+        ExactOpts d = o;
+        d.log.rows = nullptr;
+        exact_star_p(L, Rt, mean, d, nullptr, &c1, &n_mean);
+        exact_star_p(L, Rt, pe, d, nullptr, &c2, &n_err);
+        pGuess = (c2 && (!c1 || n_err < n_mean)) ? pe : mean;
     } else if (o.guess != GUESS_LEARNED || !learned) {
         pGuess = analytic_guess(L, Rt);
     } else if (learned->guess > R(0) && sfinite(learned->guess)) {

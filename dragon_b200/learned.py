@@ -172,10 +172,10 @@ def c4_training_set(net: Network, runs: int = 6, seed: int = 2024) -> dict:
     """The training recipe of the 3D blast configuration: seeded 128^3 blasts
     (MC, outflow, exact solver with the reference's mean guess and cap) with the
     inner pressure log-uniform in [10, 1e4], 16 steps each, every second
-    converged solve logged (~1e7 samples over six runs; no run fills its
-    log)."""
+    converged solve logged (~1e7 samples over six runs; the log holds 2^23
+    rows per run, more than the ~8e6 the strongest blasts log)."""
     return collect_blast_samples(net, runs=runs, n=128, steps=16, seed=seed, p_range=(10.0, 1e4), stride=2,
-                                 capacity=1 << 22)
+                                 capacity=1 << 23)
 
 
 def fit(net: Network, steps: int = 6000, batch: int = 8192, lr: float = 3e-3, gate_factor: float = 1.0) -> dict:

@@ -195,8 +195,9 @@ def test_learned_needs_a_network_and_a_3d_grid():
 @pytest.mark.parametrize("err_exp,max_iters_per_solve", [(0, 1.0), (6, 2.0)])
 def test_perfect_guess_arm_is_the_iteration_floor(err_exp, max_iters_per_solve):
     """The measurement arm GUESS_PERFECT starts Newton from the converged star
-    pressure of an uncounted first solve: every counted solve then converges
-    in one iteration (two when the start carries a 1e-6 relative error), and
+    pressure of an uncounted first solve (or from the mean guess where that
+    needs no more iterations): every counted solve then converges in one
+    iteration (at most two when the start carries a 1e-6 relative error), and
     the states equal the reference mean-guess solve's to 1e-12."""
     n, steps = 32, 4
     out = {}
