@@ -71,6 +71,33 @@ __device__ __forceinline__ Prim<double> to_prim64(const Cons<double>& u) {
     return w;
 }
 
+// CFL signal speed of a committed cell (CFL.cpp:28-84: max or sum over the
+// axes of (|v| + a) / dL) evaluated in FP32 for the forms CFL_MAX and CFL_ADD:
+// the mixed path's time step is its own, and the FP32 speed is within ~1e-7
+// of the FP64 one; the p-norm form keeps the FP64 function.
+template <bool MHD>
+__device__ __forceinline__ double cfl_speed_mx(const Prim<double>& W64, int cfl, double dx, double dy, double dz) {
+    if (cfl != 0 && cfl != 1) return cfl_speed<MHD>(W64, cfl, dx, dy, dz);
+    const Prim<float> W = cvt<float>(W64);
+    float a;
+    if constexpr (MHD) a = fast_speed_max(W);
+    else a = sound_speed(W);
+    float speed = 0.f;
+    if (dx > 1e-14) speed = (fabsf(W.vx) + a) / (float)dx;
+    if (dy > 1e-14) speed = cfl ? speed + (fabsf(W.vy) + a) / (float)dy : smax(speed, (fabsf(W.vy) + a) / (float)dy);
+    if (dz > 1e-14) speed = cfl ? speed + (fabsf(W.vz) + a) / (float)dz : smax(speed, (fabsf(W.vz) + a) / (float)dz);
+    return speed;
+}
+// The 1D grids' speed |v.x| + a (CFL.cpp:88-105) in FP32.
+template <bool MHD>
+__device__ __forceinline__ double cfl_speed_1d_mx(const Prim<double>& W64) {
+    const Prim<float> W = cvt<float>(W64);
+    float a;
+    if constexpr (MHD) a = fast_speed_max(W);
+    else a = sound_speed(W);
+    return fabsf(W.vx) + a;
+}
+
 // Primitive state from FP32 momenta / density and an FP64 total energy,
 // pressure recovered in FP64.
 template <bool MHD>

@@ -136,7 +136,7 @@ __device__ __forceinline__ void step1d_tile_mx(const Geo& G, const double* __res
         const int c = p - G.g;
         if (c >= 0 && c < G.n[0]) {
             if (!is_physical<false>(nw)) record_error(ctl, ST_UNPHYSICAL, p);
-            vmax = speed_max(vmax, cfl_speed_1d<false>(nw));
+            vmax = speed_max(vmax, cfl_speed_1d_mx<false>(nw));
         }
         store_prim<false>(wout, PL, p, nw);
     }

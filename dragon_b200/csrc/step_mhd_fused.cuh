@@ -400,7 +400,7 @@ __global__ void __launch_bounds__(NT, 2) k_mhd2d_fused_mixed(Geo G, Geo FG, cons
                 Bout[2 * FP + mf] = bz;
                 if (i == nx - 1) Bout[gF(nx, j)] = bx1;
                 if (j == ny - 1) Bout[FP + gF(i, ny)] = by1;
-                vmax = speed_max(vmax, cfl_speed<true>(nw, sa.cfl, sa.dx, sa.dy, 0.0));
+                vmax = speed_max(vmax, cfl_speed_mx<true>(nw, sa.cfl, sa.dx, sa.dy, 0.0));
             }
         }
         __syncthreads();

@@ -37,9 +37,20 @@ struct Mhd2DMixedArgs {
     StepArgs sa;
 };
 
+// shouldProtectThermal (B_fields.cpp:91-114) without the division: for
+// B^2 > 0, 8 pi p / B^2 <= 0.1 is 8 pi p <= 0.1 B^2 (rounding differs only at
+// the threshold, which the mixed path is not held to).
+__device__ __forceinline__ bool protect_thermal_mx(const Prim<double>& w, int mode) {
+    if (mode == 0) return false;
+    if (mode == 1) return true;
+    const double B2 = dot3(w.Bx, w.By, w.Bz, w.Bx, w.By, w.Bz);
+    if (B2 == 0) return false;
+    return k8pi * w.p <= 0.1 * B2;
+}
+
 // computeBodyField (B_fields.cpp:70-79) with the mixed path's FP64 conversions.
 __device__ __forceinline__ Prim<double> body_field64(Prim<double> w, double bx, double by, double bz, int mode) {
-    if (!protect_thermal(w, mode)) {
+    if (!protect_thermal_mx(w, mode)) {
         Cons<double> U = to_cons64<true>(w);
         U.Bx = bx; U.By = by; U.Bz = bz;
         return to_prim64<true>(U);
@@ -271,7 +282,7 @@ __device__ __forceinline__ void mx_update(const Mhd2DMixedArgs& A, const Tile2& 
         A.Bout[2 * FP + mf] = bz;
         if (i == nx - 1) A.Bout[gidx2(F, nx, j)] = bx1;
         if (j == ny - 1) A.Bout[FP + gidx2(F, i, ny)] = by1;
-        vmax = cfl_speed<true>(nw, A.sa.cfl, A.sa.dx, A.sa.dy, 0.0);
+        vmax = cfl_speed_mx<true>(nw, A.sa.cfl, A.sa.dx, A.sa.dy, 0.0);
     }
     for (int o = 16; o > 0; o >>= 1) vmax = speed_max(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
     const int tid = threadIdx.y * blockDim.x + threadIdx.x, nthr = blockDim.x * blockDim.y;

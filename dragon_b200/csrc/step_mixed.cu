@@ -252,7 +252,7 @@ k_step2d_hydro_mixed(Geo G, const double* __restrict__ win, double* __restrict__
         if (!is_finite<false>(U)) record_error(ctl, ST_NAN, (long long)(i + g) * (ny + 2 * g) + (j + g));
         else if (!is_physical<false>(nw)) record_error(ctl, ST_UNPHYSICAL, (long long)(i + g) * (ny + 2 * g) + (j + g));
         store_prim<false>(wout, PL, m, nw);
-        vmax = speed_max(vmax, cfl_speed<false>(nw, sa.cfl, sa.dx, sa.dy, 0.0));
+        vmax = speed_max(vmax, cfl_speed_mx<false>(nw, sa.cfl, sa.dx, sa.dy, 0.0));
     }
     copy_ghosts_2d<5>(G, win, wout, i0, j0, TI, TJ);
 
