@@ -434,20 +434,19 @@ __global__ void __launch_bounds__(256) k_prologue_coop(Geo G, Geo FG, double* __
     if (s_skip) return;
     const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long nt = (long long)gridDim.x * blockDim.x;
+    // An entry fills its cells axis by axis, then its faces axis by axis. Cell
+    // passes read and write only cells, face passes only faces, so the cell
+    // and face passes of one axis share a stage: each array still sees its
+    // passes in the reference's order, with one barrier per axis.
     if (pa.apply_bc) {
         for (int e = pa.bc_first; e < pa.bc_first + pa.nbc; e++) {
             const BCEntry be = bcs[e];
             for (int a = 0; a < G.dim; a++) {
                 bc_cells_axis<MHD>(G, w, be, a, tid, nt);
-                if (!grid_barrier(ctl)) return;
-            }
-            if constexpr (MHD) {
-                if (G.dim >= 2) {
-                    for (int a = 0; a < G.dim; a++) {
-                        bc_faces_axis(FG, G.n, B, be, a, tid, nt);
-                        if (!grid_barrier(ctl)) return;
-                    }
+                if constexpr (MHD) {
+                    if (G.dim >= 2) bc_faces_axis(FG, G.n, B, be, a, tid, nt);
                 }
+                if (!grid_barrier(ctl)) return;
             }
         }
     }

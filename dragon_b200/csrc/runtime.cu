@@ -273,7 +273,7 @@ int launch_step(dragon_grid* h, int c) {
                                    h->ctl, sa, h->stream);
         }
         // 2D: the ghost-frame copy, then seven phase kernels (FP64) or the fused kernel (mixed)
-        if (h->dim == 2) nk = 1 + (h->cfg.precision == 1 ? 1 : kMhd2DKernels);
+        if (h->dim == 2) nk = h->cfg.precision == 1 ? 1 : kMhd2DKernels;
     } else if (h->dim == 2) {
         const int mixed = h->cfg.precision == 1 ? 1 : 0;
         const CUtensorMap* map = nullptr;

@@ -37,7 +37,7 @@ struct Hydro3DScratch {
     long long plane;
     static constexpr int kPlanes = 30 + 15 + 30;
 };
-constexpr int kHydro3DKernels = 6;
+constexpr int kHydro3DKernels = 5;
 
 // 3D MHD step, on the face geometry.
 struct Mhd3DScratch {

@@ -1,14 +1,14 @@
 // 3D unsplit CTU hydro step (Grid3D::unsplit_step hydro branch,
-// Unsplit.cpp:115-206; the 12-solve ctu_sweep_hydro, CTU.cpp:222-370) as six
-// kernels over global intermediates:
+// Unsplit.cpp:115-206; the 12-solve ctu_sweep_hydro, CTU.cpp:222-370) as
+// five kernels over global intermediates:
 //   K1 half states along x, y, z for cells [-1, n]^3
 //   K2 predictor fluxes (CTU.cpp:229-232)
 //   K3 the six corner-corrected fluxes F_Xz, F_Yz, F_Xy, F_Zy, F_Yx, F_Zx
 //      (computeCTUFlux_X/Y/Z, CTU.cpp:306-370; dt/3 transverse weights)
-//   K4 the two sequential transverse corrections of every half state
-//      (correctState, CTU.cpp:246-260,280-301)
-//   K5 final fluxes (Unsplit.cpp:102-105)
-//   K6 conservative update, physicality, CFL speed
+//   K4 final fluxes (Unsplit.cpp:102-105) from the half states with their two
+//      sequential transverse corrections (correctState, CTU.cpp:246-260,
+//      280-301) applied where the face reads them, not written back
+//   K5 conservative update, physicality, CFL speed
 // Index ranges are the reference's, so every Riemann pivot that can fail does.
 #pragma once
 
@@ -45,10 +45,24 @@ __device__ __forceinline__ bool box_cell(long long t, const int* lo, const int* 
     return true;
 }
 
-__device__ __forceinline__ Prim<double> ld5(const double* a, long long P, long long m) { return load_prim<false>(a, P, m); }
+// Every array a kernel of this step reads is one it does not write (state ->
+// half states -> predictor fluxes -> corner fluxes -> final fluxes -> new
+// state), so the loads go through the read-only path: the compiler may then
+// issue a later face's loads before an earlier face's stores.
+__device__ __forceinline__ Prim<double> ld5(const double* a, long long P, long long m) {
+    Prim<double> r;
+    r.rho = __ldg(a + m);
+    r.p = __ldg(a + P + m);
+    r.vx = __ldg(a + 2 * P + m);
+    r.vy = __ldg(a + 3 * P + m);
+    r.vz = __ldg(a + 4 * P + m);
+    r.Bx = r.By = r.Bz = 0;
+    return r;
+}
 __device__ __forceinline__ void st5(double* a, long long P, long long m, const Prim<double>& w) { store_prim<false>(a, P, m, w); }
 __device__ __forceinline__ Cons<double> ldc5(const double* a, long long P, long long m) {
-    return Cons<double>{a[m], a[P + m], a[2 * P + m], a[3 * P + m], a[4 * P + m], 0, 0, 0};
+    return Cons<double>{__ldg(a + m), __ldg(a + P + m), __ldg(a + 2 * P + m), __ldg(a + 3 * P + m), __ldg(a + 4 * P + m),
+                        0, 0, 0};
 }
 __device__ __forceinline__ void stc5(double* a, long long P, long long m, const Cons<double>& u) {
     a[m] = u.rho; a[P + m] = u.E; a[2 * P + m] = u.mx; a[3 * P + m] = u.my; a[4 * P + m] = u.mz;
@@ -97,6 +111,65 @@ __device__ __forceinline__ void h3_flux(const Step3DArgs& A, double* out, int i,
     const ExactOpts eo = exact_opts(A.sa);
     if (!face_flux<false, SOLVER, AX>(L, R, dtn, eo, F, st)) record_error(A.ctl, stage, m);
     stc5(out, SP, m, F);
+}
+
+// Weights of the two transverse corrections of the half states along AX, in
+// the reference's order (CTU.cpp:246-260): x states by F_Yz (dt/2dy) then
+// F_Zy (dt/2dz); y states by F_Xz then F_Zx; z states by F_Xy then F_Yx.
+struct H3Half {
+    double hx, hy, hz;
+};
+
+// One transverse correction of a half state at cell m: U - (F(m + e_D) - F(m)) * w.
+template <int D>
+__device__ __forceinline__ Prim<double> h3_corrected_once(const Step3DArgs& A, const Prim<double>& s, const double* F,
+                                                          double w, int i, int j, int k) {
+    const Geo& G = A.G;
+    const long long SP = A.S.plane;
+    const Cons<double> tr = c_mul<false>(
+        c_sub<false>(ldc5(F, SP, gidx3(G, i + (D == 0), j + (D == 1), k + (D == 2))), ldc5(F, SP, gidx3(G, i, j, k))), w);
+    return to_prim<false>(c_sub<false>(to_cons<false>(s), tr));
+}
+
+// The corrected half state of cell (i,j,k) along AX (SIDE 0: the state at the
+// cell's low face, 1: at its high face), computed where the final flux needs
+// it instead of written back by a separate pass: the same two sequential
+// corrections with the same operands, so the value is bit-identical.
+template <int AX, int SIDE>
+__device__ __forceinline__ Prim<double> h3_corrected(const Step3DArgs& A, const H3Half& h, int i, int j, int k) {
+    const long long SP = A.S.plane;
+    const double* cf = A.S.cf;
+    Prim<double> s = ld5(A.S.hs + (10 * AX + 5 * SIDE) * SP, SP, gidx3(A.G, i, j, k));
+    if constexpr (AX == 0) {
+        s = h3_corrected_once<1>(A, s, cf + 5 * SP, h.hy, i, j, k);    // F_Yz
+        s = h3_corrected_once<2>(A, s, cf + 15 * SP, h.hz, i, j, k);   // F_Zy
+    } else if constexpr (AX == 1) {
+        s = h3_corrected_once<0>(A, s, cf, h.hx, i, j, k);             // F_Xz
+        s = h3_corrected_once<2>(A, s, cf + 25 * SP, h.hz, i, j, k);   // F_Zx
+    } else {
+        s = h3_corrected_once<0>(A, s, cf + 10 * SP, h.hx, i, j, k);   // F_Xy
+        s = h3_corrected_once<1>(A, s, cf + 20 * SP, h.hy, i, j, k);   // F_Yx
+    }
+    return s;
+}
+
+// Final flux through the AX face of cell (i,j,k) from the corrected states of
+// the cells on either side.
+template <int SOLVER, int AX>
+__device__ __forceinline__ void h3_final_flux(const Step3DArgs& A, const H3Half& h, int i, int j, int k, double dtn,
+                                              FaceStats* st) {
+    const long long SP = A.S.plane;
+    const int di = AX == 0, dj = AX == 1, dk = AX == 2;
+    const long long m = gidx3(A.G, i, j, k);
+    const Prim<double> L = h3_corrected<AX, 1>(A, h, i - di, j - dj, k - dk);
+    const Prim<double> R = h3_corrected<AX, 0>(A, h, i, j, k);
+    Cons<double> F;
+    if (!face_flux<false, SOLVER, AX>(L, R, dtn, exact_opts(A.sa), F, st)) record_error(A.ctl, ST_FINAL_FLUX, m);
+    stc5(A.S.pf + 5 * AX * SP, SP, m, F);
+}
+
+__device__ __forceinline__ H3Half h3_half(const Step3DArgs& A, double dt) {
+    return H3Half{0.5 * (dt / A.sa.dx), 0.5 * (dt / A.sa.dy), 0.5 * (dt / A.sa.dz)};
 }
 
 __device__ __forceinline__ void h3_stats(StepCtl* ctl, const FaceStats& st) {
@@ -219,6 +292,24 @@ static __global__ void k_h3_ctu_learned(Step3DArgs A) {
     h3_stats(A.ctl, st);
 }
 
+template <int AX>
+__device__ __forceinline__ void h3_final_flux_learned(const Step3DArgs& A, const H3Half& h, bool valid, int i, int j,
+                                                      int k, double dtn, FaceStats* st) {
+    const int di = AX == 0, dj = AX == 1, dk = AX == 2;
+    Prim<double> L = neutral_state(), R = neutral_state();
+    long long m = 0;
+    if (valid) {
+        m = gidx3(A.G, i, j, k);
+        L = h3_corrected<AX, 1>(A, h, i - di, j - dj, k - dk);
+        R = h3_corrected<AX, 0>(A, h, i, j, k);
+    }
+    const LearnedGuess<double> g = learned_guess_face<AX>(A, L, R, valid);
+    if (!valid) return;
+    Cons<double> F;
+    if (!face_flux<false, RS_EXACT, AX>(L, R, dtn, exact_opts(A.sa), F, st, &g)) record_error(A.ctl, ST_FINAL_FLUX, m);
+    stc5(A.S.pf + 5 * AX * A.S.plane, A.S.plane, m, F);
+}
+
 static __global__ void k_h3_final_learned(Step3DArgs A) {
     __shared__ int s;
     if (h3_skip(A.ctl, &s)) return;
@@ -228,11 +319,11 @@ static __global__ void k_h3_final_learned(Step3DArgs A) {
     const bool in = box_cell(blockIdx.x * (long long)blockDim.x + threadIdx.x, lo, ext, i, j, k);
     const int nx = G.n[0], ny = G.n[1], nz = G.n[2];
     const double dt = *(const volatile double*)&A.ctl->t1;
+    const H3Half h = h3_half(A, dt);
     FaceStats st{};
-    const long long SP = A.S.plane;
-    h3_flux_learned<0>(A, A.S.pf, in && j < ny && k < nz, i, j, k, dt / A.sa.dx, ST_FINAL_FLUX, &st);
-    h3_flux_learned<1>(A, A.S.pf + 5 * SP, in && i < nx && k < nz, i, j, k, dt / A.sa.dy, ST_FINAL_FLUX, &st);
-    h3_flux_learned<2>(A, A.S.pf + 10 * SP, in && i < nx && j < ny, i, j, k, dt / A.sa.dz, ST_FINAL_FLUX, &st);
+    h3_final_flux_learned<0>(A, h, in && j < ny && k < nz, i, j, k, dt / A.sa.dx, &st);
+    h3_final_flux_learned<1>(A, h, in && i < nx && k < nz, i, j, k, dt / A.sa.dy, &st);
+    h3_final_flux_learned<2>(A, h, in && i < nx && j < ny, i, j, k, dt / A.sa.dz, &st);
     h3_stats(A.ctl, st);
 }
 
@@ -315,49 +406,11 @@ __global__ void __launch_bounds__(256, 2) k_h3_ctu(Step3DArgs A) {
     h3_stats(A.ctl, st);
 }
 
-// in-place correction of one half-state pair by a flux difference along D
-__device__ __forceinline__ void h3_correct(const Step3DArgs& A, int state_ax, const double* F, int D, double w,
-                                           int i, int j, int k) {
-    const Geo& G = A.G;
-    const long long SP = A.S.plane, m = gidx3(G, i, j, k);
-    const Cons<double> tr = c_mul<false>(
-        c_sub<false>(ldc5(F, SP, gidx3(G, i + (D == 0), j + (D == 1), k + (D == 2))), ldc5(F, SP, m)), w);
-    double* L = A.S.hs + (10 * state_ax) * SP;
-    double* R = A.S.hs + (10 * state_ax + 5) * SP;
-    st5(L, SP, m, to_prim<false>(c_sub<false>(to_cons<false>(ld5(L, SP, m)), tr)));
-    st5(R, SP, m, to_prim<false>(c_sub<false>(to_cons<false>(ld5(R, SP, m)), tr)));
-}
-
-// K4: x states (cells [-1,nx]x[0,ny)x[0,nz)) by F_Yz then F_Zy; y states
-// ([0,nx)x[-1,ny]x[0,nz)) by F_Xz then F_Zx; z states ([0,nx)x[0,ny)x[-1,nz])
-// by F_Xy then F_Yx (CTU.cpp:246-260).
-static __global__ void k_h3_correct(Step3DArgs A) {
-    __shared__ int s;
-    if (h3_skip(A.ctl, &s)) return;
-    const Geo& G = A.G;
-    const int lo[3] = {-1, -1, -1}, ext[3] = {G.n[0] + 2, G.n[1] + 2, G.n[2] + 2};
-    int i, j, k;
-    if (!box_cell(blockIdx.x * (long long)blockDim.x + threadIdx.x, lo, ext, i, j, k)) return;
-    const int nx = G.n[0], ny = G.n[1], nz = G.n[2];
-    const double dt = *(const volatile double*)&A.ctl->t1;
-    const double hx = 0.5 * (dt / A.sa.dx), hy = 0.5 * (dt / A.sa.dy), hz = 0.5 * (dt / A.sa.dz);
-    const long long SP = A.S.plane;
-    const double* cf = A.S.cf;
-    if (j >= 0 && j < ny && k >= 0 && k < nz) {
-        h3_correct(A, 0, cf + 5 * SP, 1, hy, i, j, k);    // F_Yz
-        h3_correct(A, 0, cf + 15 * SP, 2, hz, i, j, k);   // F_Zy
-    }
-    if (i >= 0 && i < nx && k >= 0 && k < nz) {
-        h3_correct(A, 1, cf, 0, hx, i, j, k);             // F_Xz
-        h3_correct(A, 1, cf + 25 * SP, 2, hz, i, j, k);   // F_Zx
-    }
-    if (i >= 0 && i < nx && j >= 0 && j < ny) {
-        h3_correct(A, 2, cf + 10 * SP, 0, hx, i, j, k);   // F_Xy
-        h3_correct(A, 2, cf + 20 * SP, 1, hy, i, j, k);   // F_Yx
-    }
-}
-
-// K5: final fluxes on [0,n] along the normal axis, [0,n) on the others.
+// K4: final fluxes on [0,n] along the normal axis, [0,n) on the others, from
+// the half states corrected on the fly (correctState, CTU.cpp:246-260,280-301:
+// x states by F_Yz then F_Zy, y states by F_Xz then F_Zx, z states by F_Xy then
+// F_Yx). Every state a final face reads lies in the reference's corrected
+// range (x states: cells [-1,nx] x [0,ny) x [0,nz), and likewise).
 template <int SOLVER>
 __global__ void __launch_bounds__(256, 2) k_h3_final(Step3DArgs A) {
     __shared__ int s;
@@ -368,15 +421,15 @@ __global__ void __launch_bounds__(256, 2) k_h3_final(Step3DArgs A) {
     if (!box_cell(blockIdx.x * (long long)blockDim.x + threadIdx.x, lo, ext, i, j, k)) return;
     const int nx = G.n[0], ny = G.n[1], nz = G.n[2];
     const double dt = *(const volatile double*)&A.ctl->t1;
+    const H3Half h = h3_half(A, dt);
     FaceStats st{0, 0, 0, 0, 0};
-    const long long SP = A.S.plane;
-    if (j < ny && k < nz) h3_flux<SOLVER, 0>(A, A.S.pf, i, j, k, dt / A.sa.dx, ST_FINAL_FLUX, &st);
-    if (i < nx && k < nz) h3_flux<SOLVER, 1>(A, A.S.pf + 5 * SP, i, j, k, dt / A.sa.dy, ST_FINAL_FLUX, &st);
-    if (i < nx && j < ny) h3_flux<SOLVER, 2>(A, A.S.pf + 10 * SP, i, j, k, dt / A.sa.dz, ST_FINAL_FLUX, &st);
+    if (j < ny && k < nz) h3_final_flux<SOLVER, 0>(A, h, i, j, k, dt / A.sa.dx, &st);
+    if (i < nx && k < nz) h3_final_flux<SOLVER, 1>(A, h, i, j, k, dt / A.sa.dy, &st);
+    if (i < nx && j < ny) h3_final_flux<SOLVER, 2>(A, h, i, j, k, dt / A.sa.dz, &st);
     h3_stats(A.ctl, st);
 }
 
-// K6: conservative update of the interior (applyFluxes 3D, Unsplit.cpp:272-288),
+// K5: conservative update of the interior (applyFluxes 3D, Unsplit.cpp:272-288),
 // physicality, CFL speed of the committed state.
 static __global__ void k_h3_update(Step3DArgs A) {
     __shared__ int s;
@@ -422,7 +475,6 @@ inline int launch_step3d_hydro_t(const Geo& G, const double* w, double* wout, co
         if (learned) {
             k_h3_prelim_learned<<<blocks(box), 256, 0, st>>>(A);
             k_h3_ctu_learned<<<blocks(box), 256, 0, st>>>(A);
-            k_h3_correct<<<blocks(box), 256, 0, st>>>(A);
             k_h3_final_learned<<<blocks(fbox), 256, 0, st>>>(A);
             k_h3_update<<<blocks(cells), 256, 0, st>>>(A);
             return cudaGetLastError() == cudaSuccess ? 0 : 1;
@@ -430,7 +482,6 @@ inline int launch_step3d_hydro_t(const Geo& G, const double* w, double* wout, co
     }
     k_h3_prelim<SOLVER><<<blocks(box), 256, 0, st>>>(A);
     k_h3_ctu<SOLVER><<<blocks(box), 256, 0, st>>>(A);
-    k_h3_correct<<<blocks(box), 256, 0, st>>>(A);
     k_h3_final<SOLVER><<<blocks(fbox), 256, 0, st>>>(A);
     k_h3_update<<<blocks(cells), 256, 0, st>>>(A);
     return cudaGetLastError() == cudaSuccess ? 0 : 1;

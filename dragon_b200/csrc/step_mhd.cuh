@@ -455,23 +455,16 @@ __device__ __forceinline__ void mhd2d_copy_frame(const Geo& G, const Geo& FG, co
     }
 }
 
-static __global__ void k_mhd2d_copy_frame(Geo G, Geo FG, const double* __restrict__ w, double* __restrict__ wout,
-                                          const double* __restrict__ B, double* __restrict__ Bout) {
-    mhd2d_copy_frame(G, FG, w, wout, B, Bout, 0, mhd2d_frame_points(G.n[0], G.n[1], G.g),
-                     blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
-}
-
-// Enqueues the frame copy of a single-grid step.
-inline int launch_mhd2d_copy_frame(const Geo& G, const Geo& FG, const double* w, double* wout, const double* B,
-                                   double* Bout, cudaStream_t st) {
-    const long long n = mhd2d_frame_points(G.n[0], G.n[1], G.g);
-    const int blocks = (int)std::min<long long>((n + 255) / 256, 148 * 8);
-    k_mhd2d_copy_frame<<<blocks, 256, 0, st>>>(G, FG, w, wout, B, Bout);
-    return cudaGetLastError() == cudaSuccess ? 0 : 1;
-}
-
 // Kernels of the single-grid step: one 32 x 8 tile per CTA.
-static __global__ void k_mhd2d_halfstates(Mhd2DArgs A) { mhd2d_halfstates(A, launch_tile()); }
+// The first kernel also copies the ghost frame of the output buffers from
+// the inputs (grid-stride over the frame points; the step writes the rest).
+static __global__ void k_mhd2d_halfstates(Mhd2DArgs A) {
+    const long long nthr = (long long)gridDim.x * gridDim.y * blockDim.x * blockDim.y;
+    const long long tid = ((long long)blockIdx.y * gridDim.x + blockIdx.x) * (blockDim.x * blockDim.y) +
+                          threadIdx.y * blockDim.x + threadIdx.x;
+    mhd2d_copy_frame(A.G, A.FG, A.w, A.wout, A.B, A.Bout, 0, mhd2d_frame_points(A.G.n[0], A.G.n[1], A.G.g), tid, nthr);
+    mhd2d_halfstates(A, launch_tile());
+}
 // The flux kernels carry two CTAs per SM (<= 128 registers): at their natural
 // ~166 registers one 256-thread CTA fits, and the HLLD chains stall on latency.
 template <int SOLVER>
@@ -483,8 +476,8 @@ __global__ void __launch_bounds__(256, 2) k_mhd2d_final_flux(Mhd2DArgs A) { mhd2
 static __global__ void k_mhd2d_efinal(Mhd2DArgs A) { mhd2d_efinal(A, launch_tile()); }
 static __global__ void k_mhd2d_update(Mhd2DArgs A) { mhd2d_update(A, launch_tile()); }
 
-// 2D MHD CTU + CT step: the seven kernels in order, after the ghost frame of
-// the output buffers is copied from the inputs (mhd2d_copy_frame).
+// 2D MHD CTU + CT step: the seven kernels in order; the first also copies
+// the ghost frame of the output buffers from the inputs (mhd2d_copy_frame).
 template <int SOLVER>
 inline int launch_step2d_mhd_t(const Geo& G, const Geo& FG, const double* w, double* wout, const double* B, double* Bout,
                              const MhdScratch& S, StepCtl* ctl, const StepArgs& sa, cudaStream_t st) {
@@ -492,7 +485,6 @@ inline int launch_step2d_mhd_t(const Geo& G, const Geo& FG, const double* w, dou
     const dim3 blk(kTileJ, kTileI);
     auto grid_for = [&](int ni, int nj) { return dim3((nj + kTileJ - 1) / kTileJ, (ni + kTileI - 1) / kTileI); };
     const int nx = G.n[0], ny = G.n[1];
-    if (launch_mhd2d_copy_frame(G, FG, w, wout, B, Bout, st)) return 1;
     k_mhd2d_halfstates<<<grid_for(nx + 4, ny + 4), blk, 0, st>>>(A);
     k_mhd2d_prelim<SOLVER><<<grid_for(nx + 4, ny + 4), blk, 0, st>>>(A);
     k_mhd2d_e0<<<grid_for(nx + 3, ny + 3), blk, 0, st>>>(A);

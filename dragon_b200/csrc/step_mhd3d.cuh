@@ -45,6 +45,22 @@ __device__ __forceinline__ double* m3_flux_w(const Mhd3DArgs& A, int axis) {
     return axis == 0 ? A.S.fx : axis == 1 ? A.S.fy : A.S.fz;
 }
 
+// Read-only loads (ld.global.nc). Every array these are used on is one the
+// calling kernel does not write; the half states that k_m3_half corrects in
+// place keep plain loads there.
+__device__ __forceinline__ double m3_ld(const double* a, long long m) { return __ldg(a + m); }
+__device__ __forceinline__ Prim<double> m3_ld_prim(const double* a, long long P, long long m) {
+    return Prim<double>{__ldg(a + m),         __ldg(a + P + m),     __ldg(a + 2 * P + m), __ldg(a + 3 * P + m),
+                        __ldg(a + 4 * P + m), __ldg(a + 5 * P + m), __ldg(a + 6 * P + m), __ldg(a + 7 * P + m)};
+}
+__device__ __forceinline__ Cons<double> m3_ld_cons(const double* a, long long P, long long m) {
+    return Cons<double>{__ldg(a + m),         __ldg(a + P + m),     __ldg(a + 2 * P + m), __ldg(a + 3 * P + m),
+                        __ldg(a + 4 * P + m), __ldg(a + 5 * P + m), __ldg(a + 6 * P + m), __ldg(a + 7 * P + m)};
+}
+__device__ __forceinline__ V3 m3_ld_v3(const double* a, long long P, long long m) {
+    return V3{__ldg(a + m), __ldg(a + P + m), __ldg(a + 2 * P + m)};
+}
+
 __device__ __forceinline__ bool m3_cell(long long t, int lo, int hi_incl, const Geo& G, int& i, int& j, int& k) {
     const int lo3[3] = {lo, lo, lo};
     const int ext[3] = {G.n[0] + hi_incl - lo + 1, G.n[1] + hi_incl - lo + 1, G.n[2] + hi_incl - lo + 1};
@@ -64,11 +80,11 @@ __global__ void __launch_bounds__(256, 2) k_m3_halfstates(Mhd3DArgs A) {
     const Geo& G = A.G;
     const Geo& F = A.FG;
     const long long P = G.plane, FP = F.plane, SP = A.S.plane;
-    auto W = [&](int a, int b, int c) { return load_prim<true>(A.w, P, gidx3(G, a, b, c)); };
+    auto W = [&](int a, int b, int c) { return m3_ld_prim(A.w, P, gidx3(G, a, b, c)); };
     const long long f = gidx3(F, i, j, k);
-    const double bx0 = A.B[f], bx1 = A.B[gidx3(F, i + 1, j, k)];
-    const double by0 = A.B[FP + f], by1 = A.B[FP + gidx3(F, i, j + 1, k)];
-    const double bz0 = A.B[2 * FP + f], bz1 = A.B[2 * FP + gidx3(F, i, j, k + 1)];
+    const double bx0 = m3_ld(A.B, f), bx1 = m3_ld(A.B, gidx3(F, i + 1, j, k));
+    const double by0 = m3_ld(A.B, FP + f), by1 = m3_ld(A.B, FP + gidx3(F, i, j + 1, k));
+    const double bz0 = m3_ld(A.B, 2 * FP + f), bz1 = m3_ld(A.B, 2 * FP + gidx3(F, i, j, k + 1));
     const double dBx = (bx1 - bx0) * dt_dx, dBy = (by1 - by0) * dt_dy, dBz = (bz1 - bz0) * dt_dz;
     const Prim<double> wc = W(i, j, k);
     int fo = 0;
@@ -110,8 +126,8 @@ __device__ __forceinline__ void m3_face_flux(const Mhd3DArgs& A, int i, int j, i
     const Geo& F = A.FG;
     const long long SP = A.S.plane;
     const int di = AX == 0, dj = AX == 1, dk = AX == 2;
-    const Prim<double> L = load_prim<true>(m3_hs(A, AX, 1), SP, gidx3(F, i - di, j - dj, k - dk));
-    const Prim<double> R = load_prim<true>(m3_hs(A, AX, 0), SP, gidx3(F, i, j, k));
+    const Prim<double> L = m3_ld_prim(m3_hs(A, AX, 1), SP, gidx3(F, i - di, j - dj, k - dk));
+    const Prim<double> R = m3_ld_prim(m3_hs(A, AX, 0), SP, gidx3(F, i, j, k));
     Cons<double> Fl;
     face_flux<true, SOLVER, AX>(L, R, dtn, exact_opts(A.sa), Fl, st);
     store_cons8(m3_flux_w(A, AX), SP, gidx3(F, i, j, k), Fl);
@@ -139,10 +155,10 @@ __global__ void __launch_bounds__(256, 2) k_m3_fluxes(Mhd3DArgs A) {
 __device__ __forceinline__ V3 m3_edge_e(const Mhd3DArgs& A, const double* __restrict__ eref, int i, int j, int k) {
     const Geo& F = A.FG;
     const long long SP = A.S.plane;
-    auto X = [&](int a, int b, int c, int q) { return A.S.fx[q * SP + gidx3(F, a, b, c)]; };
-    auto Y = [&](int a, int b, int c, int q) { return A.S.fy[q * SP + gidx3(F, a, b, c)]; };
-    auto Z = [&](int a, int b, int c, int q) { return A.S.fz[q * SP + gidx3(F, a, b, c)]; };
-    auto ER = [&](int a, int b, int c) { return load_v3(eref, SP, gidx3(F, a, b, c)); };
+    auto X = [&](int a, int b, int c, int q) { return m3_ld(A.S.fx, q * SP + gidx3(F, a, b, c)); };
+    auto Y = [&](int a, int b, int c, int q) { return m3_ld(A.S.fy, q * SP + gidx3(F, a, b, c)); };
+    auto Z = [&](int a, int b, int c, int q) { return m3_ld(A.S.fz, q * SP + gidx3(F, a, b, c)); };
+    auto ER = [&](int a, int b, int c) { return m3_ld_v3(eref, SP, gidx3(F, a, b, c)); };
     // flux planes: 0 rho, 1 E, 2-4 momentum, 5 Bx, 6 By, 7 Bz
     V3 e;
     e.x = (Z(i, j - 1, k, 6) - Y(i, j, k - 1, 7) + Z(i, j, k, 6) - Y(i, j, k, 7)) * 0.25;
@@ -186,15 +202,15 @@ struct M3Faces {
 __device__ __forceinline__ M3Faces m3_faraday(const Mhd3DArgs& A, int i, int j, int k, double hx, double hy, double hz) {
     const Geo& F = A.FG;
     const long long FP = F.plane, SP = A.S.plane;
-    auto E = [&](int a, int b, int c) { return load_v3(A.S.e0, SP, gidx3(F, a, b, c)); };
+    auto E = [&](int a, int b, int c) { return m3_ld_v3(A.S.e0, SP, gidx3(F, a, b, c)); };
     auto bx = [&](int a) {
-        return A.B[gidx3(F, a, j, k)] - ((E(a, j + 1, k).z - E(a, j, k).z) * hy - (E(a, j, k + 1).y - E(a, j, k).y) * hz);
+        return m3_ld(A.B, gidx3(F, a, j, k)) - ((E(a, j + 1, k).z - E(a, j, k).z) * hy - (E(a, j, k + 1).y - E(a, j, k).y) * hz);
     };
     auto by = [&](int b) {
-        return A.B[FP + gidx3(F, i, b, k)] - ((E(i, b, k + 1).x - E(i, b, k).x) * hz - (E(i + 1, b, k).z - E(i, b, k).z) * hx);
+        return m3_ld(A.B, FP + gidx3(F, i, b, k)) - ((E(i, b, k + 1).x - E(i, b, k).x) * hz - (E(i + 1, b, k).z - E(i, b, k).z) * hx);
     };
     auto bz = [&](int c) {
-        return A.B[2 * FP + gidx3(F, i, j, c)] - ((E(i + 1, j, c).y - E(i, j, c).y) * hx - (E(i, j + 1, c).x - E(i, j, c).x) * hy);
+        return m3_ld(A.B, 2 * FP + gidx3(F, i, j, c)) - ((E(i + 1, j, c).y - E(i, j, c).y) * hx - (E(i, j + 1, c).x - E(i, j, c).x) * hy);
     };
     return M3Faces{bx(i), bx(i + 1), by(j), by(j + 1), bz(k), bz(k + 1)};
 }
@@ -213,10 +229,10 @@ __global__ void __launch_bounds__(256, 2) k_m3_half(Mhd3DArgs A) {
     const long long P = G.plane, FP = F.plane, SP = A.S.plane;
     const long long m = gidx3(F, i, j, k);
     const M3Faces h = m3_faraday(A, i, j, k, hdx, hdy, hdz);
-    const Prim<double> W = load_prim<true>(A.w, P, gidx3(G, i, j, k));
-    const Cons<double> px0 = load_cons8(A.S.fx, SP, m), px1 = load_cons8(A.S.fx, SP, gidx3(F, i + 1, j, k));
-    const Cons<double> py0 = load_cons8(A.S.fy, SP, m), py1 = load_cons8(A.S.fy, SP, gidx3(F, i, j + 1, k));
-    const Cons<double> pz0 = load_cons8(A.S.fz, SP, m), pz1 = load_cons8(A.S.fz, SP, gidx3(F, i, j, k + 1));
+    const Prim<double> W = m3_ld_prim(A.w, P, gidx3(G, i, j, k));
+    const Cons<double> px0 = m3_ld_cons(A.S.fx, SP, m), px1 = m3_ld_cons(A.S.fx, SP, gidx3(F, i + 1, j, k));
+    const Cons<double> py0 = m3_ld_cons(A.S.fy, SP, m), py1 = m3_ld_cons(A.S.fy, SP, gidx3(F, i, j + 1, k));
+    const Cons<double> pz0 = m3_ld_cons(A.S.fz, SP, m), pz1 = m3_ld_cons(A.S.fz, SP, gidx3(F, i, j, k + 1));
     {
         // applyFluxes g=1 at dt/2 (Unsplit.cpp:272-288), computeBodyFields, bodyElectric
         Cons<double> U = to_cons<true>(W);
@@ -229,10 +245,10 @@ __global__ void __launch_bounds__(256, 2) k_m3_half(Mhd3DArgs A) {
         store_v3(A.S.eh, SP, m, body_e(wh));
     }
     // CTU corrections (CTU.cpp:66-129)
-    const double dBx = (A.B[gidx3(F, i + 1, j, k)] - A.B[m]) * dt_dx;
-    const double dBy = (A.B[FP + gidx3(F, i, j + 1, k)] - A.B[FP + m]) * dt_dy;
-    const double dBz = (A.B[2 * FP + gidx3(F, i, j, k + 1)] - A.B[2 * FP + m]) * dt_dz;
-    auto E0 = [&](int a, int b, int c) { return load_v3(A.S.e0, SP, gidx3(F, a, b, c)); };
+    const double dBx = (m3_ld(A.B, gidx3(F, i + 1, j, k)) - m3_ld(A.B, m)) * dt_dx;
+    const double dBy = (m3_ld(A.B, FP + gidx3(F, i, j + 1, k)) - m3_ld(A.B, FP + m)) * dt_dy;
+    const double dBz = (m3_ld(A.B, 2 * FP + gidx3(F, i, j, k + 1)) - m3_ld(A.B, 2 * FP + m)) * dt_dz;
+    auto E0 = [&](int a, int b, int c) { return m3_ld_v3(A.S.e0, SP, gidx3(F, a, b, c)); };
     auto apply = [&](int axis, Cons<double> corr, double bl, double br) {
         double* pl = m3_hs(A, axis, 0);
         double* pr = m3_hs(A, axis, 1);
@@ -299,10 +315,10 @@ __global__ void k_m3_update(Mhd3DArgs A) {
         const int nx = G.n[0], ny = G.n[1], nz = G.n[2];
         const long long mc = gidx3(G, i, j, k), mf = gidx3(F, i, j, k);
         const M3Faces b = m3_faraday(A, i, j, k, dt_dx, dt_dy, dt_dz);
-        Cons<double> U = to_cons<true>(load_prim<true>(A.w, P, mc));
-        U = c_add<true>(U, c_mul<true>(c_sub<true>(load_cons8(A.S.fx, SP, mf), load_cons8(A.S.fx, SP, gidx3(F, i + 1, j, k))), dt_dx));
-        U = c_add<true>(U, c_mul<true>(c_sub<true>(load_cons8(A.S.fy, SP, mf), load_cons8(A.S.fy, SP, gidx3(F, i, j + 1, k))), dt_dy));
-        U = c_add<true>(U, c_mul<true>(c_sub<true>(load_cons8(A.S.fz, SP, mf), load_cons8(A.S.fz, SP, gidx3(F, i, j, k + 1))), dt_dz));
+        Cons<double> U = to_cons<true>(m3_ld_prim(A.w, P, mc));
+        U = c_add<true>(U, c_mul<true>(c_sub<true>(m3_ld_cons(A.S.fx, SP, mf), m3_ld_cons(A.S.fx, SP, gidx3(F, i + 1, j, k))), dt_dx));
+        U = c_add<true>(U, c_mul<true>(c_sub<true>(m3_ld_cons(A.S.fy, SP, mf), m3_ld_cons(A.S.fy, SP, gidx3(F, i, j + 1, k))), dt_dy));
+        U = c_add<true>(U, c_mul<true>(c_sub<true>(m3_ld_cons(A.S.fz, SP, mf), m3_ld_cons(A.S.fz, SP, gidx3(F, i, j, k + 1))), dt_dz));
         if (!is_finite<true>(U)) record_error(A.ctl, ST_NAN, mc);
         Prim<double> nw = body_field(to_prim<true>(U), (b.bx0 + b.bx1) * 0.5, (b.by0 + b.by1) * 0.5, (b.bz0 + b.bz1) * 0.5,
                                      A.sa.ct_energy);

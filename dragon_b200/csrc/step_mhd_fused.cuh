@@ -144,6 +144,11 @@ __global__ void __launch_bounds__(NT, 2) k_mhd2d_fused_mixed(Geo G, Geo FG, cons
     extern __shared__ __align__(16) unsigned char smem_raw[];
     S_t& S = *reinterpret_cast<S_t*>(smem_raw);
     if (mhd_skip(ctl, &S.skip)) return;
+    // The ghost frame of the output buffers (every point the update does not
+    // write) is copied from the inputs by all CTAs, before any returns early.
+    mhd2d_copy_frame(G, FG, w, wout, B, Bout, 0, mhd2d_frame_points(G.n[0], G.n[1], G.g),
+                     ((long long)blockIdx.y * gridDim.x + blockIdx.x) * NT + threadIdx.x,
+                     (long long)gridDim.x * gridDim.y * NT);
 
     const int nx = G.n[0], ny = G.n[1];
     const long long P = G.plane, FP = FG.plane;

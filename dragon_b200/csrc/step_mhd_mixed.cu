@@ -38,7 +38,6 @@ int launch_fused(const Geo& G, const Geo& FG, const double* w, double* wout, con
     int seg = (nx + segs_wanted - 1) / segs_wanted;
     seg = std::max(4 * kFuseR, (seg + kFuseR - 1) / kFuseR * kFuseR);
     const dim3 grid(strips, (nx + seg - 1) / seg);
-    if (launch_mhd2d_copy_frame(G, FG, w, wout, B, Bout, st)) return 1;
     kern<<<grid, kFuseNT, smem, st>>>(G, FG, w, wout, B, Bout, ctl, sa, seg);
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
