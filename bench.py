@@ -560,8 +560,10 @@ def stated_length_report(n=1024, kh_steps=2000, ot_time=0.5):
 def custom_bc_report(n=1024, steps=20, warmup=3):
     """A user GhostFill element (an inflow jet on X-, the reference's Jet
     pattern) on the n^2 shear layer against the same grid with built-in
-    elements only: wall time per CFL step of advance_steps. The user element
-    runs on the host; only the slabs along its face cross the host link."""
+    elements only: wall time per CFL step of advance_steps. The jet runs as a
+    host apply() (only the slabs along its face cross the host link) and as a
+    device fill compiled with NVRTC (DeviceGhostFill: inside the device
+    advance loop); both give the same states bit for bit."""
     import torch
 
     import dragon_b200 as dg
@@ -580,10 +582,24 @@ def custom_bc_report(n=1024, steps=20, warmup=3):
                 w[g - gl] = w[g]
                 w[g - gl, jet] = (2.0, 3.0, 1.5, 0.0, 0.0)
 
+    jet_src = """
+__device__ void jet(const dragon_fill_ctx& c, int i, int j, int k) {
+    for (int f = 0; f < c.nf; f++) c.set(f, i, j, k, c.get(f, 0, j, k));
+    if (fabs((j + 0.5) * c.d[1] - 0.5) < 0.1) {
+        c.set(DRAGON_RHO, i, j, k, 2.0);
+        c.set(DRAGON_P, i, j, k, 3.0);
+        c.set(DRAGON_VX, i, j, k, 1.5);
+        c.set(DRAGON_VY, i, j, k, 0.0);
+        c.set(DRAGON_VZ, i, j, k, 0.0);
+    }
+}
+"""
     w0, dx, dy = problems.kelvin_helmholtz_2d(n, ghosts=2, seed=1234)
     out = {"workload": f"shear layer {n}^2, X- inflow jet (user element) + Outflow X+ + Periodic Y"}
+    states = {}
     for name, bl in (("builtin", dg.Outflow("X") + dg.Periodic("Y")),
-                     ("user_element", dg.Periodic("Y") + Jet(dy, 2))):
+                     ("user_element", dg.Periodic("Y") + Jet(dy, 2)),
+                     ("device_element", dg.Periodic("Y") + dg.DeviceGhostFill(jet_src, "jet", faces="X-"))):
         G = dg.Grid2D(n, n, dx, dy, ghosts=2, config=dg.Config(riemann=dg.RIEMANN_HLLC, limiter=dg.LIMITER_VANLEER))
         G.w[...] = w0
         G.boundary = bl
@@ -593,8 +609,11 @@ def custom_bc_report(n=1024, steps=20, warmup=3):
         G.advance_steps(steps)
         torch.cuda.synchronize()
         out[name + "_ms_per_step"] = (time.perf_counter() - t0) / steps * 1e3
+        states[name] = G.w.copy()
         G.close()
     out["ratio"] = out["user_element_ms_per_step"] / out["builtin_ms_per_step"]
+    out["device_ratio"] = out["device_element_ms_per_step"] / out["builtin_ms_per_step"]
+    out["device_equals_host_element"] = bool(np.array_equal(states["device_element"], states["user_element"]))
     return out
 
 
@@ -761,7 +780,8 @@ def summary_of(d):
         out["learned_guess"]["iters_per_solve"] = {k: g[k]["newton_iters_per_solve"] for k in g
                                                    if isinstance(g[k], dict) and "newton_iters_per_solve" in g[k]}
     if "custom_bc" in d:
-        out["user_ghostfill_step_vs_builtin"] = d["custom_bc"]["ratio"]
+        out["user_ghostfill_step_vs_builtin"] = {"host_apply": d["custom_bc"]["ratio"],
+                                                 "device_fill": d["custom_bc"]["device_ratio"]}
     if "dist" in d:
         out["distgrid_4096_strong"] = {"value": d["dist"]["value"], "ms_per_step": d["dist"]["ms_per_step"]}
     if "batch" in d:

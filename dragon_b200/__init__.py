@@ -3,7 +3,7 @@
 The host-side mirror of DRAGON's Grid / Boundary API over the C ABI declared
 in include/dragon_gpu.h (library: dragon_b200/libdragon_gpu.so).
 """
-from .boundary import (X, Y, Z, BoundaryList, Fixed, GhostFill, Ignore, Outflow, Periodic, Reflective,
+from .boundary import (X, Y, Z, BoundaryList, DeviceGhostFill, Fixed, GhostFill, Ignore, Outflow, Periodic, Reflective,
                        X_negative, X_positive, Y_negative, Y_positive, Z_negative, Z_positive, face_mask)
 from .grid import (CFL_ADD, CFL_MAX, CT_CONSV_BETA_GATED, CT_CONSV_THERMAL, CT_CONSV_TOTAL_E, GUESS_ANALYTIC,
                    GUESS_LEARNED, GUESS_MEAN, GUESS_PERFECT, LIMITER_MC,

@@ -153,6 +153,11 @@ SIGNATURES = {
     "dragon_gpu_launch_count": (ctypes.c_ulonglong, [ctypes.c_void_p]),
     "dragon_gpu_profile_enable": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "dragon_gpu_debug_set": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "dragon_gpu_user_fill_create": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)]),
+    "dragon_gpu_user_fill_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "dragon_gpu_user_fill_log": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "dragon_gpu_set_user_fill": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                                ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_int]),
     "dragon_gpu_profile_read": (
         ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong),
                        ctypes.c_int]),

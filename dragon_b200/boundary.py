@@ -12,6 +12,8 @@ Example (the reference's ``Boundary::Reflective("X") + Boundary::Periodic("YZ")`
 """
 from __future__ import annotations
 
+import ctypes
+
 from typing import Iterable, Sequence
 
 # Face bits (Boundary.hpp:139-149)
@@ -25,7 +27,7 @@ Z_negative = 1 << 4
 Z_positive = 1 << 5
 Z = Z_negative | Z_positive
 
-OUTFLOW, OUTFLOW_GATED, FIXED, REFLECTIVE, PERIODIC, IGNORE = range(6)
+OUTFLOW, OUTFLOW_GATED, FIXED, REFLECTIVE, PERIODIC, IGNORE, USER = range(7)
 
 
 def face_mask(s: str) -> int:
@@ -98,6 +100,54 @@ class GhostFill:
 
     def __repr__(self):
         return f"{type(self).__name__}(faces={self.faces}, corners={self.corners})"
+
+
+class DeviceGhostFill(GhostFill):
+    """A user element (GhostFill.hpp:16-30) whose fill runs on the device.
+
+    `source` is CUDA C++ defining ``__device__ void <function>(const
+    dragon_fill_ctx& c, int i, int j, int k)``, called once per ghost cell of
+    `fill_faces` (the faces whose ghost layers it fills; default its own
+    `faces` mask) with c.get / c.set (primitive fields DRAGON_RHO, DRAGON_P,
+    DRAGON_VX.. , DRAGON_BX..), c.getB / c.setB (face B), c.n, c.g, c.d,
+    c.axis / c.side and c.params (`params`); include/dragon_gpu.h gives the
+    contract. It is compiled once with NVRTC and the grid launches it at the
+    element's place in the list inside the device advance loop, so unlike a
+    host `apply` no state crosses the host link. `faces` keeps its
+    BoundaryList meaning: the faces the element claims (the reference's Jet
+    claims none, GhostFill(0, true), and fills its jet face over the implicit
+    Outflow)."""
+
+    kind = USER
+    _compiled = {}
+
+    def __init__(self, source: str, function: str, faces=0, corner_ghosts: bool = True, fill_faces=None,
+                 params: Sequence[float] = ()):
+        super().__init__(faces, corner_ghosts)
+        self.fill_faces = self.faces if fill_faces is None else _faces(fill_faces)
+        self.params = [float(v) for v in params]
+        self.source, self.function = source, function
+        self._fill = DeviceGhostFill.compile(source, function)
+
+    @staticmethod
+    def compile(source: str, function: str):
+        """The compiled fill (a dragon_user_fill*), shared by every element
+        with the same source and function."""
+        key = (source, function)
+        if key not in DeviceGhostFill._compiled:
+            from . import _lib
+            lib = _lib.load()
+            out = ctypes.c_void_p()
+            _lib.check(lib.dragon_gpu_user_fill_create(source.encode(), function.encode(), ctypes.byref(out)))
+            DeviceGhostFill._compiled[key] = out
+        return DeviceGhostFill._compiled[key]
+
+    def bind(self, lib, handle, entry: int):
+        """dragon_gpu_set_user_fill for list entry `entry` of a grid."""
+        from . import _lib
+        arr = (ctypes.c_double * max(1, len(self.params)))(*self.params)
+        _lib.check(lib.dragon_gpu_set_user_fill(handle, entry, self._fill, self.fill_faces, int(self.corners), arr,
+                                                len(self.params)))
 
 
 class Outflow(GhostFill):

@@ -387,6 +387,8 @@ int dragon_gpu_batch_add_instance(dragon_batch* b, dragon_grid* h, int* index) {
     if (h->cfg.precision != 0 && h->cfg.precision != 1) return fail(DRAGON_GPU_EINVAL, "unknown precision");
     if (b->prec >= 0 && b->prec != h->cfg.precision)
         return fail(DRAGON_GPU_EUNSUPPORTED, "batched members share one precision (FP64 or mixed)");
+    if (!h->user_entries.empty())
+        return fail(DRAGON_GPU_EUNSUPPORTED, "batched members run built-in boundary elements only (no user fills)");
     if (h->dim == 1 && !h->mhd) {
         if (h->solver != RS_HLLC && h->solver != RS_EXACT)
             return fail(DRAGON_GPU_EUNSUPPORTED, "batched 1D members use HLLC / HLLX or the exact solver");

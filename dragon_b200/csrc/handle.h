@@ -16,6 +16,18 @@
 namespace dgpu {
 struct MlpNet;
 }
+struct dragon_user_fill;
+
+// A user ghost fill bound to one entry of a grid's boundary list
+// (dragon_gpu_set_user_fill): the compiled fill, the faces whose ghost cells it
+// visits, whether it visits their corners, and its parameters on the device.
+struct UserFillBinding {
+    dragon_user_fill* fill = nullptr;
+    int fill_faces = 0;
+    int corners = 1;
+    double* dparams = nullptr;
+    int nparams = 0;
+};
 
 // The device advance loop between its first batch and its completion
 // (dragon_gpu_advance_steps_async / dragon_gpu_advance_wait).
@@ -87,6 +99,12 @@ struct dragon_grid {
     // of devices without cooperative launch
     int dbg_stall_cta = -1;
     bool dbg_no_coop = false;
+    // user ghost fills: entries of the compiled list that are device user
+    // fills (in list order), their bindings (indexed by entry), and the length
+    // of the caller's list (the compiled list may start with an implicit Outflow)
+    std::vector<int> user_entries;
+    std::vector<UserFillBinding> ufill;
+    int caller_entries = 0;
     // TMA tensor maps of the two state buffers for the fused 2D hydro kernels
     // (FP64, mixed), encoded on first use
     CUtensorMap tmap[2][2];
@@ -108,5 +126,11 @@ int zero_slot(dragon_grid* h, int slot);
 void reset_ctl(dragon_grid* h, double remaining, int max_steps, int check_cfl);
 void add_newton(dragon_grid* h, const dgpu::StepCtl& c);
 const char* stage_name(int s);
+// Enqueues the bound user fill of compiled boundary entry `entry` on state
+// buffer c (w_buf overrides the cell array); skipped on the device once the
+// advance is done or failed (user_fill.cu).
+int launch_user_fill(dragon_grid* h, int c, int entry, double* w_buf);
+// Releases a handle's user-fill bindings (their device parameters).
+void clear_user_fills(dragon_grid* h);
 
 }  // namespace dgpu_rt

@@ -294,8 +294,8 @@ int launch_step(dragon_grid* h, int c) {
 }
 
 // w_buf overrides the state buffer (the Strang-split sweeps fill ghosts of their intermediate buffers).
-int launch_prologue(dragon_grid* h, int c, int bookkeeping, int apply_bc, int compute_dt, int slot_in, int slot_out,
-                    double* w_buf = nullptr, int bc_first = 0, int bc_count = -1) {
+static int launch_prologue_range(dragon_grid* h, int c, int bookkeeping, int apply_bc, int compute_dt, int slot_in,
+                                 int slot_out, double* w_buf, int bc_first, int bc_count) {
     double* W = w_buf ? w_buf : h->w[c];
     if (bc_count < 0) bc_count = h->nbc - bc_first;
     PrologueArgs pa;
@@ -385,6 +385,33 @@ int launch_prologue(dragon_grid* h, int c, int bookkeeping, int apply_bc, int co
         one_cta(tail);
     }
     CK(cudaGetLastError());
+    return 0;
+}
+
+// The prologue over entries [bc_first, bc_first + bc_count) of the compiled
+// list (all of them by default). A user fill compiled for the device splits
+// it: the prologue of the entries before it (with the bookkeeping), the fill's
+// kernel, then the rest, the last part computing dt; everything stays in the
+// stream, so the device advance loop runs on without the host.
+int launch_prologue(dragon_grid* h, int c, int bookkeeping, int apply_bc, int compute_dt, int slot_in, int slot_out,
+                    double* w_buf = nullptr, int bc_first = 0, int bc_count = -1) {
+    if (bc_count < 0) bc_count = h->nbc - bc_first;
+    if (!apply_bc || h->user_entries.empty())
+        return launch_prologue_range(h, c, bookkeeping, apply_bc, compute_dt, slot_in, slot_out, w_buf, bc_first,
+                                     bc_count);
+    int seg = bc_first, head = 1, rc;
+    for (int u : h->user_entries) {
+        if (u < bc_first || u >= bc_first + bc_count) continue;
+        if (u > seg || (head && bookkeeping))
+            if ((rc = launch_prologue_range(h, c, head ? bookkeeping : 0, 1, 0, slot_in, slot_out, w_buf, seg, u - seg)))
+                return rc;
+        if ((rc = launch_user_fill(h, c, u, w_buf))) return rc;
+        seg = u + 1;
+        head = 0;
+    }
+    const int rest = bc_first + bc_count - seg;
+    if (rest > 0 || compute_dt || (head && bookkeeping))
+        return launch_prologue_range(h, c, head ? bookkeeping : 0, 1, compute_dt, slot_in, slot_out, w_buf, seg, rest);
     return 0;
 }
 
@@ -791,6 +818,7 @@ int dragon_gpu_grid_destroy(dragon_grid* h) {
     if (!h) return 0;
     if (h->stream) cudaStreamSynchronize(h->stream);
     collect_profile(h);
+    clear_user_fills(h);
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
     for (int b = 0; b < 2; b++) {
         if (h->w[b]) cudaFree(h->w[b]);
@@ -864,9 +892,16 @@ int dragon_gpu_set_boundary(dragon_grid* h, const dragon_bc_desc* list, int n) {
     // implicit Outflow over every face no entry covers (BoundaryList.hpp:97-104)
     int uncovered = FX_NEG | FX_POS | FY_NEG | FY_POS | FZ_NEG | FZ_POS;
     std::vector<BCEntry> user;
+    std::vector<int> device_fill;  // caller indices of user fills compiled for the device
     for (int i = 0; i < n; i++) {
         BCEntry e{};
         e.type = list[i].type;
+        if (e.type == DRAGON_BC_USER) {
+            // the device list carries it as Ignore (its faces count as covered);
+            // the prologue launches its bound fill at this place
+            e.type = BC_IGNORE;
+            device_fill.push_back(i);
+        }
         if (e.type < BC_OUTFLOW || e.type > BC_IGNORE) return fail(DRAGON_GPU_EINVAL, "unknown boundary type");
         e.faces = list[i].faces & 63;
         if (e.type == BC_PERIODIC) {
@@ -893,6 +928,11 @@ int dragon_gpu_set_boundary(dragon_grid* h, const dragon_bc_desc* list, int n) {
     if (h->dbcs) { cudaStreamSynchronize(h->stream); cudaFree(h->dbcs); h->dbcs = nullptr; }
     h->nbc = (int)v.size();
     h->hbcs = v;
+    clear_user_fills(h);
+    h->caller_entries = n;
+    h->user_entries.clear();
+    for (int i : device_fill) h->user_entries.push_back(h->nbc - n + i);
+    h->ufill.assign(h->nbc, UserFillBinding{});
     if (h->nbc) {
         CK(cudaMalloc(&h->dbcs, sizeof(BCEntry) * v.size()));
         CK(cudaMemcpyAsync(h->dbcs, v.data(), sizeof(BCEntry) * v.size(), cudaMemcpyHostToDevice, h->stream));

@@ -48,7 +48,7 @@ import torch
 import torch.distributed as tdist
 
 from . import _lib
-from .boundary import IGNORE, OUTFLOW, PERIODIC, X, X_negative, X_positive, BoundaryList, as_list
+from .boundary import IGNORE, OUTFLOW, PERIODIC, USER, X, X_negative, X_positive, BoundaryList, as_list
 from .grid import AdvanceResult, Config, Grid1D, Grid2D, Grid3D, StepFailed
 
 ALL_FACES = 63
@@ -100,6 +100,8 @@ class SlabProgram:
         els = list(blist)
         if any(e.is_custom for e in els):
             raise NotImplementedError("boundary elements with a host apply() are not supported on a DistGrid")
+        if any(e.kind == USER for e in els):
+            raise NotImplementedError("device user fills (DeviceGhostFill) are not supported on a DistGrid")
         uncovered = ALL_FACES
         for e in els:
             uncovered &= ~_normalised_faces(e)

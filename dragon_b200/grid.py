@@ -20,7 +20,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _lib
-from .boundary import IGNORE, BoundaryList, as_list
+from .boundary import IGNORE, USER, BoundaryList, as_list
 
 # Config ids (DRAGON/Config.h)
 RIEMANN_EXACT, RIEMANN_HLL, RIEMANN_HLLC, RIEMANN_HLLD, RIEMANN_HLLE, RIEMANN_HLLX, RIEMANN_ROE = range(7)
@@ -298,6 +298,9 @@ class _GridBase:
             for q in range(8):
                 arr[k].state[q] = st[q]
         _lib.check(self._lib.dragon_gpu_set_boundary(self._h, arr, len(els)))
+        for k, e in enumerate(els):
+            if e.kind == USER:
+                e.bind(self._lib, self._h, k)
 
     def _apply_boundary_host(self):
         """BoundaryList::apply (BoundaryList.hpp:79-93) with user elements: the

@@ -121,6 +121,9 @@ void DistGrid::program() {
     if (rank_ == parts_ - 1) own |= Boundary::X_positive;
     if (boundary.has_user_elements())
         throw std::logic_error("boundary elements with a host apply() are not supported on a DistGrid");
+    for (size_t k = 0; k < boundary.size(); k++)
+        if (boundary[k].device_type() == DRAGON_BC_USER)
+            throw std::logic_error("device user fills (Boundary::DeviceFill) are not supported on a DistGrid");
     std::vector<dragon_bc_desc> e;
     auto entry = [](int type, int faces, int corners, const double* st) {
         dragon_bc_desc d;

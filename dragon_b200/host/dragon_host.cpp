@@ -108,6 +108,14 @@ int BoundaryList::uncovered_faces() const {
     return unc;
 }
 
+DeviceFill::DeviceFill(const std::string& source, const std::string& function, int faces, int fill_faces_,
+                       std::vector<double> params_, bool corner_ghosts)
+    : GhostFill(faces, corner_ghosts), fill_faces(fill_faces_), params(std::move(params_)) {
+    dragon_user_fill* f = nullptr;
+    if (dragon_gpu_user_fill_create(source.c_str(), function.c_str(), &f)) throw std::runtime_error(dragon_gpu_last_error());
+    fill_.reset(f, [](dragon_user_fill* p) { dragon_gpu_user_fill_destroy(p); });
+}
+
 std::vector<dragon_bc_desc> BoundaryList::descriptors() const {
     std::vector<dragon_bc_desc> out;
     out.reserve(elements.size());
@@ -247,11 +255,24 @@ void Grid::to_device() {
 
 void Grid::push_boundary() {
     const std::vector<dragon_bc_desc> d = boundary.descriptors();
+    std::vector<std::tuple<const void*, int, std::vector<double>>> fills;
+    for (size_t k = 0; k < boundary.size(); k++)
+        if (auto* f = dynamic_cast<const Boundary::DeviceFill*>(&boundary[k]))
+            fills.emplace_back(f->compiled(), f->fill_faces, f->params);
     if (pushed_valid_ && d.size() == pushed_.size() &&
-        (d.empty() || std::memcmp(d.data(), pushed_.data(), sizeof(dragon_bc_desc) * d.size()) == 0))
+        (d.empty() || std::memcmp(d.data(), pushed_.data(), sizeof(dragon_bc_desc) * d.size()) == 0) &&
+        fills == pushed_fills_)
         return;
+    pushed_valid_ = false;
     if (int rc = dragon_gpu_set_boundary(h_, d.data(), (int)d.size())) raise(rc);
+    // bind each device fill to its entry (dragon_gpu_set_boundary dropped the old bindings)
+    for (size_t k = 0; k < boundary.size(); k++)
+        if (auto* f = dynamic_cast<const Boundary::DeviceFill*>(&boundary[k]))
+            if (int rc = dragon_gpu_set_user_fill(h_, (int)k, f->compiled(), f->fill_faces, f->get_corners() ? 1 : 0,
+                                                  f->params.data(), (int)f->params.size()))
+                raise(rc);
     pushed_ = d;
+    pushed_fills_ = std::move(fills);
     pushed_valid_ = true;
 }
 

@@ -33,6 +33,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <tuple>
 #include <type_traits>
 #include <utility>
 #include <vector>
@@ -228,6 +229,30 @@ public:
     int device_type() const override { return 5; }
 };
 
+// A user element compiled for the device (dragon_gpu_user_fill_create):
+// `source` defines __device__ void <function>(const dragon_fill_ctx& c, int i,
+// int j, int k), called for every ghost cell of `fill_faces` (the contract is
+// in dragon_gpu.h). It runs at its place in the list inside the device
+// advance loop, with no host round trip; `faces` keeps its BoundaryList
+// meaning (the reference's Jet claims none, GhostFill(0, true)). Throws
+// std::runtime_error with NVRTC's log when the source does not compile.
+class DeviceFill : public GhostFill {
+public:
+    DeviceFill(const std::string& source, const std::string& function, int faces, int fill_faces,
+               std::vector<double> params = {}, bool corner_ghosts = true);
+    DeviceFill(const std::string& source, const std::string& function, std::string faces, std::string fill_faces,
+               std::vector<double> params = {}, bool corner_ghosts = true)
+        : DeviceFill(source, function, face_mask(std::move(faces)), face_mask(std::move(fill_faces)),
+                     std::move(params), corner_ghosts) {}
+    int device_type() const override { return DRAGON_BC_USER; }
+    dragon_user_fill* compiled() const { return fill_.get(); }
+    int fill_faces;
+    std::vector<double> params;
+
+private:
+    std::shared_ptr<dragon_user_fill> fill_;
+};
+
 // Elements applied in order after an implicit Outflow over every face no
 // element covers (BoundaryList.hpp:79-104). Move-only, like the reference's.
 class BoundaryList : public GhostFill {
@@ -387,6 +412,8 @@ protected:
     mutable bool dev_newer_ = false;
     bool host_newer_ = true;
     std::vector<dragon_bc_desc> pushed_;
+    // device fills bound with the pushed list: (fill, fill faces, params) per entry
+    std::vector<std::tuple<const void*, int, std::vector<double>>> pushed_fills_;
     bool pushed_valid_ = false;
     AdvanceStats stats_{};
 

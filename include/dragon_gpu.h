@@ -66,9 +66,12 @@ typedef struct dragon_config {
 void dragon_gpu_default_config(dragon_config* cfg, int mhd);
 
 /* Boundary list entry (DRAGON/Boundary/Boundary.hpp:158-229). type: 0 Outflow,
- * 1 Outflow::Gated, 2 Fixed, 3 Reflective, 4 Periodic, 5 Ignore. faces is the
- * bit mask of Boundary::face_mask (X- 1, X+ 2, Y- 4, Y+ 8, Z- 16, Z+ 32);
- * state is Fixed's primitive state (NF values). */
+ * 1 Outflow::Gated, 2 Fixed, 3 Reflective, 4 Periodic, 5 Ignore, 6 a user
+ * GhostFill compiled for the device (DRAGON_BC_USER; bind its fill with
+ * dragon_gpu_set_user_fill). faces is the bit mask of Boundary::face_mask
+ * (X- 1, X+ 2, Y- 4, Y+ 8, Z- 16, Z+ 32); state is Fixed's primitive state
+ * (NF values). */
+#define DRAGON_BC_USER 6
 typedef struct dragon_bc_desc {
     int type;
     int faces;
@@ -134,6 +137,41 @@ int dragon_gpu_apply_boundary(dragon_grid* g);
  * in list order (BoundaryList.hpp:79-93). */
 int dragon_gpu_boundary_entries(const dragon_grid* g);
 int dragon_gpu_apply_boundary_range(dragon_grid* g, int first, int count);
+
+/* A user GhostFill element (Boundary/GhostFill.hpp:16-30; the Jet of
+ * Examples/CollidingFlows/Jets/Jets.hpp:12-39 is the reference's example)
+ * written as a CUDA device function and compiled for the device with NVRTC:
+ *
+ *     __device__ void NAME(const dragon_fill_ctx& c, int i, int j, int k);
+ *
+ * is called once per ghost cell (i, j, k) of the faces it is bound to fill
+ * (interior coordinates: ghosts are negative or >= n), with c.axis / c.side
+ * the face. dragon_fill_ctx gives the padded state: c.get(f, i, j, k) /
+ * c.set(f, i, j, k, v) on primitive field f (DRAGON_RHO, DRAGON_P,
+ * DRAGON_VX..VZ, DRAGON_BX..BZ), c.getB / c.setB on face B (MHD 2D / 3D),
+ * c.n[3], c.g, c.d[3], c.dim and c.params[0 .. c.nparams). One thread walks
+ * the ghost layers of a transverse point of one face outward (layer 1 first),
+ * transverse points and the two faces of an axis run in parallel, the axes
+ * one after another; a fill writes only the ghost cell (and its face B) it is
+ * called for. Compiled without FMA contraction, with IEEE division and square
+ * root, like the library's FP64 kernels. A failed compile returns
+ * DRAGON_GPU_EINVAL with NVRTC's log as the error message; without NVRTC,
+ * DRAGON_GPU_ECUDA. A fill may be bound to any number of grids. */
+typedef struct dragon_user_fill dragon_user_fill;
+int dragon_gpu_user_fill_create(const char* source, const char* function, dragon_user_fill** out);
+int dragon_gpu_user_fill_destroy(dragon_user_fill* f);
+/* NVRTC's log of the compile (warnings), "" if none. */
+const char* dragon_gpu_user_fill_log(const dragon_user_fill* f);
+/* Binds fill f to entry `entry` (an index into the list last passed to
+ * dragon_gpu_set_boundary, whose type must be DRAGON_BC_USER): it fills the
+ * ghost cells of fill_faces (a face mask; the reference's Jet fills its jet
+ * face while its GhostFill faces mask is 0), with their corner ghosts when
+ * corners != 0, reading params (copied to the device). The grid runs it at
+ * the entry's place in BoundaryList::apply order (BoundaryList.hpp:79-93) in
+ * every ghost fill and inside the device advance loop, with no host
+ * round trip. dragon_gpu_set_boundary drops the bindings. */
+int dragon_gpu_set_user_fill(dragon_grid* g, int entry, dragon_user_fill* f, int fill_faces, int corners,
+                             const double* params, int nparams);
 /* Grid::initialize_B_fields (MHD/B_fields.cpp:117-149) */
 int dragon_gpu_initialize_B_fields(dragon_grid* g);
 

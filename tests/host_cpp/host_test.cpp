@@ -144,7 +144,7 @@ static int run_case(const std::string& name, const std::string& dir) {
         grid.advance(0.2);  // implicit Outflow on every face
         std::printf("steps %d last_dt %.17g\n", grid.last_advance().steps, grid.last_advance().last_dt);
         for (int i = -g; i < n + g; i++) put_state(out, grid[i]);
-    } else if (name == "kh2d" || name == "kh2d_walls" || name == "kh2d_inflow") {
+    } else if (name == "kh2d" || name == "kh2d_walls" || name == "kh2d_inflow" || name == "kh2d_device_inflow") {
         const int nx = 64, ny = 48, g = 2;
         cfg.riemann = 2;
         cfg.limiter = 2;  // van Leer
@@ -157,12 +157,22 @@ static int run_case(const std::string& name, const std::string& dir) {
         } else if (name == "kh2d_walls") {
             grid.boundary = Boundary::Reflective("X") + Boundary::Periodic("YZ");
             grid.advance(0.02);
-        } else {
+        } else if (name == "kh2d_inflow") {
             PrimitiveState jet;
             jet.rho = 3.0;
             jet.p = 2.5;
             jet.v = vec3(0.8, 0.0, 0.0);
             grid.boundary = Boundary::Periodic("Y") + Inflow(jet);
+            grid.advance(0.02);
+        } else {
+            // the same inflow as a fill compiled for the device
+            const char* src = R"(
+__device__ void inflow(const dragon_fill_ctx& c, int i, int j, int k) {
+    for (int f = 0; f < c.nparams; f++) c.set(f, i, j, k, c.params[f]);
+})";
+            grid.boundary = Boundary::Periodic("Y") +
+                            Boundary::DeviceFill(src, "inflow", Boundary::X_negative, Boundary::X_negative,
+                                                 {3.0, 2.5, 0.8, 0.0, 0.0});
             grid.advance(0.02);
         }
         for (int i = -g; i < nx + g; i++)

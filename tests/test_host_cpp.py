@@ -85,7 +85,7 @@ def test_cpp_sod_1d_to_t02(host_test):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["kh2d", "kh2d_walls", "kh2d_inflow"])
+@pytest.mark.parametrize("case", ["kh2d", "kh2d_walls", "kh2d_inflow", "kh2d_device_inflow"])
 def test_cpp_kh_2d(host_test, case):
     if not cuda_ok():
         pytest.fail("CUDA device required")
