@@ -240,6 +240,20 @@ __device__ __forceinline__ int prologue_bookkeeping(StepCtl* ctl, const Prologue
     return 0;
 }
 
+// Whether the bookkeeping ends the advance, computed from the control block
+// without writing it (the same operations as prologue_bookkeeping): a prior
+// step's dt is taken off the interval first, so remaining - t1 is the value
+// the bookkeeping compares.
+__device__ __forceinline__ int bookkeeping_done(const StepCtl* ctl, const PrologueArgs& pa) {
+    const volatile StepCtl* c = ctl;
+    if (c->done) return 1;
+    if (!pa.bookkeeping) return 0;
+    const bool prev = c->have_prev != 0;
+    const double rem = prev ? c->remaining - c->t1 : c->remaining;
+    const int steps = prev ? c->steps_done + 1 : c->steps_done;
+    return (!(rem > pa.tol) || (c->max_steps > 0 && steps >= c->max_steps)) ? 1 : 0;
+}
+
 // Max CFL signal speed over the one-cell ghost ring (CFL.cpp:91,110,125:
 // ng = min(1, ghosts)) of a 2D / 3D grid, ring points t0, t0 + stride, ...
 template <bool MHD>
@@ -417,21 +431,36 @@ __global__ void __launch_bounds__(256) k_prologue_coop(Geo G, Geo FG, double* __
                                                       const BCEntry* __restrict__ bcs, StepCtl* ctl, PrologueArgs pa) {
     __shared__ int s_skip;
     __shared__ double s_red[32];
-    // A failure recorded by an earlier launch of this advance (a flux, state or
-    // barrier failure of the batch the host has not read yet): every CTA
-    // returns before the first barrier. Nothing in this launch writes err
-    // before that barrier (bookkeeping only writes done), so all CTAs agree.
-    if (threadIdx.x == 0) s_skip = *(const volatile int*)&ctl->err | (int)(blockIdx.x == pa.stall_cta);
-    __syncthreads();
-    if (s_skip) return;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        ctl->ring_bits = 0ull;
-        prologue_bookkeeping(ctl, pa);
+    // Every CTA reads the control block and decides alone: a failure recorded
+    // by an earlier launch of this advance (a flux, state or barrier failure
+    // of the batch the host has not read yet) or an advance the bookkeeping
+    // ends (bookkeeping_done) returns before any barrier. Nothing writes the
+    // control block until every CTA has read it, so all CTAs decide alike:
+    // CTA 0 writes the bookkeeping after the first grid barrier, or, when the
+    // advance is done, the last CTA to decide writes it.
+    if (threadIdx.x == 0) {
+        s_skip = *(const volatile int*)&ctl->err ? 1 : bookkeeping_done(ctl, pa) ? 2 : 0;
+        if (blockIdx.x == pa.stall_cta) s_skip = 1;
     }
-    if (!grid_barrier(ctl)) return;
-    if (threadIdx.x == 0) s_skip = *(const volatile int*)&ctl->err | *(const volatile int*)&ctl->done;
     __syncthreads();
-    if (s_skip) return;
+    if (s_skip == 1) return;
+    if (s_skip == 2) {
+        if (threadIdx.x == 0) {
+            __threadfence();
+            if (atomicAdd(&ctl->bar_arrive, 1u) == gridDim.x - 1) {
+                atomicExch(&ctl->bar_arrive, 0u);
+                prologue_bookkeeping(ctl, pa);
+            }
+        }
+        return;
+    }
+    const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+    if (lead) ctl->ring_bits = 0ull;
+    bool booked = false;
+    auto book = [&] {
+        if (lead && !booked) prologue_bookkeeping(ctl, pa);
+        booked = true;
+    };
     const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long nt = (long long)gridDim.x * blockDim.x;
     // An entry fills its cells axis by axis, then its faces axis by axis. Cell
@@ -447,16 +476,19 @@ __global__ void __launch_bounds__(256) k_prologue_coop(Geo G, Geo FG, double* __
                     if (G.dim >= 2) bc_faces_axis(FG, G.n, B, be, a, tid, nt);
                 }
                 if (!grid_barrier(ctl)) return;
+                book();
             }
         }
     }
+    // The host launches this kernel only with a ghost-fill stage, so the
+    // bookkeeping was written after the first stage's barrier.
     if (!pa.compute_dt) return;
     double m = ring_speed_max<MHD>(G, w, pa, tid, nt);
     m = block_max(m, s_red);
     if (threadIdx.x == 0) atomic_max_speed(&ctl->ring_bits, m);
     if (!grid_barrier(ctl)) return;
-    if (blockIdx.x == 0 && threadIdx.x == 0)
-        prologue_set_dt(G, ctl, pa, __longlong_as_double((long long)*(volatile unsigned long long*)&ctl->ring_bits));
+    book();
+    if (lead) prologue_set_dt(G, ctl, pa, __longlong_as_double((long long)*(volatile unsigned long long*)&ctl->ring_bits));
 }
 
 // One ghost-fill pass (entry, axis; cells or faces) spread over a whole grid,
