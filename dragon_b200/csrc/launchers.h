@@ -22,7 +22,7 @@ int launch_step1d_mixed(int solver, const Geo& G, const double* win, double* wou
 // The fused 2D hydro steps load each tile with one TMA copy through `map`, a
 // tensor map of the input buffer with the box step2d_tile_box gives (columns,
 // rows, fields) for the FP64 (mixed = 0) or the mixed kernel.
-constexpr int kMx2dTI = 16;
+constexpr int kMx2dTI = 16, kMx2dTJ = 32;
 int step2d_tile_box(int mixed, int box[3]);
 int launch_step2d_hydro(int solver, const Geo& G, const double* win, double* wout, StepCtl* ctl, const StepArgs& sa,
                         const CUtensorMap* map, cudaStream_t st);

@@ -94,7 +94,7 @@ __device__ __forceinline__ void copy_ghosts_2d(const Geo& G, const double* __res
 }
 
 template <int SOLVER, int TI, int TJ, int NT>
-__global__ void __launch_bounds__(NT, 2)
+__global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2)
 k_step2d_hydro(Geo G, const double* __restrict__ win, double* __restrict__ wout, StepCtl* ctl, StepArgs sa,
                const __grid_constant__ CUtensorMap tile_map) {
     extern __shared__ __align__(128) unsigned char smem_raw[];

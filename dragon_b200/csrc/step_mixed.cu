@@ -71,7 +71,7 @@ __device__ __forceinline__ double block_min(double v, double* scratch) {
 // Three CTAs per SM (80 registers, 72.7 KB shared memory each): measured 14 %
 // faster than two CTAs at 110 registers on a 2048^2 shear layer, same results.
 template <int SOLVER, int TI, int TJ, int NT>
-__global__ void __launch_bounds__(NT, 3)
+__global__ void __launch_bounds__(NT, NT >= 384 ? 2 : 3)
 k_step2d_hydro_mixed(Geo G, const double* __restrict__ win, double* __restrict__ wout, StepCtl* ctl, StepArgs sa,
                      const __grid_constant__ CUtensorMap tile_map) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -267,7 +267,7 @@ k_step2d_hydro_mixed(Geo G, const double* __restrict__ win, double* __restrict__
     }
 }
 
-constexpr int kMxTI = kMx2dTI, kMxTJ = 32, kMxNT = 256;
+constexpr int kMxTI = kMx2dTI, kMxTJ = kMx2dTJ, kMxNT = 256;
 
 template <int SOLVER>
 static int launch_mixed_t(const Geo& G, const double* win, double* wout, StepCtl* ctl, const StepArgs& sa,
