@@ -99,23 +99,25 @@ __device__ __forceinline__ double cfl_speed_1d_mx(const Prim<double>& W64) {
 }
 
 // Primitive state from FP32 momenta / density and an FP64 total energy,
-// pressure recovered in FP64. The velocities multiply by the correctly rounded
-// reciprocal of the density (__frcp_rn): the mixed translation units are
-// built with approximate FP32 division, whose rounding errors do not cancel
-// over many steps. On the 1024^2 shear layer they carried the transverse
-// velocity's relative L1 after 2000 steps to 3.4e-4; the rounded reciprocals
-// here and in the HLLC star state below bring it to 9.2e-5 for about 5 % of
-// the step's time (IEEE division throughout: 7.2e-5 for 27 %).
+// pressure recovered in FP64. The velocities are the momenta times the FP64
+// reciprocal of the density that the pressure recovery computes anyway,
+// rounded once to FP32: the mixed translation units are built with
+// approximate FP32 division, whose rounding errors do not cancel over many
+// steps. On the 1024^2 shear layer they carried the transverse velocity's
+// relative L1 after 2000 steps to 3.4e-4; these velocities and the rounded
+// reciprocals of the HLLC star state below bring it to 7.5e-5 (IEEE FP32
+// division throughout: 7.2e-5) and 9.9e-6 after 25 steps, with a step 1 %
+// faster than with approximate division.
 template <bool MHD>
 __device__ __forceinline__ Prim<float> prim_from(const Cons<float>& u, double E64) {
     Prim<float> w;
     w.rho = u.rho;
-    const float ir = __frcp_rn(u.rho);
-    w.vx = u.mx * ir;
-    w.vy = u.my * ir;
-    w.vz = u.mz * ir;
     const double rho = u.rho, mx = u.mx, my = u.my, mz = u.mz;
-    double Eth = E64 - (mx * mx + my * my + mz * mz) * (0.5 * __drcp_rn(rho));
+    const double inv = __drcp_rn(rho);
+    w.vx = (float)(mx * inv);
+    w.vy = (float)(my * inv);
+    w.vz = (float)(mz * inv);
+    double Eth = E64 - (mx * mx + my * my + mz * mz) * (0.5 * inv);
     if constexpr (MHD) {
         const double bx = u.Bx, by = u.By, bz = u.Bz;
         Eth -= (bx * bx + by * by + bz * bz) * k1_8pi;
@@ -246,12 +248,12 @@ __device__ __forceinline__ double energy64_off(const Prim<float>& w, double ref)
 __device__ __forceinline__ Prim<float> prim_from_off(const Cons<float>& u, double E64, double ref, bool* phys) {
     Prim<float> w;
     w.rho = u.rho;
-    const float ir = __frcp_rn(u.rho);
-    w.vx = u.mx * ir;
-    w.vy = u.my * ir;
-    w.vz = u.mz * ir;
     const double rho = u.rho, mx = u.mx, my = u.my, mz = u.mz;
-    const double p = kGm1 * (E64 - (mx * mx + my * my + mz * mz) * (0.5 * __drcp_rn(rho)));
+    const double inv = __drcp_rn(rho);
+    w.vx = (float)(mx * inv);
+    w.vy = (float)(my * inv);
+    w.vz = (float)(mz * inv);
+    const double p = kGm1 * (E64 - (mx * mx + my * my + mz * mz) * (0.5 * inv));
     w.p = (float)(p - ref);
     w.Bx = w.By = w.Bz = 0.f;
     if (phys)

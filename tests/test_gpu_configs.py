@@ -175,7 +175,7 @@ def test_mixed_shear_layer_1024_2000_steps_vs_fp64(shear_layer_2000):
     assert np.all(l1[[0, 1, 2, 4]] <= TOL_MIXED), dict(zip(["rho", "p", "vx", "vy", "vz"], l1))
 
 
-@pytest.mark.xfail(strict=True, reason="vy, the seeded perturbation, ends at ~9e-5 relative L1 after 2000 steps "
+@pytest.mark.xfail(strict=True, reason="vy, the seeded perturbation, ends at ~7.5e-5 relative L1 after 2000 steps "
                    "(growing with the step count; 7e-5 with IEEE FP32 division throughout) while rho, p and vx "
                    "stay at ~2e-7")
 def test_mixed_shear_layer_vy_1024_2000_steps_vs_fp64(shear_layer_2000):
