@@ -22,7 +22,7 @@ ORDER_PHASE_MAJOR, ORDER_1D_FIRST, ORDER_LARGEST_FIRST, ORDER_WAVEFRONT = 0, 1, 
 
 @dataclass
 class Tuning:
-    tile_1d: int = 256
+    tile_1d: int = 254
     ctas_per_sm: int = 0     # 0: as many as fit
     order: int = ORDER_PHASE_MAJOR
     graph_steps: int = 32

@@ -57,19 +57,21 @@ __global__ void k_batch_summary(const BatchInst* __restrict__ insts, int n, Summ
     out[i] = Summary{ldv(&c->err), ldv(&c->done), ldv(&c->steps_done), ldv(&c->cur)};
 }
 
-// Built solver combinations: 1D hydro {HLLC, exact} x 2D MHD {HLLD} x tile {128, 256}.
+// Built solver combinations: 1D hydro {HLLC, exact} x 2D MHD {HLLD} x tile
+// {126, 254} cells (the tile's half states, TS + 2 cells, fill 128 or 256
+// threads of the CTA's round).
 StepKernel pick_kernel(int s1d, int tile) {
     const bool exact = s1d == RS_EXACT;
-    if (tile == 128)
-        return exact ? k_batch_step<false, RS_EXACT, RS_HLLD, 128> : k_batch_step<false, RS_HLLC, RS_HLLD, 128>;
-    return exact ? k_batch_step<false, RS_EXACT, RS_HLLD, 256> : k_batch_step<false, RS_HLLC, RS_HLLD, 256>;
+    if (tile == 126)
+        return exact ? k_batch_step<false, RS_EXACT, RS_HLLD, 126> : k_batch_step<false, RS_HLLC, RS_HLLD, 126>;
+    return exact ? k_batch_step<false, RS_EXACT, RS_HLLD, 254> : k_batch_step<false, RS_HLLC, RS_HLLD, 254>;
 }
 
 }  // namespace
 
 struct dragon_batch {
     std::vector<dragon_grid*> members;
-    dragon_batch_tuning tune{256, 0, 0, 32, 8, 1};
+    dragon_batch_tuning tune{254, 0, 0, 32, 8, 1};
     int s1d = -1;
     int prec = -1;  // the members' precision (0 FP64, 1 mixed)
     cudaStream_t stream = nullptr;
@@ -414,7 +416,7 @@ int dragon_gpu_batch_size(const dragon_batch* b) { return b ? (int)b->members.si
 
 int dragon_gpu_batch_set_tuning(dragon_batch* b, const dragon_batch_tuning* t) {
     if (!b || !t) return fail(DRAGON_GPU_EINVAL, "null argument");
-    if ((t->tile_1d != 128 && t->tile_1d != 256) || t->ctas_per_sm < 0 || t->ctas_per_sm > 8 || t->order < 0 ||
+    if ((t->tile_1d != 126 && t->tile_1d != 254) || t->ctas_per_sm < 0 || t->ctas_per_sm > 8 || t->order < 0 ||
         t->order > 3 || t->graph_steps < 1 || t->graph_steps > 1024 ||
         !(t->mhd_tiles == 0 || t->mhd_tiles == 1 || t->mhd_tiles == 2 || t->mhd_tiles == 4 || t->mhd_tiles == 8) ||
         t->wave < 0 || t->wave > 64)
@@ -506,7 +508,7 @@ int dragon_gpu_batch_autotune(dragon_batch* b, int steps, dragon_batch_tuning* b
     };
     // launch shape and queue order with one MHD tile per item, then the MHD
     // tiles per item for the best of those, then the wavefront order
-    for (int tile : {128, 256})
+    for (int tile : {126, 254})
         for (int per_sm : {1, 2, 4, 8})
             for (int order : {0, 1, 2})
                 if (!rc) rc = trial(dragon_batch_tuning{tile, per_sm, order, steps, 1, 1});

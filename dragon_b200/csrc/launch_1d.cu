@@ -4,12 +4,21 @@
 
 namespace dgpu {
 
-constexpr int k1dTS = 128;
+// Tiles of TS = NT - 2 cells on NT threads: the half states (TS + 2 cells)
+// and the faces (TS + 1) of a tile fit one round of the CTA's threads, where
+// tiles of 128 cells on 128 threads ran each of those phases in two rounds,
+// the second holding one or two items. Hydro: 254 cells on 256 threads; MHD
+// (eight fields in static shared memory, at most 48 KB): 126 on 128.
+template <bool MHD>
+struct Tile1D {
+    static constexpr int NT = MHD ? 128 : 256, TS = NT - 2;
+};
 
 template <bool MHD, int S>
 static int go(const Geo& G, const double* win, double* wout, StepCtl* ctl, const StepArgs& sa, cudaStream_t st) {
     const int np = G.n[0] + 2 * G.g;
-    k_step1d<MHD, S, k1dTS><<<(np + k1dTS - 1) / k1dTS, k1dTS, 0, st>>>(G, win, wout, ctl, sa);
+    constexpr int TS = Tile1D<MHD>::TS, NT = Tile1D<MHD>::NT;
+    k_step1d<MHD, S, TS, NT><<<(np + TS - 1) / TS, NT, 0, st>>>(G, win, wout, ctl, sa);
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 

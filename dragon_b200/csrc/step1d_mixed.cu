@@ -8,8 +8,8 @@ namespace dgpu {
 
 namespace {
 
-template <int SOLVER, int TS>
-__global__ void __launch_bounds__(TS)
+template <int SOLVER, int TS, int NT>
+__global__ void __launch_bounds__(NT)
 k_step1d_mx(Geo G, const double* __restrict__ win, double* __restrict__ wout, StepCtl* ctl, StepArgs sa) {
     step1d_tile_mx<SOLVER, TS>(G, win, wout, ctl, sa, blockIdx.x);
 }
@@ -17,7 +17,8 @@ k_step1d_mx(Geo G, const double* __restrict__ win, double* __restrict__ wout, St
 template <int S>
 int go(const Geo& G, const double* win, double* wout, StepCtl* ctl, const StepArgs& sa, cudaStream_t st) {
     const int np = G.n[0] + 2 * G.g;
-    k_step1d_mx<S, kMx1dTile><<<(np + kMx1dTile - 1) / kMx1dTile, kMx1dTile, 0, st>>>(G, win, wout, ctl, sa);
+    k_step1d_mx<S, kMx1dTile, kMx1dThreads><<<(np + kMx1dTile - 1) / kMx1dTile, kMx1dThreads, 0, st>>>(G, win, wout,
+                                                                                                    ctl, sa);
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 

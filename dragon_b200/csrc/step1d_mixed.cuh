@@ -22,8 +22,10 @@ namespace dgpu {
 
 // Cells per mixed 1D tile, in the single-grid sweep and in a batch alike: the
 // pressure reference is a per-tile quantity, so the tiling is part of the
-// arithmetic.
-constexpr int kMx1dTile = 128;
+// arithmetic. 254 cells: the half states (256 cells) and faces (255) of a
+// tile fit one round of a 256-thread CTA (the single-grid launch's threads,
+// kMx1dThreads, and the batched step's).
+constexpr int kMx1dTile = 254, kMx1dThreads = 256;
 
 // Block-wide minimum of a per-thread value (a 1D block); every thread gets it.
 __device__ __forceinline__ double tile_min_1d(double v, double* scratch) {

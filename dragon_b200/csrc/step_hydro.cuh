@@ -292,8 +292,9 @@ k_step2d_hydro(Geo G, const double* __restrict__ win, double* __restrict__ wout,
 // state and the last face the raw rightmost ghost as its right state; every
 // cell but the two outermost is updated, and cell n+2g-2 gets the reference's
 // second zero-flux round trip (Splitting.cpp:93-94). All cells are committed.
-// One tile of TS cells (cells tile*TS ...); TS threads. k_step1d runs one
-// tile per CTA, the batched step runs tiles as work items.
+// One tile of TS cells (cells tile*TS ...), any number of threads (the
+// phases stride by blockDim.x). k_step1d runs one tile per CTA, the batched
+// step runs tiles as work items.
 template <bool MHD, int SOLVER, int TS>
 __device__ __forceinline__ void step1d_tile(const Geo& G, const double* __restrict__ win, double* __restrict__ wout,
                                             StepCtl* ctl, const StepArgs& sa, int tile) {
@@ -400,8 +401,8 @@ __device__ __forceinline__ void step1d_tile(const Geo& G, const double* __restri
     if (first_order) atomicAdd(&ctl->muscl_first_order, (unsigned long long)first_order);
 }
 
-template <bool MHD, int SOLVER, int TS>
-__global__ void __launch_bounds__(TS)
+template <bool MHD, int SOLVER, int TS, int NT>
+__global__ void __launch_bounds__(NT)
 k_step1d(Geo G, const double* __restrict__ win, double* __restrict__ wout, StepCtl* ctl, StepArgs sa) {
     step1d_tile<MHD, SOLVER, TS>(G, win, wout, ctl, sa, blockIdx.x);
 }

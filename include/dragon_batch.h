@@ -34,7 +34,7 @@ typedef struct dragon_batch dragon_batch;
 /* Launch shape of the batched step, chosen by dragon_gpu_batch_autotune or
  * set by the caller. */
 typedef struct dragon_batch_tuning {
-    int tile_1d;      /* cells per 1D work item: 128 or 256 (FP64 batches; mixed: always 128) */
+    int tile_1d;      /* cells per 1D work item: 126 or 254 (FP64 batches; mixed: always 254) */
     int ctas_per_sm;  /* resident CTAs of the persistent kernel per SM (1..8, capped by occupancy) */
     int order;        /* queue order: 0 phase-major (all grids' phase k before phase k+1, 1D tiles after
                          the first MHD phase), 1 1D grids first, 2 largest grids first within each phase,

@@ -59,9 +59,9 @@ def assert_same(a, b):
             np.testing.assert_array_equal(b1, b2)
 
 
-@pytest.mark.parametrize("tile,order,per_sm,group,wave", [(256, 0, 0, 1, 1), (128, 1, 1, 1, 1), (256, 2, 2, 1, 1),
-                                                          (256, 0, 0, 2, 1), (128, 2, 1, 4, 1), (256, 1, 2, 8, 1),
-                                                          (256, 3, 2, 8, 1), (128, 3, 0, 2, 3)])
+@pytest.mark.parametrize("tile,order,per_sm,group,wave", [(254, 0, 0, 1, 1), (126, 1, 1, 1, 1), (254, 2, 2, 1, 1),
+                                                          (254, 0, 0, 2, 1), (126, 2, 1, 4, 1), (254, 1, 2, 8, 1),
+                                                          (254, 3, 2, 8, 1), (126, 3, 0, 2, 3)])
 def test_batch_matches_single_grid_advance(workload, tile, order, per_sm, group, wave):
     one, two = workload
     steps = 9
@@ -98,7 +98,7 @@ def test_autotune_keeps_states(workload):
     before = states(grids)
     b = batch.Batch(grids)
     t, ms = b.autotune(2)
-    assert ms > 0 and t.tile_1d in (128, 256) and t.order in (0, 1, 2, 3)
+    assert ms > 0 and t.tile_1d in (126, 254) and t.order in (0, 1, 2, 3)
     assert_same(states(grids), before)
     ref = make_grids(one, two)
     for G in ref:
@@ -120,7 +120,7 @@ TOL_MIXED = 1e-5
 TOL_MIXED_BATCH_MHD = 1e-6  # relative L1, mixed batch vs single-grid mixed, 9 steps
 
 
-@pytest.mark.parametrize("tile,order,per_sm,group,wave", [(256, 0, 0, 1, 1), (128, 2, 1, 8, 1), (256, 3, 2, 8, 2)])
+@pytest.mark.parametrize("tile,order,per_sm,group,wave", [(254, 0, 0, 1, 1), (126, 2, 1, 8, 1), (254, 3, 2, 8, 2)])
 def test_mixed_batch_matches_single_grid_mixed_advance(workload, tile, order, per_sm, group, wave):
     one, two = workload
     steps = 9
