@@ -23,11 +23,14 @@ __device__ __forceinline__ bool cta_should_skip_sweep(const StepCtl* ctl, int* s
     return *s_flag != 0;
 }
 
+// Tile shapes on 256 threads: a tile's half states (TL x (TC + 2)) fill one
+// round of threads and its faces (TL x (TC + 1)) nearly one, where 8 x 32 and
+// 32 x 8 tiles ran both phases in two rounds (272 to 320 items).
 template <int DIM, int AX>
 struct SweepShape {
     static constexpr bool kPosFast = AX == DIM - 1;  // the swept axis is the contiguous one
     static constexpr int TL = kPosFast ? 8 : 32;     // lines per tile
-    static constexpr int TC = kPosFast ? 32 : 8;     // cells per line per tile
+    static constexpr int TC = kPosFast ? 30 : 6;     // cells per line per tile
     static constexpr size_t kSmem = sizeof(double) * 5 * TL * ((TC + 4) + 2 * (TC + 2) + (TC + 1));
 };
 
