@@ -169,7 +169,9 @@ const char* dragon_gpu_user_fill_log(const dragon_user_fill* f);
  * corners != 0, reading params (copied to the device). The grid runs it at
  * the entry's place in BoundaryList::apply order (BoundaryList.hpp:79-93) in
  * every ghost fill and inside the device advance loop, with no host
- * round trip. dragon_gpu_set_boundary drops the bindings. */
+ * round trip. dragon_gpu_set_boundary drops the bindings. f must stay alive
+ * while it is bound: destroy it only after the grids it is bound to are
+ * destroyed or have had their boundary list set again. */
 int dragon_gpu_set_user_fill(dragon_grid* g, int entry, dragon_user_fill* f, int fill_faces, int corners,
                              const double* params, int nparams);
 /* Grid::initialize_B_fields (MHD/B_fields.cpp:117-149) */
