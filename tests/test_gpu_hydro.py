@@ -81,7 +81,7 @@ def ref_advance_log(R, interval, tol=1e-14):
 
 # ---------------------------------------------------------------------------
 def test_sod_1d_to_t02_bitwise_and_dt_sequence():
-    """BASELINE config: 512 cells, HLLC, minmod, outflow, CFL 0.3, t = 0.2."""
+    """The 1D Sod configuration: 512 cells, HLLC, minmod, outflow, CFL 0.3, t = 0.2."""
     w0, dx = problems.sod_1d(512, ghosts=2)
     G, R = make_pair(1, (512,), (dx,), w0, dg.Outflow(), riemann=dg.RIEMANN_HLLC, limiter=dg.LIMITER_MINMOD)
     dts = ref_advance_log(R, 0.2)
