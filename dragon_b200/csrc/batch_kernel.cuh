@@ -173,8 +173,8 @@ __device__ __forceinline__ void run_item(const BatchInst& I, const WorkItem& wi,
 
 // Resident CTAs per SM the kernel is built for: two for FP64 (128 registers);
 // three for the lighter mixed bodies (85 registers, some spilled), which on the
-// C5 batch ran 10 % faster than two (1.69e9 against 1.54e9 cell-updates/s) and
-// faster than four (1.55e9).
+// batch of 2048 1D hydro and 256 2D MHD grids ran 10 % faster than two (1.69e9
+// against 1.54e9 cell-updates/s) and faster than four (1.55e9).
 template <bool MIXED>
 constexpr int kBatchCtasPerSm = MIXED ? 3 : 2;
 

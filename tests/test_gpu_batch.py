@@ -145,7 +145,7 @@ def test_mixed_batch_matches_single_grid_mixed_advance(workload, tile, order, pe
 
 
 def test_mixed_batch_within_the_mixed_bar_of_fp64():
-    """Members of the C5 batch's sizes (1D N in [64, 1024], MHD blasts 64^2
+    """Members of the 2048 1D + 256 2D MHD batch's sizes (1D N in [64, 1024], MHD blasts 64^2
     and 128^2): every field of every member within the mixed bar of its FP64
     batch state after 20 steps."""
     one, two = problems.batch_instances(n1d=16, n2d=3, seed=4, sizes_1d=(64, 1024), sizes_2d=(64, 128))
