@@ -86,6 +86,10 @@ struct dragon_batch {
     cudaGraphExec_t gexec = nullptr;
     bool dirty = true;
     int grid_ctas = 0;
+    // a mixed batch's 2D MHD members (by increasing fuse_first) and the CTAs of their fused launch
+    int* d_fmembers = nullptr;
+    int n_fmembers = 0;
+    int fuse_ctas = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
@@ -96,8 +100,11 @@ void release_device(dragon_batch* b) {
     if (b->graph) cudaGraphDestroy(b->graph);
     b->gexec = nullptr;
     b->graph = nullptr;
-    for (void* p : {(void*)b->d_insts, (void*)b->d_items, (void*)b->d_ctr, (void*)b->d_sum})
+    for (void* p : {(void*)b->d_insts, (void*)b->d_items, (void*)b->d_ctr, (void*)b->d_sum, (void*)b->d_fmembers})
         if (p) cudaFree(p);
+    b->d_fmembers = nullptr;
+    b->n_fmembers = 0;
+    b->fuse_ctas = 0;
     if (b->h_sum) cudaFreeHost(b->h_sum);
     b->d_insts = nullptr;
     b->d_items = nullptr;
@@ -146,6 +153,16 @@ BatchInst make_inst(dragon_grid* h, int tile, int group, bool mixed) {
     }
     const int nx = h->n[0], ny = h->n[1];
     I.frame = mhd2d_frame_points(h->cg.n[0], h->cg.n[1], h->cg.g);
+    if (mixed) {
+        // the fused step, in the batch's fused launch: segments of up to 128
+        // rows (a multiple of the 8 rows an iteration advances; each segment
+        // refills the rings once)
+        I.last_phase = 0;
+        I.fuse_strips = tiles_along(ny, kFuseTJ);
+        I.fuse_seg_rows = std::min(128, tiles_along(nx, kFuseR) * kFuseR);
+        I.fuse_ctas = I.fuse_strips * tiles_along(nx, I.fuse_seg_rows);
+        return I;
+    }
     I.last_phase = 8;
     I.ntiles[1] = (int)std::max<long long>(1, (I.frame + kCopyChunk - 1) / kCopyChunk);
     I.ntj[1] = 1;
@@ -220,16 +237,34 @@ int build(dragon_batch* b) {
     insts.reserve(n);
     const bool mixed = b->prec == 1;
     for (dragon_grid* h : b->members) insts.push_back(make_inst(h, b->tune.tile_1d, b->tune.mhd_tiles, mixed));
+    std::vector<int> fmembers;  // a mixed batch's 2D MHD members, in the fused launch's CTA order
+    if (mixed) {
+        int first = 0;
+        for (int i = 0; i < n; i++) {
+            if (insts[i].kind != KMHD2D) continue;
+            insts[i].fuse_first = first;
+            first += insts[i].fuse_ctas;
+            fmembers.push_back(i);
+        }
+        b->fuse_ctas = first;
+        b->n_fmembers = (int)fmembers.size();
+    }
     const std::vector<WorkItem> q = make_queue(insts, b->tune.order, std::max(1, b->tune.wave));
     b->nitems = (int)q.size();
     b->ctr_words = kCtrDone + (size_t)kPhases * n;
     CKB(cudaMalloc(&b->d_insts, sizeof(BatchInst) * n));
-    CKB(cudaMalloc(&b->d_items, sizeof(WorkItem) * q.size()));
+    CKB(cudaMalloc(&b->d_items, sizeof(WorkItem) * std::max<size_t>(1, q.size())));
     CKB(cudaMalloc(&b->d_ctr, sizeof(unsigned) * b->ctr_words));
     CKB(cudaMalloc(&b->d_sum, sizeof(Summary) * n));
     CKB(cudaMallocHost(&b->h_sum, sizeof(Summary) * n));
     CKB(cudaMemcpyAsync(b->d_insts, insts.data(), sizeof(BatchInst) * n, cudaMemcpyHostToDevice, b->stream));
-    CKB(cudaMemcpyAsync(b->d_items, q.data(), sizeof(WorkItem) * q.size(), cudaMemcpyHostToDevice, b->stream));
+    if (!q.empty())
+        CKB(cudaMemcpyAsync(b->d_items, q.data(), sizeof(WorkItem) * q.size(), cudaMemcpyHostToDevice, b->stream));
+    if (!fmembers.empty()) {
+        CKB(cudaMalloc(&b->d_fmembers, sizeof(int) * fmembers.size()));
+        CKB(cudaMemcpyAsync(b->d_fmembers, fmembers.data(), sizeof(int) * fmembers.size(), cudaMemcpyHostToDevice,
+                            b->stream));
+    }
     CKB(cudaMemsetAsync(b->d_ctr, 0, sizeof(unsigned) * b->ctr_words, b->stream));
     CKB(cudaStreamSynchronize(b->stream));
 
@@ -246,7 +281,14 @@ int build(dragon_batch* b) {
     for (int k = 0; k < b->tune.graph_steps; k++) {
         cudaMemsetAsync(b->d_ctr + kCtrHead, 0, sizeof(unsigned) * (b->ctr_words - kCtrHead), b->stream);
         if (mixed) k_batch_prologue<<<std::min(n, sms * 8), kThreads, 0, b->stream>>>(b->d_insts, n, b->d_ctr);
-        kern<<<b->grid_ctas, kThreads, 0, b->stream>>>(b->d_insts, b->d_items, b->nitems, b->d_ctr);
+        if (b->nitems > 0) kern<<<b->grid_ctas, kThreads, 0, b->stream>>>(b->d_insts, b->d_items, b->nitems, b->d_ctr);
+        if (b->fuse_ctas > 0 &&
+            launch_fused_mhd(b->d_insts, b->d_fmembers, b->n_fmembers, b->fuse_ctas, b->d_ctr, b->stream)) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(b->stream, &g);
+            if (g) cudaGraphDestroy(g);
+            return fail(DRAGON_GPU_ECUDA, "fused MHD launch of the batch failed");
+        }
     }
     k_batch_summary<<<(n + 255) / 256, 256, 0, b->stream>>>(b->d_insts, n, b->d_sum);
     cudaMemcpyAsync(b->h_sum, b->d_sum, sizeof(Summary) * n, cudaMemcpyDeviceToHost, b->stream);

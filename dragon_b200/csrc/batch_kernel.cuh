@@ -18,7 +18,10 @@
 //   2D MHD       phase 1: copy of the ghost frame of the state and face B into
 //                the output buffers (mhd2d_copy_frame),
 //                phases 2-8: the seven phases of the single-grid step, one
-//                or more 32 x 8 cell tiles per item
+//                or more 32 x 8 cell tiles per item (FP64 batches; a mixed
+//                batch steps its 2D MHD members with the fused one-kernel
+//                step of step_mhd_fused.cuh in a launch of its own,
+//                k_batch_fused_mhd in batch_mixed.cu)
 // A CTA takes the next item from a global counter, waits until every item of
 // the member's previous phase has finished, runs it and counts it done. The
 // queue lists a member's phases in order, so every item a CTA can wait for was
@@ -36,6 +39,7 @@
 #include "step_hydro.cuh"
 #include "step_mhd.cuh"
 #include "step_mhd_mixed.cuh"
+#include "step_mhd_fused.cuh"
 
 namespace dgpu_batch {
 
@@ -63,6 +67,10 @@ struct BatchInst {
     StepArgs sa;
     PrologueArgs pa;
     long long frame;         // ghost-frame points copied by phase 1 (MHD, mhd2d_frame_points)
+    // a mixed batch's 2D MHD member runs the fused one-kernel step instead of
+    // phases 1-8: its strips, rows per segment, CTAs and first CTA in the
+    // batch's fused launch (k_batch_fused_mhd)
+    int fuse_strips, fuse_seg_rows, fuse_ctas, fuse_first;
 };
 
 struct WorkItem {
@@ -217,5 +225,10 @@ __global__ void __launch_bounds__(kThreads, kBatchCtasPerSm<MIXED>) k_batch_step
 
 // The mixed batch's step kernel for a 1D solver and tile size (batch_mixed.cu).
 StepKernel pick_kernel_mx(int s1d, int tile);
+
+// A mixed batch's fused 2D MHD launch (batch_mixed.cu): `ctas` CTAs over the
+// members listed in `members` (by increasing fuse_first).
+int launch_fused_mhd(const BatchInst* insts, const int* members, int nm, int ctas, unsigned* ctr, cudaStream_t st);
+size_t fused_mhd_smem();
 
 }  // namespace dgpu_batch

@@ -35,6 +35,15 @@
 
 namespace dgpu {
 
+// Strips of kFuseTJ columns marching kFuseR rows per iteration, kFuseNT threads.
+// Each phase's items per iteration (rows x its column window) against the
+// 256 threads: with 28 columns every phase fills its last round of threads
+// well (S2 504 and S5 472 solves: two rounds each; S3, S6, S7 one round),
+// where 32 columns left rounds of 24 to 56 items in five phases. Measured on
+// Orszag-Tang 1024^2: 0.432 ms per step against 0.496 ms with 32 columns
+// (24 columns: 0.518 ms; 6 rows x 32 columns: 0.462 ms).
+constexpr int kFuseTJ = 28, kFuseR = 8, kFuseNT = 256;
+
 template <int TJ, int R>
 struct FusedMhdSmem {
     static constexpr int KW = R + 2;  // rows of w (FP32) and its body E
@@ -135,25 +144,27 @@ __device__ __forceinline__ RowSpan span_of(int a, int se, int off, int first) {
 template <int R>
 constexpr int kFill = R * ((6 + R - 1) / R);
 
+// The step of one strip (columns from strip * TJ) and one segment (rows from
+// seg * seg_rows) of one grid, run by the calling CTA; `cta` of `ctas` is the
+// CTA's place among all CTAs stepping this grid (they share the ghost-frame
+// copy). CTA-uniform early returns only.
 template <int SOLVER, int TJ, int R, int NT>
-__global__ void __launch_bounds__(NT, 2) k_mhd2d_fused_mixed(Geo G, Geo FG, const double* __restrict__ w,
-                                                          double* __restrict__ wout, const double* __restrict__ B,
-                                                          double* __restrict__ Bout, StepCtl* ctl, StepArgs sa,
-                                                          int seg_rows) {
+__device__ __forceinline__ void mhd2d_fused_body(const Geo& G, const Geo& FG, const double* __restrict__ w,
+                                                 double* __restrict__ wout, const double* __restrict__ B,
+                                                 double* __restrict__ Bout, StepCtl* ctl, const StepArgs& sa,
+                                                 int seg_rows, int strip, int seg, long long cta, long long ctas,
+                                                 FusedMhdSmem<TJ, R>& S) {
     using S_t = FusedMhdSmem<TJ, R>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    S_t& S = *reinterpret_cast<S_t*>(smem_raw);
     if (mhd_skip(ctl, &S.skip)) return;
     // The ghost frame of the output buffers (every point the update does not
     // write) is copied from the inputs by all CTAs, before any returns early.
-    mhd2d_copy_frame(G, FG, w, wout, B, Bout, 0, mhd2d_frame_points(G.n[0], G.n[1], G.g),
-                     ((long long)blockIdx.y * gridDim.x + blockIdx.x) * NT + threadIdx.x,
-                     (long long)gridDim.x * gridDim.y * NT);
+    mhd2d_copy_frame(G, FG, w, wout, B, Bout, 0, mhd2d_frame_points(G.n[0], G.n[1], G.g), cta * NT + threadIdx.x,
+                     ctas * NT);
 
     const int nx = G.n[0], ny = G.n[1];
     const long long P = G.plane, FP = FG.plane;
-    const int j0 = blockIdx.x * TJ;
-    const int sb = blockIdx.y * seg_rows, se = min(sb + seg_rows, nx);
+    const int j0 = strip * TJ;
+    const int sb = seg * seg_rows, se = min(sb + seg_rows, nx);
     if (sb >= se) return;
     const double dt = *(const volatile double*)&ctl->t1;
     const double dt_dx = dt / sa.dx, dt_dy = dt / sa.dy, hdx = 0.5 * dt_dx, hdy = 0.5 * dt_dy;
@@ -414,6 +425,19 @@ __global__ void __launch_bounds__(NT, 2) k_mhd2d_fused_mixed(Geo G, Geo FG, cons
     warp_add_stat(&ctl->hlld_to_hlle, st.hlld_to_hlle);
     vmax = block_max(vmax, S.red);
     if (threadIdx.x == 0) atomic_max_speed(&ctl->vmax[sa.slot_out], vmax);
+}
+
+// The single-grid step: a strip per blockIdx.x, a segment per blockIdx.y.
+template <int SOLVER, int TJ, int R, int NT>
+__global__ void __launch_bounds__(NT, 2) k_mhd2d_fused_mixed(Geo G, Geo FG, const double* __restrict__ w,
+                                                          double* __restrict__ wout, const double* __restrict__ B,
+                                                          double* __restrict__ Bout, StepCtl* ctl, StepArgs sa,
+                                                          int seg_rows) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    auto& S = *reinterpret_cast<FusedMhdSmem<TJ, R>*>(smem_raw);
+    mhd2d_fused_body<SOLVER, TJ, R, NT>(G, FG, w, wout, B, Bout, ctl, sa, seg_rows, blockIdx.x, blockIdx.y,
+                                        (long long)blockIdx.y * gridDim.x + blockIdx.x,
+                                        (long long)gridDim.x * gridDim.y, S);
 }
 
 }  // namespace dgpu

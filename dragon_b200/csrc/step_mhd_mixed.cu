@@ -11,15 +11,6 @@ namespace dgpu {
 
 namespace {
 
-// Strips of kFuseTJ columns marching kFuseR rows per iteration, kFuseNT threads.
-// Each phase's items per iteration (rows x its column window) against the
-// 256 threads: with 28 columns every phase fills its last round of threads
-// well (S2 504 and S5 472 solves: two rounds each; S3, S6, S7 one round),
-// where 32 columns left rounds of 24 to 56 items in five phases. Measured on
-// Orszag-Tang 1024^2: 0.432 ms per step against 0.496 ms with 32 columns
-// (24 columns: 0.518 ms; 6 rows x 32 columns: 0.462 ms).
-constexpr int kFuseTJ = 28, kFuseR = 8, kFuseNT = 256;
-
 // One fused launch: a strip of columns per blockIdx.x, a segment of rows per
 // blockIdx.y. Segments are sized so the CTAs fill the device's resident
 // slots about once (each segment costs one ring-filling iteration extra).
