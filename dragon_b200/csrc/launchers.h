@@ -38,6 +38,9 @@ int launch_sweep(int solver, int axis, const Geo& G, const double* win, double* 
 int launch_init_body_fields(const Geo& G, const Geo& FG, double* w, const double* B, cudaStream_t s);
 int launch_step3d_hydro(int solver, const Geo& G, const double* w, double* wout, const Hydro3DScratch& S,
                         StepCtl* ctl, const StepArgs& sa, cudaStream_t st);
+// Mixed FP32/FP64 3D hydro step (step3d_mixed.cu): FP32 intermediates in S's planes.
+int launch_step3d_hydro_mixed(int solver, const Geo& G, const double* w, double* wout, const Hydro3DScratch& S,
+                              StepCtl* ctl, const StepArgs& sa, cudaStream_t st);
 int launch_step3d_mhd(int solver, const Geo& G, const Geo& FG, const double* w, double* wout, const double* B,
                       double* Bout, const Mhd3DScratch& S, StepCtl* ctl, const StepArgs& sa, cudaStream_t st);
 

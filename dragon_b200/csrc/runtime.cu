@@ -281,7 +281,9 @@ int launch_step(dragon_grid* h, int c) {
         rc = mixed ? launch_step2d_hydro_mixed(h->solver, h->cg, h->w[c], h->w[c ^ 1], h->ctl, sa, map, h->stream)
                    : launch_step2d_hydro(h->solver, h->cg, h->w[c], h->w[c ^ 1], h->ctl, sa, map, h->stream);
     } else {
-        rc = launch_step3d_hydro(h->solver, h->cg, h->w[c], h->w[c ^ 1], h->h3_s, h->ctl, sa, h->stream);
+        rc = (h->cfg.precision == 1)
+                 ? launch_step3d_hydro_mixed(h->solver, h->cg, h->w[c], h->w[c ^ 1], h->h3_s, h->ctl, sa, h->stream)
+                 : launch_step3d_hydro(h->solver, h->cg, h->w[c], h->w[c ^ 1], h->h3_s, h->ctl, sa, h->stream);
         nk = kHydro3DKernels;
     }
     if (rc) return fail(DRAGON_GPU_ECUDA, std::string("step launch failed: ") + cudaGetErrorString(cudaGetLastError()));
@@ -742,9 +744,13 @@ int dragon_gpu_grid_create(int dim, int nx, int ny, int nz, double dx, double dy
         delete h;
         return fail(DRAGON_GPU_EUNSUPPORTED, "the learned star-pressure guess is built for 3D hydro grids");
     }
-    if (h->cfg.precision != 0 && !(dim == 2 || (dim == 1 && !h->mhd))) {
+    if (h->cfg.precision != 0 && !(dim == 2 || !h->mhd)) {
         delete h;
-        return fail(DRAGON_GPU_EUNSUPPORTED, "the mixed-precision path is built for 1D hydro and 2D grids");
+        return fail(DRAGON_GPU_EUNSUPPORTED, "the mixed-precision path is built for hydro grids and 2D MHD grids");
+    }
+    if (h->cfg.precision != 0 && h->cfg.exact_guess == GUESS_LEARNED) {
+        delete h;
+        return fail(DRAGON_GPU_EUNSUPPORTED, "the learned star-pressure guess runs on the FP64 3D step");
     }
     h->cg = make_geo(dim, h->n, h->g);
     int nfc[3] = {h->n[0] + 1, h->n[1] + 1, h->n[2] + 1};

@@ -92,11 +92,66 @@ def test_mixed_sod_strong_shock_stays_physical():
     assert np.all(np.isfinite(G.w)) and np.all(l1 <= TOL_MIXED), l1
 
 
-def test_mixed_only_on_1d_hydro_and_2d_grids():
+def test_mixed_on_hydro_grids_and_2d_mhd_only():
     with pytest.raises(dg.grid._lib.DragonGPUError):
-        dg.Grid3D(4, 4, 4, 0.1, 0.1, 0.1, config=dg.Config(precision=dg.PREC_MIXED))
+        dg.Grid3D(4, 4, 4, 0.1, 0.1, 0.1, config=dg.Config(mhd=True, precision=dg.PREC_MIXED))
     with pytest.raises(dg.grid._lib.DragonGPUError):
         dg.Grid1D(16, 1 / 16, config=dg.Config(mhd=True, precision=dg.PREC_MIXED))
+    with pytest.raises(dg.grid._lib.DragonGPUError):
+        dg.Grid3D(4, 4, 4, 0.1, 0.1, 0.1, config=dg.Config(riemann=dg.RIEMANN_EXACT, exact_guess=dg.GUESS_LEARNED,
+                                                           precision=dg.PREC_MIXED))
+
+
+def _blast3d(n, seed, p_in=10.0):
+    w, d = problems.blast_3d(n, ghosts=2, p_in=p_in)
+    rng = np.random.default_rng(seed)
+    w[..., 2:5] = rng.uniform(-0.1, 0.1, w.shape[:-1] + (3,))
+    return w, d
+
+
+@pytest.mark.parametrize("riemann,limiter", [(dg.RIEMANN_HLLC, dg.LIMITER_MC), (dg.RIEMANN_HLL, dg.LIMITER_MINMOD),
+                                             (dg.RIEMANN_HLLE, dg.LIMITER_VANLEER), (dg.RIEMANN_ROE, dg.LIMITER_MC),
+                                             (dg.RIEMANN_EXACT, dg.LIMITER_MC)])
+def test_mixed_3d_blast_vs_fp64_oracle(riemann, limiter):
+    """The mixed 3D step (FP32 reconstruction, corrections and fluxes, FP64
+    energies and accumulation) within the bar of the FP64 oracle on a 16^3
+    blast with a seeded velocity field, ragged spacings, outflow."""
+    n = 16
+    w0, d = _blast3d(n, seed=riemann)
+    ds = (d, d * 1.25, d * 0.8)
+    G = dg.Grid3D(n, n, n, *ds, ghosts=2, config=dg.Config(riemann=riemann, limiter=limiter,
+                                                           precision=dg.PREC_MIXED))
+    R = oracle_grid(dim=3, n=(n, n, n), d=ds, ghosts=2, riemann=riemann, limiter=limiter)
+    G.w[...] = w0
+    R.set_prim(w0)
+    for _ in range(6):
+        R.step_cfl()
+    res = G.advance_steps(6)
+    assert res.steps == 6
+    g = 2
+    got, ref = G.w[g:-g, g:-g, g:-g], R.get_prim()[g:-g, g:-g, g:-g]
+    assert np.any(got != ref)  # really the FP32 path
+    l1 = problems.rel_l1(got.reshape(-1, 5), ref.reshape(-1, 5))
+    assert np.all(l1 <= TOL_MIXED), l1
+
+
+def test_mixed_3d_is_physical_on_a_strong_blast():
+    """p_in = 1e4 against p = 0.1: the FP64 pressure recovery keeps every
+    cell physical and the step within the bar of the FP64 grid."""
+    n = 24
+    w0, d = _blast3d(n, seed=3, p_in=1.0e4)
+    grids = {}
+    for prec in (dg.PREC_FP64, dg.PREC_MIXED):
+        G = dg.Grid3D(n, n, n, d, d, d, ghosts=2, config=dg.Config(riemann=dg.RIEMANN_HLLC, limiter=dg.LIMITER_MC,
+                                                                   precision=prec))
+        G.w[...] = w0
+        assert G.advance_steps(10).steps == 10
+        grids[prec] = G.w[2:-2, 2:-2, 2:-2].copy()
+        G.close()
+    a, b = grids[dg.PREC_MIXED], grids[dg.PREC_FP64]
+    assert np.all(np.isfinite(a)) and np.all(a[..., 0] > 0) and np.all(a[..., 1] > 0)
+    l1 = problems.rel_l1(a.reshape(-1, 5), b.reshape(-1, 5))
+    assert np.all(l1 <= TOL_MIXED), l1
 
 
 # The 1D two-state problems of the reference's Examples/1D (rho, u, p left /
