@@ -500,6 +500,48 @@ def mhd_report(n=1024, steps=20, warmup=3):
     return out
 
 
+def mixed3d_report(n=256, steps=8, warmup=2):
+    """The mixed FP32/FP64 3D hydro step against the FP64 one: the 3D blast
+    n^3 (p_in 10, MC, HLLC, outflow), device time per CFL step (CUDA events on
+    the grid's stream, L2 flushed), and the relative L1 per field of the two
+    states after warmup + steps steps from the same initial state."""
+    import torch
+
+    import dragon_b200 as dg
+    from dragon_b200 import problems
+
+    w5, d = problems.blast_3d(n, ghosts=2, p_in=10.0)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    out = {"workload": f"3D blast {n}^3, p_in 10, MC, HLLC, outflow", "steps": steps + warmup}
+    states = {}
+    for name, prec in (("fp64", dg.PREC_FP64), ("mixed", dg.PREC_MIXED)):
+        G = dg.Grid3D(n, n, n, d, d, d, ghosts=2,
+                      config=dg.Config(riemann=dg.RIEMANN_HLLC, limiter=dg.LIMITER_MC, precision=prec))
+        G.w[...] = w5
+        G.advance_steps(warmup)
+        stream = torch.cuda.ExternalStream(G._lib.dragon_gpu_stream(G._h))
+        ev = []
+        torch.cuda.synchronize()
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+            G.advance_steps_async(1)
+            b.record(stream)
+            G.advance_wait()
+            ev.append((a, b))
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in ev) / steps
+        out[name] = {"ms_per_step": ms, "value": n ** 3 / (ms / 1e3), "unit": "cell-updates/s"}
+        states[name] = G.w[2:-2, 2:-2, 2:-2].reshape(-1, 5).copy()
+        G.close()
+    out["mixed"]["speedup_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    out["mixed"]["rel_l1_vs_fp64_per_field"] = [float(x) for x in problems.rel_l1(states["mixed"], states["fp64"])]
+    return out
+
+
 def stated_length_report(n=1024, kh_steps=2000, ot_time=0.5):
     """The mixed path against the FP64 path (bit-identical to the reference) at
     the stated lengths of the two 2D configurations: the shear layer for
@@ -773,6 +815,11 @@ def summary_of(d):
         m = d["mhd"]
         out["mhd_orszag_tang_1024"] = {"fp64_value": m["fp64"]["value"], "mixed_value": m["mixed"]["value"],
                                        "mixed_speedup": m["mixed"]["speedup_vs_fp64"]}
+    if "mixed3d" in d:
+        m = d["mixed3d"]
+        out["mixed_3d_blast_256"] = {"fp64_value": m["fp64"]["value"], "mixed_value": m["mixed"]["value"],
+                                     "mixed_speedup": m["mixed"]["speedup_vs_fp64"],
+                                     "max_rel_l1_vs_fp64": max(m["mixed"]["rel_l1_vs_fp64_per_field"])}
     if "learned_guess" in d:
         g = d["learned_guess"]
         out["learned_guess"] = {k: g[k] for k in g if k.startswith(("iteration_reduction", "ceiling_reduction"))}
@@ -969,6 +1016,8 @@ def run_gpu(args):
             detail["batch"] = batch_report()
         if not args.no_mhd:
             detail["mhd"] = mhd_report()
+        if not args.no_mixed3d:
+            detail["mixed3d"] = mixed3d_report()
         if not args.no_stated_length:
             detail["stated_length"] = stated_length_report()
         if not args.no_custom_bc:
@@ -1001,6 +1050,7 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned star-pressure guess report")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched uneven-instance report")
     ap.add_argument("--no-mhd", action="store_true", help="skip the 2D MHD (Orszag-Tang) report")
+    ap.add_argument("--no-mixed3d", action="store_true", help="skip the mixed 3D hydro (256^3 blast) report")
     ap.add_argument("--no-custom-bc", action="store_true", help="skip the user-GhostFill step cost")
     ap.add_argument("--no-dist", action="store_true", help="multi-GPU runs: skip the sharded 4096^2 grid")
     ap.add_argument("--no-stated-length", action="store_true",
