@@ -3,7 +3,7 @@ profiling and quick checks on a GPU):
 
     python -m dragon_b200.workloads kh      --n 1024 --steps 5 [--mixed]
     python -m dragon_b200.workloads ot      --n 512  --steps 5 [--mixed]
-    python -m dragon_b200.workloads blast3d --n 128  --steps 3 [--riemann exact] [--mhd]
+    python -m dragon_b200.workloads blast3d --n 128  --steps 3 [--riemann exact] [--mhd | --mixed]
     python -m dragon_b200.workloads batch   --n1d 256 --n2d 32 --steps 5 [--mixed]
 
 kh: 2D shear layer (HLLC, van Leer, periodic); ot: 2D MHD Orszag-Tang (HLLD,
@@ -45,10 +45,11 @@ def ot(n, steps, mixed):
     return G
 
 
-def blast3d(n, riemann, mhd):
+def blast3d(n, riemann, mhd, mixed=False):
     w5, d = problems.blast_3d(n, ghosts=3 if mhd else 2, p_in=10.0)
     if not mhd:
-        cfg = _grid.Config(riemann=riemann, limiter=_grid.LIMITER_MC)
+        cfg = _grid.Config(riemann=riemann, limiter=_grid.LIMITER_MC,
+                           precision=_grid.PREC_MIXED if mixed else _grid.PREC_FP64)
         G = _grid.Grid3D(n, n, n, d, d, d, ghosts=2, config=cfg)
         G.w[...] = w5
         return G
@@ -105,7 +106,7 @@ def main(argv=None):
               f"replay_ms={st['replay_ms']:.3f}")
         return
     G = {"kh": lambda: kh(a.n, a.steps, a.mixed), "ot": lambda: ot(a.n, a.steps, a.mixed),
-         "blast3d": lambda: blast3d(a.n, rs, a.mhd)}[a.workload]()
+         "blast3d": lambda: blast3d(a.n, rs, a.mhd, a.mixed)}[a.workload]()
     G.advance_steps(1)
     G.w  # noqa: B018  (synchronises)
     t = time.perf_counter()
