@@ -16,9 +16,9 @@ struct Mhd3DScratch;
 
 int launch_step1d(bool mhd, int solver, const Geo& G, const double* win, double* wout, StepCtl* ctl,
                   const StepArgs& sa, cudaStream_t st);
-// Mixed FP32/FP64 1D hydro sweep (step1d_mixed.cu).
-int launch_step1d_mixed(int solver, const Geo& G, const double* win, double* wout, StepCtl* ctl, const StepArgs& sa,
-                        cudaStream_t st);
+// Mixed FP32/FP64 1D sweep, hydro or MHD (step1d_mixed.cu).
+int launch_step1d_mixed(bool mhd, int solver, const Geo& G, const double* win, double* wout, StepCtl* ctl,
+                        const StepArgs& sa, cudaStream_t st);
 // The fused 2D hydro steps load each tile with one TMA copy through `map`, a
 // tensor map of the input buffer with the box step2d_tile_box gives (columns,
 // rows, fields) for the FP64 (mixed = 0) or the mixed kernel.

@@ -256,7 +256,7 @@ int launch_step(dragon_grid* h, int c) {
     int rc = 0, nk = 1;
     if (h->dim == 1) {
         rc = (h->cfg.precision == 1)
-                 ? launch_step1d_mixed(h->solver, h->cg, h->w[c], h->w[c ^ 1], h->ctl, sa, h->stream)
+                 ? launch_step1d_mixed(h->mhd, h->solver, h->cg, h->w[c], h->w[c ^ 1], h->ctl, sa, h->stream)
                  : launch_step1d(h->mhd, h->solver, h->cg, h->w[c], h->w[c ^ 1], h->ctl, sa, h->stream);
     } else if (h->mhd) {
         if (h->dim == 3) {
@@ -744,9 +744,9 @@ int dragon_gpu_grid_create(int dim, int nx, int ny, int nz, double dx, double dy
         delete h;
         return fail(DRAGON_GPU_EUNSUPPORTED, "the learned star-pressure guess is built for 3D hydro grids");
     }
-    if (h->cfg.precision != 0 && !(dim == 2 || !h->mhd)) {
+    if (h->cfg.precision != 0 && dim == 3 && h->mhd) {
         delete h;
-        return fail(DRAGON_GPU_EUNSUPPORTED, "the mixed-precision path is built for hydro grids and 2D MHD grids");
+        return fail(DRAGON_GPU_EUNSUPPORTED, "the mixed-precision path is built for hydro grids and 1D / 2D MHD grids");
     }
     if (h->cfg.precision != 0 && h->cfg.exact_guess == GUESS_LEARNED) {
         delete h;

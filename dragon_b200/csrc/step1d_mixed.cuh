@@ -152,4 +152,94 @@ __device__ __forceinline__ void step1d_tile_mx(const Geo& G, const double* __res
     if (first_order) atomicAdd(&ctl->muscl_first_order, (unsigned long long)first_order);
 }
 
+// The 1D MHD sweep (cell-centred B; the HLLD / HLL / HLLE fluxes) in mixed
+// precision: FP32 MUSCL (no face-B source terms in 1D, as the FP64 sweep) and
+// fluxes on absolute pressures, FP64 energies in every FP32 reconstruction,
+// FP64 update of the FP64 state, the FP64 sweep's index ranges and end faces.
+template <int SOLVER, int TS>
+__device__ __forceinline__ void step1d_tile_mx_mhd(const Geo& G, const double* __restrict__ win,
+                                                   double* __restrict__ wout, StepCtl* ctl, const StepArgs& sa,
+                                                   int tile) {
+    constexpr int NF = 8;
+    __shared__ float sw[NF][TS + 4];
+    __shared__ float sL[NF][TS + 2], sR[NF][TS + 2];
+    __shared__ float sF[NF][TS + 1];
+    __shared__ double red[32];
+    __shared__ int s_skip;
+    if (cta_should_skip(ctl, &s_skip)) return;
+    const int np = G.n[0] + 2 * G.g;
+    const int p0 = tile * TS;
+    const long long PL = G.plane;
+    const double dt = *(volatile double*)&ctl->t1;
+    const double dt_dx = dt / sa.dx;
+    const float fdx = (float)dt_dx;
+    const ExactOpts eo = exact_opts(sa);
+    FaceStats st{0, 0, 0, 0, 0};
+    int first_order = 0;
+    for (int q = threadIdx.x; q < TS + 4; q += blockDim.x) {  // cell p = p0 - 2 + q
+        const int p = p0 - 2 + q;
+        if (p >= 0 && p < np)
+#pragma unroll
+            for (int f = 0; f < NF; f++) sw[f][q] = (float)win[f * PL + p];
+    }
+    __syncthreads();
+    auto getw = [&](int q) {
+        return Prim<float>{sw[0][q], sw[1][q], sw[2][q], sw[3][q], sw[4][q], sw[5][q], sw[6][q], sw[7][q]};
+    };
+    auto put = [&](float (*arr)[TS + 2], int q, const Prim<float>& r) {
+        arr[0][q] = r.rho; arr[1][q] = r.p; arr[2][q] = r.vx; arr[3][q] = r.vy; arr[4][q] = r.vz;
+        arr[5][q] = r.Bx; arr[6][q] = r.By; arr[7][q] = r.Bz;
+    };
+    auto get = [&](float (*arr)[TS + 2], int q) {
+        return Prim<float>{arr[0][q], arr[1][q], arr[2][q], arr[3][q], arr[4][q], arr[5][q], arr[6][q], arr[7][q]};
+    };
+    for (int q = threadIdx.x; q < TS + 2; q += blockDim.x) {  // cells p in [p0-1, p0+TS]
+        const int p = p0 - 1 + q;
+        if (p >= 1 && p <= np - 2) {
+            Prim<float> oL, oR;
+            first_order += !muscl_mixed<true>(sa.limiter, getw(q), oL, getw(q + 1), oR, getw(q + 2), fdx, 0.f, 0.f, 0.f);
+            put(sL, q, oL);
+            put(sR, q, oR);
+        }
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < TS + 1; q += blockDim.x) {  // faces p in [p0-1, p0+TS-1]
+        const int p = p0 - 1 + q;
+        if (p < 0 || p > np - 2) continue;
+        const Prim<float> L = (p == 0) ? getw(q + 1) : get(sR, q);
+        const Prim<float> R = (p + 1 == np - 1) ? getw(q + 2) : get(sL, q + 1);
+        Cons<float> F;
+        if (!face_flux_mixed<true, SOLVER, 0>(L, R, fdx, eo, F, &st)) record_error(ctl, ST_FINAL_FLUX, p);
+        sF[0][q] = F.rho; sF[1][q] = F.E; sF[2][q] = F.mx; sF[3][q] = F.my; sF[4][q] = F.mz;
+        sF[5][q] = F.Bx; sF[6][q] = F.By; sF[7][q] = F.Bz;
+    }
+    __syncthreads();
+    double vmax = 0.0;
+    for (int q = threadIdx.x; q < TS; q += blockDim.x) {  // cell p = p0 + q
+        const int p = p0 + q;
+        if (p >= np) continue;
+        const Prim<double> w0 = load_prim<true>(win, PL, p);
+        Prim<double> nw = w0;
+        if (p >= 1 && p <= np - 2) {
+            Cons<double> U = to_cons64<true>(w0);
+            double* u8[NF] = {&U.rho, &U.E, &U.mx, &U.my, &U.mz, &U.Bx, &U.By, &U.Bz};
+#pragma unroll
+            for (int f = 0; f < NF; f++) *u8[f] += ((double)sF[f][q] - (double)sF[f][q + 1]) * dt_dx;
+            nw = to_prim64<true>(U);
+            // the FP64 sweep's second, zero-difference round trip on cell np-2
+            if (p == np - 2) nw = to_prim64<true>(to_cons64<true>(nw));
+        }
+        const int c = p - G.g;
+        if (c >= 0 && c < G.n[0]) {
+            if (!is_physical<true>(nw)) record_error(ctl, ST_UNPHYSICAL, p);
+            vmax = speed_max(vmax, cfl_speed_1d_mx<true>(nw));
+        }
+        store_prim<true>(wout, PL, p, nw);
+    }
+    vmax = block_max(vmax, red);
+    if (threadIdx.x == 0) atomic_max_speed(&ctl->vmax[sa.slot_out], vmax);
+    if (st.hlld_to_hlle) atomicAdd(&ctl->hlld_to_hlle, (unsigned long long)st.hlld_to_hlle);
+    if (first_order) atomicAdd(&ctl->muscl_first_order, (unsigned long long)first_order);
+}
+
 }  // namespace dgpu

@@ -1,4 +1,4 @@
-"""The mixed FP32/FP64 1D hydro, 2D hydro and 2D MHD paths against the FP64 oracle.
+"""The mixed FP32/FP64 1D, 2D and 3D hydro and 1D and 2D MHD paths against the FP64 oracle.
 
 The mixed path runs reconstruction, limiters, the Riemann solves and the CTU
 corrections in FP32 while the state, every pressure recovery, the
@@ -92,11 +92,9 @@ def test_mixed_sod_strong_shock_stays_physical():
     assert np.all(np.isfinite(G.w)) and np.all(l1 <= TOL_MIXED), l1
 
 
-def test_mixed_on_hydro_grids_and_2d_mhd_only():
+def test_mixed_refused_on_3d_mhd_and_learned_guess():
     with pytest.raises(dg.grid._lib.DragonGPUError):
         dg.Grid3D(4, 4, 4, 0.1, 0.1, 0.1, config=dg.Config(mhd=True, precision=dg.PREC_MIXED))
-    with pytest.raises(dg.grid._lib.DragonGPUError):
-        dg.Grid1D(16, 1 / 16, config=dg.Config(mhd=True, precision=dg.PREC_MIXED))
     with pytest.raises(dg.grid._lib.DragonGPUError):
         dg.Grid3D(4, 4, 4, 0.1, 0.1, 0.1, config=dg.Config(riemann=dg.RIEMANN_EXACT, exact_guess=dg.GUESS_LEARNED,
                                                            precision=dg.PREC_MIXED))
@@ -188,6 +186,61 @@ def test_mixed_1d_riemann_l1_vs_fp64_oracle(case, riemann, limiter):
     assert np.all(np.isfinite(G.w)) and np.all(l1[:3] <= TOL_MIXED), l1
     assert np.all(G.w[g:-g, 3:] == 0.0)
     assert np.any(G.w[g:-g] != ref)  # really the FP32 path
+
+
+def brio_wu_1d(n, g):
+    """Brio-Wu-like tube (Gaussian units: B scaled by sqrt(4 pi)), cell B only."""
+    w = np.zeros((n + 2 * g, 8))
+    x = (np.arange(n) + 0.5) / n
+    L = x < 0.5
+    w[g:g + n, 0] = np.where(L, 1.0, 0.125)
+    w[g:g + n, 1] = np.where(L, 1.0, 0.1)
+    w[g:g + n, 5] = 0.75 * np.sqrt(4 * np.pi)
+    w[g:g + n, 6] = np.where(L, 1.0, -1.0) * np.sqrt(4 * np.pi)
+    return w
+
+
+@pytest.mark.parametrize("riemann,limiter", [(dg.RIEMANN_HLLD, dg.LIMITER_MC), (dg.RIEMANN_HLL, dg.LIMITER_MINMOD),
+                                             (dg.RIEMANN_HLLE, dg.LIMITER_VANLEER)])
+def test_mixed_1d_mhd_brio_wu_vs_fp64_oracle(riemann, limiter):
+    """1D MHD sweep, mixed: every nonzero field within the bar of the FP64
+    oracle on a Brio-Wu-like tube to t = 0.05 (256 cells, outflow); the
+    fields the problem leaves zero stay exactly zero, and Bx stays exactly
+    its initial value (the 1D sweep never updates it)."""
+    n, g = 256, 3
+    w = brio_wu_1d(n, g)
+    G = dg.Grid1D(n, 1.0 / n, ghosts=g, config=dg.Config(mhd=True, riemann=riemann, limiter=limiter,
+                                                         precision=dg.PREC_MIXED))
+    R = oracle_grid(dim=1, n=(n,), d=(1.0 / n,), ghosts=g, mhd=True, riemann=riemann, limiter=limiter)
+    G.w[...] = w
+    R.set_prim(w)
+    R.advance(0.05)
+    res = G.advance(0.05)
+    assert res.steps > 20
+    ref, got = R.get_prim()[g:-g], G.w[g:-g]
+    assert np.all(np.isfinite(got)) and np.all(got[:, 0] > 0) and np.all(got[:, 1] > 0)
+    nonzero = np.abs(ref).sum(axis=0) > 0
+    l1 = problems.rel_l1(got, ref)
+    assert np.all(l1[nonzero] <= TOL_MIXED), l1
+    assert np.all(got[:, ~nonzero] == 0.0)
+    assert np.all(got[:, 5] == w[g:-g, 5])
+    assert np.any(got != ref)  # really the FP32 path
+
+
+def test_mixed_1d_mhd_strong_field_stays_physical():
+    """A magnetically dominated tube (plasma beta 2e-4 on the right): the FP64
+    energy and pressure recovery keep the mixed sweep positive."""
+    n, g = 512, 3
+    w = brio_wu_1d(n, g)
+    w[g + n // 2:g + n, 1] = 1e-3
+    w[g:g + n, 6] *= 3.0
+    G = dg.Grid1D(n, 1.0 / n, ghosts=g, config=dg.Config(mhd=True, riemann=dg.RIEMANN_HLLD,
+                                                         limiter=dg.LIMITER_MC, precision=dg.PREC_MIXED))
+    G.w[...] = w
+    res = G.advance(0.02)
+    assert res.steps > 20
+    got = G.w[g:-g]
+    assert np.all(np.isfinite(got)) and np.all(got[:, 0] > 0) and np.all(got[:, 1] > 0)
 
 
 def divb_max(B, g, n, dx, dy):
