@@ -10,5 +10,6 @@ from .grid import (CFL_ADD, CFL_MAX, CT_CONSV_BETA_GATED, CT_CONSV_THERMAL, CT_C
                    LIMITER_MINMOD, LIMITER_SUPERBEE, LIMITER_VANALBADA, LIMITER_VANLEER, PREC_FP64, PREC_MIXED,
                    RIEMANN_EXACT, RIEMANN_HLL, RIEMANN_HLLC, RIEMANN_HLLD, RIEMANN_HLLE, RIEMANN_HLLX, RIEMANN_ROE,
                    AdvanceResult, Config, Grid1D, Grid2D, Grid3D, StepFailed)
+from . import hoard  # noqa: E402  (DRAGONHOARD: output and restart from device buffers)
 
 __all__ = [n for n in dir() if not n.startswith("_")]

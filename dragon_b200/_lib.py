@@ -100,6 +100,27 @@ class BatchStats(ctypes.Structure):
     _fields_ = [("steps", ctypes.c_int), ("retries", ctypes.c_int), ("graph_replays", ctypes.c_int),
                 ("work_items", ctypes.c_longlong), ("spin_timeouts", ctypes.c_ulonglong), ("replay_ms", ctypes.c_double)]
 
+class HoardOpts(ctypes.Structure):
+    """dragon_hoard_opts."""
+
+    _fields_ = [("write_option", ctypes.c_int), ("redundant", ctypes.c_int), ("compression", ctypes.c_int),
+                ("ghosts", ctypes.c_int), ("threads", ctypes.c_int), ("reserved", ctypes.c_int * 3)]
+
+
+class H5Dataset(ctypes.Structure):
+    """dragon_h5_dataset."""
+
+    _fields_ = [("path", ctypes.c_char_p), ("rank", ctypes.c_int), ("dims", ctypes.c_longlong * 3),
+                ("type", ctypes.c_int), ("data", ctypes.c_void_p)]
+
+
+class H5Attr(ctypes.Structure):
+    """dragon_h5_attr."""
+
+    _fields_ = [("name", ctypes.c_char_p), ("type", ctypes.c_int), ("ivalue", ctypes.c_int),
+                ("dvalue", ctypes.c_double)]
+
+
 # Every symbol include/dragon_gpu.h, include/dragon_learned.h and
 # include/dragon_batch.h declare, with its ctypes signature.
 SIGNATURES = {
@@ -202,6 +223,21 @@ SIGNATURES = {
     "dragon_gpu_batch_autotune": (
         ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(BatchTuning), ctypes.POINTER(ctypes.c_double)]),
     "dragon_gpu_batch_advance_steps": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(BatchStats)]),
+    "dragon_gpu_hoard_default_opts": (None, [ctypes.POINTER(HoardOpts)]),
+    "dragon_gpu_hoard_write": (
+        ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_char_p, ctypes.POINTER(HoardOpts)]),
+    "dragon_gpu_hoard_write_async": (
+        ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_char_p, ctypes.POINTER(HoardOpts)]),
+    "dragon_gpu_hoard_wait": (ctypes.c_int, [ctypes.c_void_p]),
+    "dragon_gpu_hoard_load": (
+        ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, c_double_p, ctypes.POINTER(ctypes.c_int)]),
+    "dragon_h5_write": (
+        ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(H5Attr), ctypes.c_int, ctypes.POINTER(H5Dataset), ctypes.c_int,
+                       ctypes.c_int, ctypes.c_int]),
+    "dragon_h5_read_attr": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, c_double_p]),
+    "dragon_h5_dataset_shape": (
+        ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_longlong)]),
+    "dragon_h5_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, c_double_p, ctypes.c_longlong]),
 }
 
 _lib = None

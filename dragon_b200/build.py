@@ -90,7 +90,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
 
     with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         objs = list(ex.map(compile_one, _sources()))
-    subprocess.run([nvcc, *ARCH, "-shared", "-o", LIB + ".tmp", *objs, "-ldl"], check=True)
+    subprocess.run([nvcc, *ARCH, "-shared", "-o", LIB + ".tmp", *objs, "-ldl", "-lz"], check=True)
     os.replace(LIB + ".tmp", LIB)
     build_host(force=True, verbose=verbose)
     return LIB

@@ -17,6 +17,7 @@ namespace dgpu {
 struct MlpNet;
 }
 struct dragon_user_fill;
+struct HoardState;
 
 // A user ghost fill bound to one entry of a grid's boundary list
 // (dragon_gpu_set_user_fill): the compiled fill, the faces whose ghost cells it
@@ -109,6 +110,8 @@ struct dragon_grid {
     // (FP64, mixed), encoded on first use
     CUtensorMap tmap[2][2];
     bool tmap_ok[2][2] = {{false, false}, {false, false}};
+    // output snapshots in flight (hoard.cu), created on first use
+    HoardState* hoard = nullptr;
 };
 
 namespace dgpu_rt {
@@ -132,5 +135,7 @@ const char* stage_name(int s);
 int launch_user_fill(dragon_grid* h, int c, int entry, double* w_buf);
 // Releases a handle's user-fill bindings (their device parameters).
 void clear_user_fills(dragon_grid* h);
+// Waits for a handle's output snapshots and frees their buffers (hoard.cu).
+void hoard_release(dragon_grid* h);
 
 }  // namespace dgpu_rt

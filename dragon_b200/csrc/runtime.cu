@@ -823,6 +823,7 @@ int dragon_gpu_grid_create(int dim, int nx, int ny, int nz, double dx, double dy
 int dragon_gpu_grid_destroy(dragon_grid* h) {
     if (!h) return 0;
     if (h->stream) cudaStreamSynchronize(h->stream);
+    hoard_release(h);
     collect_profile(h);
     clear_user_fills(h);
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);

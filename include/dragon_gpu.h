@@ -273,6 +273,72 @@ int dragon_gpu_cfl_time_noalloc(int dim, int nx, int ny, int nz, int ghosts, int
                                 long long plane_stride, long long pitch, double dx, double dy, double dz, int cfl,
                                 double cfl_coeff, void* stream, double* dt_out);
 
+/* ---- Output and restart from device buffers ------------------------------
+ * Replaces DRAGONHOARD::writeToFile and DRAGONHOARD::loadFromFile
+ * (DRAGONHOARD/DragonHoard.hpp:16-33; HDF5Output.cpp:103-528,
+ * HDF5Restart.cpp:61-377). A file holds the reference's layout and keys
+ * (HDF5_Attrs.hpp:14-59): int and double attributes format_version (1),
+ * write_option, dim, MHD, ng, nx[, ny, nz], dx[, dy, dz], cycle, time on the
+ * root group, and datasets /fluid/rho, /fluid/v/{x,y,z}, /fluid/p, /fluid/E,
+ * /fluid/momentum/{x,y,z}, /fluid/B/{x,y,z}, /fluid/Bf/{x,y,z} as the options
+ * select them, flattened x fastest (HDF5Output.cpp:308) with dimensions
+ * {nz, ny, nx}. Files are HDF5 (superblock 0, chunked + deflate or
+ * contiguous), written without the HDF5 library. */
+typedef struct {
+    int write_option; /* HDF5_WRITE_OPTION (DRAGONHOARD_Config.h:24-28): 1 primitive, 3 primitive + energy,
+                         6 conservative, 7 both; default 3 */
+    int redundant;    /* HDF5_REDUNDANT_VALS_OPTION (:31-35): 0 omit, 1 float, 2 double; default 1 */
+    int compression;  /* HDF5_COMPRESSION_LEVEL (:22): deflate level (1-9) of chunked datasets; <= 0 writes
+                         them contiguous and uncompressed; default 4 */
+    int ghosts;       /* WRITE_GHOSTS_TO_FILE (:32): nonzero writes the ghost layers too; default 0 */
+    int threads;      /* host threads that compress chunks; 0: every core */
+    int reserved[3];
+} dragon_hoard_opts;
+
+void dragon_gpu_hoard_default_opts(dragon_hoard_opts* o);
+/* Writes the grid's current state to `path` (the full file name) and returns
+ * when the file is complete. */
+int dragon_gpu_hoard_write(dragon_grid* g, double t, int cycle, const char* path, const dragon_hoard_opts* o);
+/* Snapshots the current state on the grid's stream and returns: the device
+ * packs the datasets into one of two staging buffers, a copy stream downloads
+ * it while later steps run, and a host thread writes the file. A third call
+ * waits for the oldest snapshot's file first. Later steps and boundary calls
+ * do not change a snapshot already taken. */
+int dragon_gpu_hoard_write_async(dragon_grid* g, double t, int cycle, const char* path, const dragon_hoard_opts* o);
+/* Waits for every file of g in flight; returns the first failure among them. */
+int dragon_gpu_hoard_wait(dragon_grid* g);
+/* Restart (HDF5Restart.cpp:61-377): checks format_version <= 1, dim, MHD
+ * and the extents against the grid, then loads dx/dy/dz (the grid's spacing
+ * becomes the file's), the cells and (MHD 2D / 3D) face B of the file's
+ * range: primitive values when write_option has bit 1, else rho, momentum and
+ * E converted to primitive values. Returns *t and *cycle. */
+int dragon_gpu_hoard_load(dragon_grid* g, const char* path, double* t, int* cycle);
+
+/* The HDF5 subset itself, on host arrays (no device involved). */
+#define DRAGON_H5_F64 0
+#define DRAGON_H5_F32 1
+#define DRAGON_H5_I32 2
+typedef struct {
+    const char* path;  /* absolute, e.g. "/fluid/v/x"; parent groups are created */
+    int rank;          /* 1 to 3 */
+    long long dims[3]; /* slowest first */
+    int type;          /* DRAGON_H5_F64 or DRAGON_H5_F32 */
+    const void* data;  /* row-major */
+} dragon_h5_dataset;
+typedef struct {
+    const char* name;
+    int type; /* DRAGON_H5_I32 or DRAGON_H5_F64 */
+    int ivalue;
+    double dvalue;
+} dragon_h5_attr;
+int dragon_h5_write(const char* file, const dragon_h5_attr* attrs, int nattrs, const dragon_h5_dataset* dsets,
+                    int ndsets, int level, int threads);
+int dragon_h5_read_attr(const char* file, const char* name, double* value);
+/* rank 0 for a scalar; dims3 receives up to three dimensions, slowest first. */
+int dragon_h5_dataset_shape(const char* file, const char* path, int* rank, long long* dims3);
+/* Reads a dataset converted to double; capacity is out's length in elements. */
+int dragon_h5_read(const char* file, const char* path, double* out, long long capacity);
+
 const char* dragon_gpu_last_error(void);
 
 #ifdef __cplusplus
