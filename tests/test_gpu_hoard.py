@@ -197,7 +197,7 @@ def test_reference_io_round_trip(dim, n, d, mhd, ghosts):
     t, cyc = hoard.load_from_file(G2, "TEMP_IO" if dim == 1 else "TEMP_IO.h5")
     assert t == 0.666 and cyc == 666
     assert [getattr(G2, k) for k in ("dx", "dy", "dz")[:dim]] == list(d)
-    g = 0 if ghosts else 2
+    g = 0 if ghosts else G.ghosts  # MHD grids raise the ghost width to 3 (validGhosts)
     sl = tuple(slice(g, s - g) for s in G.w.shape[:dim])
     a, b = G.w[sl], G2.w[sl]
     np.testing.assert_array_equal(a[..., :5], b[..., :5])
@@ -209,7 +209,7 @@ def test_reference_io_round_trip(dim, n, d, mhd, ghosts):
             fs = tuple(slice(g, s - g) for s in G.B.shape[:dim])
             np.testing.assert_array_equal(G.B[fs], G2.B[fs])
     if not ghosts:  # cells outside the file's range keep the fresh grid's zeros
-        assert np.all(G2.w[(slice(0, 2),) + (slice(None),) * (dim - 1)] == 0)
+        assert np.all(G2.w[(slice(0, G.ghosts),) + (slice(None),) * (dim - 1)] == 0)
 
 
 def test_reference_io_dimension_and_size_checks():
