@@ -659,6 +659,101 @@ __device__ void jet(const dragon_fill_ctx& c, int i, int j, int k) {
     return out
 
 
+def hoard_report(n=1024, reps=8, every=50, frames=6):
+    """Output from device buffers (DRAGONHOARD's writeToFile) on the n^2 FP64
+    shear layer with the reference's default options (primitive values + E as
+    float, deflate level 4): the pack kernel's device time and bandwidth (L2
+    flushed; algorithmic bytes = 5 FP64 fields read + the datasets written),
+    the wall time of a complete file (pack, download, deflate on every host
+    core, write) compressed and uncompressed, the same file built on the host
+    from the downloaded padded state (the route without a device pack), and
+    the wall time per step of a run that snapshots every `every` steps
+    asynchronously against the same run without snapshots."""
+    import tempfile
+
+    import torch
+
+    import dragon_b200 as dg
+    from dragon_b200 import hoard, problems
+
+    w0, dx, dy = problems.kelvin_helmholtz_2d(n, ghosts=2, seed=1234)
+    G = dg.Grid2D(n, n, dx, dy, ghosts=2, config=dg.Config(riemann=dg.RIEMANN_HLLC, limiter=dg.LIMITER_VANLEER))
+    G.w[...] = w0
+    G.boundary = dg.Periodic()
+    G.advance_steps(3)
+    tmp = tempfile.mkdtemp(prefix="hoard_")
+    old_dir = hoard.output_dir
+    hoard.output_dir = tmp
+    out = {"workload": f"shear layer {n}^2 FP64, write option 3 (primitive + E as float), deflate 4",
+           "host_threads": os.cpu_count()}
+    try:
+        G._to_device()
+        stream = torch.cuda.ExternalStream(G._lib.dragon_gpu_stream(G._h))
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+        raw = hoard.Options(compression_level=0)
+        ev = []
+        for r in range(reps + 2):
+            hoard.wait(G)
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+            hoard.write_to_file(G, 0.0, r, "pack", wait=False, opts=raw)
+            b.record(stream)
+            if r >= 2:
+                ev.append((a, b))
+        hoard.wait(G)
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in ev) / len(ev)
+        cells = n * n
+        alg = cells * (5 * 8 + 5 * 8 + 4)
+        peak, peak_kind = measured_peaks()
+        out["pack"] = {"kernel": "k_hoard_pack", "ms": ms, "bytes_per_cell": 84, "achieved_gbs": alg / ms / 1e6,
+                       "peak_gbs": peak, "peak_source": peak_kind, "frac": alg / ms / 1e6 / peak}
+        for name, opts in (("deflate4", hoard.Options()), ("uncompressed", raw)):
+            t0 = time.perf_counter()
+            for r in range(3):
+                hoard.write_to_file(G, 0.0, r, f"{name}_{r}", opts=opts)
+            dt = (time.perf_counter() - t0) / 3
+            size = os.path.getsize(os.path.join(tmp, f"{name}_0.h5"))
+            out["file_" + name] = {"s_per_file": dt, "bytes": size, "mb_per_s_of_datasets": cells * 44 / dt / 1e6}
+        # the host route: download the padded state, flatten and convert on the host, write
+        t0 = time.perf_counter()
+        for r in range(3):
+            G._dev_dirty = True
+            w = G.w[2:-2, 2:-2]
+            ds = {"/fluid/rho": w[..., 0].T, "/fluid/v/x": w[..., 2].T, "/fluid/v/y": w[..., 3].T,
+                  "/fluid/v/z": w[..., 4].T, "/fluid/p": w[..., 1].T,
+                  "/fluid/E": (w[..., 1] / (5.0 / 3.0 - 1.0) + (w[..., 0] / 2.0) *
+                               (w[..., 2] ** 2 + w[..., 3] ** 2 + w[..., 4] ** 2)).T.astype(np.float32)}
+            hoard.write_h5(os.path.join(tmp, f"host_{r}.h5"), {"dim": 2}, ds, level=4)
+        out["file_host_route"] = {"s_per_file": (time.perf_counter() - t0) / 3}
+        # stepping with asynchronous snapshots
+        G.advance_steps(every)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(frames):
+            G.advance_steps(every)
+        torch.cuda.synchronize()
+        base = (time.perf_counter() - t0) / (frames * every) * 1e3
+        t0 = time.perf_counter()
+        for f in range(frames):
+            G.advance_steps(every)
+            hoard.write_to_file(G, 0.0, f, f"frame_{hoard.cycle_string(f)}", wait=False)
+        hoard.wait(G)
+        torch.cuda.synchronize()
+        snap = (time.perf_counter() - t0) / (frames * every) * 1e3
+        out["stepping"] = {"every_steps": every, "frames": frames, "ms_per_step_no_output": base,
+                           "ms_per_step_with_async_output": snap, "overhead": snap / base - 1.0}
+    finally:
+        hoard.output_dir = old_dir
+        G.close()
+        import shutil
+        shutil.rmtree(tmp, ignore_errors=True)
+    return out
+
+
 def _batch_run(precision, steps, one_by_one_steps):
     """One precision of the batched uneven-instance workload: the batch
     (autotuned, then timed over `steps` steps) and the same grids advanced one
@@ -829,6 +924,12 @@ def summary_of(d):
     if "custom_bc" in d:
         out["user_ghostfill_step_vs_builtin"] = {"host_apply": d["custom_bc"]["ratio"],
                                                  "device_fill": d["custom_bc"]["device_ratio"]}
+    if "hoard" in d:
+        h = d["hoard"]
+        out["hoard_output_1024"] = {"pack_ms": h["pack"]["ms"], "pack_hbm_frac": h["pack"]["frac"],
+                                    "file_s": h["file_deflate4"]["s_per_file"],
+                                    "host_route_file_s": h["file_host_route"]["s_per_file"],
+                                    "async_output_overhead": h["stepping"]["overhead"]}
     if "dist" in d:
         out["distgrid_4096_strong"] = {"value": d["dist"]["value"], "ms_per_step": d["dist"]["ms_per_step"]}
     if "batch" in d:
@@ -1022,6 +1123,8 @@ def run_gpu(args):
             detail["stated_length"] = stated_length_report()
         if not args.no_custom_bc:
             detail["custom_bc"] = custom_bc_report()
+        if not args.no_hoard:
+            detail["hoard"] = hoard_report()
         if not args.no_cpu_baseline:
             cb, why = reference_baseline(1000, 0, budget_s=args.cpu_budget)
             line["cpu_baseline"] = cb if cb else {"unavailable": why}
@@ -1051,6 +1154,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched uneven-instance report")
     ap.add_argument("--no-mhd", action="store_true", help="skip the 2D MHD (Orszag-Tang) report")
     ap.add_argument("--no-mixed3d", action="store_true", help="skip the mixed 3D hydro (256^3 blast) report")
+    ap.add_argument("--no-hoard", action="store_true", help="skip the output-from-device-buffers report")
     ap.add_argument("--no-custom-bc", action="store_true", help="skip the user-GhostFill step cost")
     ap.add_argument("--no-dist", action="store_true", help="multi-GPU runs: skip the sharded 4096^2 grid")
     ap.add_argument("--no-stated-length", action="store_true",
