@@ -659,7 +659,7 @@ __device__ void jet(const dragon_fill_ctx& c, int i, int j, int k) {
     return out
 
 
-def hoard_report(n=1024, reps=8, every=50, frames=6):
+def hoard_report(n=1024, reps=8, intervals=(50, 250), frames=6):
     """Output from device buffers (DRAGONHOARD's writeToFile) on the n^2 FP64
     shear layer with the reference's default options (primitive values + E as
     float, deflate level 4): the pack kernel's device time and bandwidth (L2
@@ -667,8 +667,9 @@ def hoard_report(n=1024, reps=8, every=50, frames=6):
     the wall time of a complete file (pack, download, deflate on every host
     core, write) compressed and uncompressed, the same file built on the host
     from the downloaded padded state (the route without a device pack), and
-    the wall time per step of a run that snapshots every `every` steps
-    asynchronously against the same run without snapshots."""
+    the wall time per step of runs that snapshot every k steps (k in
+    `intervals`) asynchronously against the same run without snapshots: the
+    stepping hides a file when k steps take longer than writing one."""
     import tempfile
 
     import torch
@@ -730,22 +731,24 @@ def hoard_report(n=1024, reps=8, every=50, frames=6):
             hoard.write_h5(os.path.join(tmp, f"host_{r}.h5"), {"dim": 2}, ds, level=4)
         out["file_host_route"] = {"s_per_file": (time.perf_counter() - t0) / 3}
         # stepping with asynchronous snapshots
-        G.advance_steps(every)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for _ in range(frames):
+        out["stepping"] = []
+        for every in intervals:
             G.advance_steps(every)
-        torch.cuda.synchronize()
-        base = (time.perf_counter() - t0) / (frames * every) * 1e3
-        t0 = time.perf_counter()
-        for f in range(frames):
-            G.advance_steps(every)
-            hoard.write_to_file(G, 0.0, f, f"frame_{hoard.cycle_string(f)}", wait=False)
-        hoard.wait(G)
-        torch.cuda.synchronize()
-        snap = (time.perf_counter() - t0) / (frames * every) * 1e3
-        out["stepping"] = {"every_steps": every, "frames": frames, "ms_per_step_no_output": base,
-                           "ms_per_step_with_async_output": snap, "overhead": snap / base - 1.0}
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(frames):
+                G.advance_steps(every)
+            torch.cuda.synchronize()
+            base = (time.perf_counter() - t0) / (frames * every) * 1e3
+            t0 = time.perf_counter()
+            for f in range(frames):
+                G.advance_steps(every)
+                hoard.write_to_file(G, 0.0, f, f"frame_{hoard.cycle_string(f)}", wait=False)
+            hoard.wait(G)
+            torch.cuda.synchronize()
+            snap = (time.perf_counter() - t0) / (frames * every) * 1e3
+            out["stepping"].append({"every_steps": every, "frames": frames, "ms_per_step_no_output": base,
+                                    "ms_per_step_with_async_output": snap, "overhead": snap / base - 1.0})
     finally:
         hoard.output_dir = old_dir
         G.close()
@@ -929,7 +932,8 @@ def summary_of(d):
         out["hoard_output_1024"] = {"pack_ms": h["pack"]["ms"], "pack_hbm_frac": h["pack"]["frac"],
                                     "file_s": h["file_deflate4"]["s_per_file"],
                                     "host_route_file_s": h["file_host_route"]["s_per_file"],
-                                    "async_output_overhead": h["stepping"]["overhead"]}
+                                    "async_output_overhead": {f"every_{x['every_steps']}": x["overhead"]
+                                                              for x in h["stepping"]}}
     if "dist" in d:
         out["distgrid_4096_strong"] = {"value": d["dist"]["value"], "ms_per_step": d["dist"]["ms_per_step"]}
     if "batch" in d:

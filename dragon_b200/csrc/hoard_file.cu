@@ -171,9 +171,9 @@ uint64_t snod_size() { return 8 + 2 * kGroupLeafK * 40; }
 uint64_t chunk_key_size(int rank) { return 8 + 8 * (rank + 1); }
 uint64_t chunk_node_size(int rank) { return 24 + 2 * kChunkK * 8 + (2 * kChunkK + 1) * chunk_key_size(rank); }
 
-void compress_chunks(DsetNode& n, int level, int threads) {
+// Chunk origins of a chunked dataset, in row-major order of the chunk grid.
+void plan_chunks(DsetNode& n) {
     const Dataset& d = *n.d;
-    const int es = esize_of(d.type);
     const int r = d.rank;
     uint64_t cnt[3] = {1, 1, 1};
     for (int a = 0; a < r; a++) cnt[a] = (d.dims[a] + n.cdims[a] - 1) / n.cdims[a];
@@ -189,47 +189,62 @@ void compress_chunks(DsetNode& n, int level, int threads) {
         }
         n.coffs[c] = o;
     }
-    const uint64_t celems = uint64_t(n.cdims[0]) * (r > 1 ? n.cdims[1] : 1) * (r > 2 ? n.cdims[2] : 1);
+}
+
+// Gathers chunk c of n (zero past the dataset's edge) into raw and deflates it.
+void compress_one(DsetNode& n, uint64_t c, int level, Bytes& raw) {
+    const Dataset& d = *n.d;
+    const int es = esize_of(d.type);
+    const int r = d.rank;
+    const uint64_t C1 = r > 1 ? n.cdims[1] : 1, C2 = r > 2 ? n.cdims[2] : 1;
+    raw.assign(uint64_t(n.cdims[0]) * C1 * C2 * es, 0);
+    const auto& o = n.coffs[c];
+    // copy the chunk's rows (the last dimension is contiguous)
+    const uint64_t D1 = r > 1 ? d.dims[1] : 1, D2 = r > 2 ? d.dims[2] : 1;
+    const uint64_t row = std::min<uint64_t>(n.cdims[r - 1], d.dims[r - 1] - o[r - 1]) * es;
+    const uint64_t e0 = std::min<uint64_t>(n.cdims[0], d.dims[0] - o[0]);
+    const uint64_t e1 = r > 1 ? std::min<uint64_t>(C1, D1 - o[1]) : 1;
+    const auto* src = static_cast<const uint8_t*>(d.data);
+    if (r == 1) {
+        std::memcpy(raw.data(), src + o[0] * es, row);
+    } else if (r == 2) {
+        for (uint64_t a = 0; a < e0; a++)
+            std::memcpy(raw.data() + a * C1 * es, src + ((o[0] + a) * D1 + o[1]) * es, row);
+    } else {
+        for (uint64_t a = 0; a < e0; a++)
+            for (uint64_t b = 0; b < e1; b++)
+                std::memcpy(raw.data() + (a * C1 + b) * C2 * es, src + (((o[0] + a) * D1 + o[1] + b) * D2 + o[2]) * es,
+                            row);
+    }
+    uLongf zn = compressBound(raw.size());
+    Bytes z(zn);
+    compress2(z.data(), &zn, raw.data(), raw.size(), level);
+    z.resize(zn);
+    n.zchunks[c] = std::move(z);
+}
+
+// Deflates every chunk of every chunked dataset: `threads` host threads take
+// chunks from one shared list, so datasets do not wait for one another.
+void compress_all(std::vector<DsetNode>& dn, int level, int threads) {
+    std::vector<std::pair<uint32_t, uint64_t>> work;
+    for (uint32_t i = 0; i < dn.size(); i++) {
+        if (!dn[i].chunked) continue;
+        plan_chunks(dn[i]);
+        for (uint64_t c = 0; c < dn[i].nchunks; c++) work.push_back({i, c});
+    }
     std::atomic<uint64_t> next{0};
-    auto work = [&]() {
-        Bytes raw(celems * es);
+    auto run = [&]() {
+        Bytes raw;
         for (;;) {
-            const uint64_t c = next.fetch_add(1);
-            if (c >= n.nchunks) break;
-            std::fill(raw.begin(), raw.end(), 0);
-            const auto& o = n.coffs[c];
-            // copy the chunk's rows (the last dimension is contiguous)
-            const uint64_t D1 = r > 1 ? d.dims[1] : 1, D2 = r > 2 ? d.dims[2] : 1;
-            const uint64_t C1 = r > 1 ? n.cdims[1] : 1, C2 = r > 2 ? n.cdims[2] : 1;
-            const uint64_t last = d.dims[r - 1], clast = n.cdims[r - 1];
-            const uint64_t row = std::min<uint64_t>(clast, last - o[r - 1]) * es;
-            const uint64_t e0 = std::min<uint64_t>(n.cdims[0], d.dims[0] - o[0]);
-            const uint64_t e1 = r > 1 ? std::min<uint64_t>(C1, D1 - o[1]) : 1;
-            const uint64_t e2 = r > 2 ? std::min<uint64_t>(C2, D2 - o[2]) : 1;
-            const auto* src = static_cast<const uint8_t*>(d.data);
-            if (r == 1) {
-                std::memcpy(raw.data(), src + o[0] * es, row);
-            } else if (r == 2) {
-                for (uint64_t a = 0; a < e0; a++)
-                    std::memcpy(raw.data() + a * C1 * es, src + ((o[0] + a) * D1 + o[1]) * es, row);
-            } else {
-                for (uint64_t a = 0; a < e0; a++)
-                    for (uint64_t b = 0; b < e1; b++)
-                        std::memcpy(raw.data() + (a * C1 + b) * C2 * es,
-                                    src + (((o[0] + a) * D1 + o[1] + b) * D2 + o[2]) * es, row);
-            }
-            (void)e2;
-            uLongf zn = compressBound(raw.size());
-            Bytes z(zn);
-            compress2(z.data(), &zn, raw.data(), raw.size(), level);
-            z.resize(zn);
-            n.zchunks[c] = std::move(z);
+            const uint64_t k = next.fetch_add(1);
+            if (k >= work.size()) break;
+            compress_one(dn[work[k].first], work[k].second, level, raw);
         }
     };
-    const int nt = std::max(1, std::min<int>(threads, int(std::min<uint64_t>(n.nchunks, 256))));
+    const int nt = std::max(1, std::min<int>(threads, int(std::min<uint64_t>(work.size(), 1024))));
     std::vector<std::thread> pool;
-    for (int t = 1; t < nt; t++) pool.emplace_back(work);
-    work();
+    for (int t = 1; t < nt; t++) pool.emplace_back(run);
+    run();
     for (auto& t : pool) t.join();
 }
 
@@ -321,9 +336,8 @@ int write_file(const std::string& path, const std::vector<Attr>& attrs, const st
             return -1;
         }
 
-    // -- compress every chunk (threads over the chunks of each dataset)
-    for (auto& n : dn)
-        if (n.chunked) compress_chunks(n, level, threads);
+    // -- compress every chunk
+    compress_all(dn, level, threads);
 
     // -- sizes, then addresses (metadata first, raw data after)
     uint64_t at = 96;  // superblock version 0
