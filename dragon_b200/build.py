@@ -62,6 +62,7 @@ def needs_build() -> bool:
 
 def _host_stale() -> bool:
     deps = [HOST_SRC, DIST_SRC, os.path.join(ROOT, "include", "dragon", "dragon.hpp"),
+            os.path.join(ROOT, "include", "dragon", "hoard.hpp"),
             os.path.join(ROOT, "include", "dragon", "dist.hpp"), os.path.join(ROOT, "include", "dragon_gpu.h"), LIB]
     outs = list(HOST_LIBS.values()) + [os.path.join(HERE, "libdragon_dist.so"), os.path.join(HERE, "libdragon_dist_mhd.so")]
     return any(not os.path.exists(o) or any(os.path.getmtime(d) > os.path.getmtime(o) for d in deps) for o in outs)
@@ -107,8 +108,8 @@ def build_host(force: bool = False, verbose: bool = False) -> None:
     libdragon_host.so (hydro) and libdragon_host_mhd.so (built with MHD), both
     linked against libdragon_gpu.so in the same directory."""
     cxx = os.environ.get("CXX", "g++")
-    deps = [HOST_SRC, os.path.join(ROOT, "include", "dragon", "dragon.hpp"), os.path.join(ROOT, "include", "dragon_gpu.h"),
-            LIB]
+    deps = [HOST_SRC, os.path.join(ROOT, "include", "dragon", "dragon.hpp"), os.path.join(ROOT, "include", "dragon", "hoard.hpp"),
+            os.path.join(ROOT, "include", "dragon_gpu.h"), LIB]
     for flag, out in HOST_LIBS.items():
         if not force and os.path.exists(out) and all(os.path.getmtime(d) <= os.path.getmtime(out) for d in deps):
             continue

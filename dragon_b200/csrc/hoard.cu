@@ -16,6 +16,10 @@
 #include <memory>
 #include <string>
 #include <thread>
+
+#include <sys/resource.h>
+#include <sys/syscall.h>
+#include <unistd.h>
 #include <vector>
 
 #include "fluid.cuh"
@@ -321,7 +325,11 @@ int ensure_state(dragon_grid* h) {
     return 0;
 }
 
-int snapshot(dragon_grid* h, double t, int cycle, const char* path, const dragon_hoard_opts* opts, int* slot_used) {
+// background: the caller keeps stepping while the file is written, so the
+// writer and its deflate threads run at a lower scheduling priority than the
+// thread that drives the steps.
+int snapshot(dragon_grid* h, double t, int cycle, const char* path, const dragon_hoard_opts* opts, int* slot_used,
+             bool background) {
     if (!h || !path) return fail_h(DRAGON_GPU_EINVAL, "null argument");
     if (h->adv.pending) return fail_h(DRAGON_GPU_EINVAL, "an asynchronous advance is in flight");
     dragon_hoard_opts o;
@@ -361,7 +369,9 @@ int snapshot(dragon_grid* h, double t, int cycle, const char* path, const dragon
     const std::string file(path);
     const int level = o.compression, threads = o.threads;
     HoardSlot* sp = &s;
-    s.writer = std::thread([sp, P = std::move(P), file, level, threads, dev]() {
+    s.writer = std::thread([sp, P = std::move(P), file, level, threads, dev, background]() {
+        // threads created by this one (the deflate pool) inherit its nice value
+        if (background) setpriority(PRIO_PROCESS, id_t(syscall(SYS_gettid)), 10);
         cudaSetDevice(dev);
         const cudaError_t e = cudaEventSynchronize(sp->copied);
         if (e != cudaSuccess) {
@@ -423,12 +433,12 @@ void dragon_gpu_hoard_default_opts(dragon_hoard_opts* o) {
 }
 
 int dragon_gpu_hoard_write_async(dragon_grid* h, double t, int cycle, const char* path, const dragon_hoard_opts* o) {
-    return snapshot(h, t, cycle, path, o, nullptr);
+    return snapshot(h, t, cycle, path, o, nullptr, true);
 }
 
 int dragon_gpu_hoard_write(dragon_grid* h, double t, int cycle, const char* path, const dragon_hoard_opts* o) {
     int k = 0;
-    if (int rc = snapshot(h, t, cycle, path, o, &k)) return rc;
+    if (int rc = snapshot(h, t, cycle, path, o, &k, false)) return rc;
     std::string err;
     const int rc = join_slot(h->hoard->slot[k], &err);
     return rc ? fail_h(rc, err) : 0;

@@ -3,8 +3,10 @@
 // reference's MHD switch: libdragon_host.so (hydro) and, with -DMHD,
 // libdragon_host_mhd.so.
 #include "../../include/dragon/dragon.hpp"
+#include "../../include/dragon/hoard.hpp"
 
 #include <cctype>
+#include <filesystem>
 #include <cstring>
 #include <iostream>
 
@@ -412,3 +414,110 @@ Grid3D::Grid3D(int nx, int ny, int nz, double dx_, double dy_, double dz_, int g
     : Grid(3, nx, ny, nz, dx_, dy_, dz_, ghosts, cfg), dx(dx_), dy(dy_), dz(dz_) {}
 
 }  // namespace dragon
+
+// ---------------------------------------------------------------------------
+// DRAGONHOARD (DragonHoard.hpp:16-33) over dragon_gpu_hoard_*
+
+namespace DRAGONHOARD {
+namespace {
+
+dragon_hoard_opts c_opts() {
+    dragon_hoard_opts o;
+    dragon_gpu_hoard_default_opts(&o);
+    o.write_option = options.write_option;
+    o.redundant = options.redundant_vals;
+    o.compression = options.compression_level;
+    o.ghosts = options.write_ghosts ? 1 : 0;
+    o.threads = options.threads;
+    return o;
+}
+
+std::string with_ext(const std::string& f) {
+    const std::string ext = ".h5";
+    if (f.size() > ext.size() && f.compare(f.size() - ext.size(), ext.size(), ext) == 0) return f;
+    return f + ext;
+}
+
+void write(dragon::Grid& grid, double t, int cycle, const std::string& filename, bool wait) {
+    grid.sync_device();
+    const dragon_hoard_opts o = c_opts();
+    const std::string path = output_dir + "/" + filename + ".h5";
+    const int rc = wait ? dragon_gpu_hoard_write(grid.handle(), t, cycle, path.c_str(), &o)
+                        : dragon_gpu_hoard_write_async(grid.handle(), t, cycle, path.c_str(), &o);
+    if (rc) throw std::runtime_error(dragon_gpu_last_error());
+}
+
+}  // namespace
+
+void writeToFile(dragon::Grid& grid, double t, int cycle, const std::string& filename) {
+    write(grid, t, cycle, filename, true);
+}
+
+void writeToFileAsync(dragon::Grid& grid, double t, int cycle, const std::string& filename) {
+    write(grid, t, cycle, filename, false);
+}
+
+void waitForFiles(dragon::Grid& grid) {
+    if (dragon_gpu_hoard_wait(grid.handle())) throw std::runtime_error(dragon_gpu_last_error());
+}
+
+void loadFromFile(dragon::Grid& grid, double& t, int& cycle, const std::string& filename) {
+    grid.sync_device();
+    const std::string path = output_dir + "/" + with_ext(filename);
+    if (dragon_gpu_hoard_load(grid.handle(), path.c_str(), &t, &cycle)) throw std::runtime_error(dragon_gpu_last_error());
+    grid.device_changed();
+    double d[3] = {0, 0, 0};
+    const char* keys[3] = {"dx", "dy", "dz"};
+    for (int a = 0; a < 3; a++) dragon_h5_read_attr(path.c_str(), keys[a], &d[a]);
+    if (auto* g = dynamic_cast<dragon::Grid3D*>(&grid)) {
+        g->dx = d[0];
+        g->dy = d[1];
+        g->dz = d[2];
+    } else if (auto* g2 = dynamic_cast<dragon::Grid2D*>(&grid)) {
+        g2->dx = d[0];
+        g2->dy = d[1];
+    } else if (auto* g1 = dynamic_cast<dragon::Grid1D*>(&grid)) {
+        g1->dx = d[0];
+    }
+}
+
+void verifyOutputDirectory() {
+    const std::filesystem::path dir = output_dir;
+    if (std::filesystem::exists(dir)) {
+        if (!std::filesystem::is_directory(dir)) throw std::runtime_error(dir.string() + " exists but is not a directory");
+    } else {
+        std::filesystem::create_directories(dir);
+    }
+}
+
+std::string restartFileName() {
+    std::string best;
+    int best_n = -1;
+    for (const auto& e : std::filesystem::directory_iterator(output_dir)) {
+        if (!e.is_regular_file()) continue;
+        const std::string s = e.path().filename().string();
+        const size_t dot = s.rfind('.');
+        if ((dot == std::string::npos ? std::string() : s.substr(dot)) != ".h5") continue;
+        const size_t end = s.find('.');
+        const size_t pos = s.rfind('_', end);
+        if (pos == std::string::npos || pos + 1 >= end) continue;
+        bool digits = true;
+        for (size_t i = pos + 1; i < end; i++) digits = digits && std::isdigit(static_cast<unsigned char>(s[i]));
+        if (!digits) continue;
+        const int n = std::stoi(s.substr(pos + 1, end - pos - 1));
+        if (restart_frame >= 0) {
+            if (n == restart_frame) return s;
+        } else if (n > best_n) {
+            best = s;
+            best_n = n;
+        }
+    }
+    return best;
+}
+
+std::string cycle_string(int n) {
+    const char* z = n < 10 ? "0000" : n < 100 ? "000" : n < 1000 ? "00" : n < 10000 ? "0" : "";
+    return z + std::to_string(n);
+}
+
+}  // namespace DRAGONHOARD

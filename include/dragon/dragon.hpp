@@ -387,6 +387,11 @@ public:
     const AdvanceStats& last_advance() const { return stats_; }
     void upload();    // host mirror -> device now
     void download();  // device -> host mirror now
+    // For callers of the C ABI on handle(): make the device state current
+    // (host-side edits uploaded first), and record that the device state
+    // changed behind the host mirror (it refreshes on its next access).
+    void sync_device() { to_device(); }
+    void device_changed() { dev_newer_ = true; }
     int getGhosts() const { return g_; }
 
 protected:

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "dragon/dragon.hpp"
+#include "dragon/hoard.hpp"
 
 using namespace dragon;
 
@@ -204,6 +205,37 @@ __device__ void inflow(const dragon_fill_ctx& c, int i, int j, int k) {
                 out.push_back(b.z);
             }
 #endif
+    } else if (name == "hoard2d") {
+        // DRAGONHOARD from C++: run 3 steps, write a frame, restart a fresh
+        // grid (spacing 0) from the newest frame, run 3 more steps on both
+        const int nx = 64, ny = 48, g = 2;
+        cfg.riemann = 2;
+        cfg.limiter = 2;
+        Grid2D grid(nx, ny, 1.0 / nx, 1.0 / ny, g, cfg);
+        for (int i = -g; i < nx + g; i++)
+            for (int j = -g; j < ny + g; j++) grid[i, j] = state_at(in, (size_t)((i + g) * (ny + 2 * g) + (j + g)));
+        grid.boundary = Boundary::Periodic();
+        grid.advance_steps(3);
+        DRAGONHOARD::output_dir = dir + "/frames";
+        DRAGONHOARD::verifyOutputDirectory();
+        DRAGONHOARD::options.write_option = 1;
+        DRAGONHOARD::writeToFileAsync(grid, 0.25, 2, DRAGONHOARD::output_base_name + "_" + DRAGONHOARD::cycle_string(2));
+        DRAGONHOARD::writeToFile(grid, 0.5, 3, DRAGONHOARD::output_base_name + "_" + DRAGONHOARD::cycle_string(3));
+        DRAGONHOARD::waitForFiles(grid);
+        DRAGONHOARD::restart_frame = -1;
+        const std::string file = DRAGONHOARD::restartFileName();
+        Grid2D again(nx, ny, 0.0, 0.0, g, cfg);
+        double t = 0;
+        int cycle = 0;
+        DRAGONHOARD::loadFromFile(again, t, cycle, file);
+        std::printf("file %s t %.17g cycle %d dx %.17g dy %.17g\n", file.c_str(), t, cycle, again.dx, again.dy);
+        again.boundary = Boundary::Periodic();
+        grid.advance_steps(3);
+        again.advance_steps(3);
+        for (int i = -g; i < nx + g; i++)
+            for (int j = -g; j < ny + g; j++) put_state(out, grid[i, j]);
+        for (int i = -g; i < nx + g; i++)
+            for (int j = -g; j < ny + g; j++) put_state(out, again[i, j]);
     } else if (name == "blast3d") {
         const int n = 16, g = 2;
         cfg.riemann = 2;

@@ -128,6 +128,24 @@ def test_cpp_orszag_tang_mhd(host_test):
 
 
 @pytest.mark.gpu
+def test_cpp_hoard_restart(host_test):
+    """DRAGONHOARD from C++ (include/dragon/hoard.hpp): frames written through
+    writeToFileAsync / writeToFile, the newest found by restartFileName, a
+    fresh grid restarted from it: t, cycle and spacing come back, and three
+    more steps on both grids end bit for bit in the same state."""
+    rng = np.random.default_rng(21)
+    w0 = np.zeros((68, 52, 5))
+    w0[..., 0] = rng.uniform(0.5, 2.0, w0.shape[:2])
+    w0[..., 1] = rng.uniform(1.0, 2.0, w0.shape[:2])
+    w0[..., 2:4] = rng.uniform(-0.3, 0.3, w0.shape[:2] + (2,))
+    got, stdout = run_cpp(host_test, "hoard2d", [w0])
+    assert "frame_00003.h5 t 0.5 cycle 3 dx 0.015625 dy 0.020833333333333332" in stdout
+    half = got.size // 2
+    np.testing.assert_array_equal(got[half:], got[:half])
+    assert np.all(np.isfinite(got))
+
+
+@pytest.mark.gpu
 def test_cpp_blast_3d(host_test):
     if not cuda_ok():
         pytest.fail("CUDA device required")
