@@ -744,11 +744,14 @@ def hoard_report(n=1024, reps=8, intervals=(50, 250), frames=6):
             for f in range(frames):
                 G.advance_steps(every)
                 hoard.write_to_file(G, 0.0, f, f"frame_{hoard.cycle_string(f)}", wait=False)
-            hoard.wait(G)
             torch.cuda.synchronize()
-            snap = (time.perf_counter() - t0) / (frames * every) * 1e3
+            t1 = time.perf_counter()
+            hoard.wait(G)  # the last file: no steps left to hide it
+            tail = time.perf_counter() - t1
+            snap = (t1 - t0) / (frames * every) * 1e3
             out["stepping"].append({"every_steps": every, "frames": frames, "ms_per_step_no_output": base,
-                                    "ms_per_step_with_async_output": snap, "overhead": snap / base - 1.0})
+                                    "ms_per_step_with_async_output": snap, "overhead": snap / base - 1.0,
+                                    "last_file_wait_s": tail})
     finally:
         hoard.output_dir = old_dir
         G.close()

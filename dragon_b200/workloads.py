@@ -5,11 +5,15 @@ profiling and quick checks on a GPU):
     python -m dragon_b200.workloads ot      --n 512  --steps 5 [--mixed]
     python -m dragon_b200.workloads blast3d --n 128  --steps 3 [--riemann exact] [--mhd | --mixed]
     python -m dragon_b200.workloads batch   --n1d 256 --n2d 32 --steps 5 [--mixed]
+    python -m dragon_b200.workloads hoard   --n 2048 --steps 2 [--level 4]
 
 kh: 2D shear layer (HLLC, van Leer, periodic); ot: 2D MHD Orszag-Tang (HLLD,
 MC, CT, periodic); blast3d: 3D blast (MC, outflow; HLLC by default, or the
 exact solver, or MHD with a uniform field); batch: uneven 1D hydro + 2D MHD
-grids advanced by the batched step. Prints one line with steps and wall time.
+grids advanced by the batched step; hoard: the kh grid written to `steps`
+files from its device state (write option 3, deflate at --level, 0 for
+contiguous datasets) in a temporary directory. Prints one line with steps and
+wall time.
 """
 from __future__ import annotations
 
@@ -86,7 +90,7 @@ def batch(n1d, n2d, mixed=False):
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
-    ap.add_argument("workload", choices=["kh", "ot", "blast3d", "batch"])
+    ap.add_argument("workload", choices=["kh", "ot", "blast3d", "batch", "hoard"])
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--mixed", action="store_true")
@@ -94,6 +98,7 @@ def main(argv=None):
     ap.add_argument("--riemann", default="hllc", choices=["hllc", "exact", "hll", "hlle", "roe"])
     ap.add_argument("--n1d", type=int, default=256)
     ap.add_argument("--n2d", type=int, default=32)
+    ap.add_argument("--level", type=int, default=0, help="hoard: deflate level (0: contiguous)")
     a = ap.parse_args(argv)
     rs = {"hllc": _grid.RIEMANN_HLLC, "exact": _grid.RIEMANN_EXACT, "hll": _grid.RIEMANN_HLL,
           "hlle": _grid.RIEMANN_HLLE, "roe": _grid.RIEMANN_ROE}[a.riemann]
@@ -104,6 +109,22 @@ def main(argv=None):
         st = b.advance_steps(a.steps)
         print(f"batch members={len(grids)} steps={a.steps} wall_s={time.perf_counter() - t:.4f} "
               f"replay_ms={st['replay_ms']:.3f}")
+        return
+    if a.workload == "hoard":
+        import shutil
+        import tempfile
+
+        from . import hoard
+        G = kh(a.n, a.steps, False)
+        G.advance_steps(2)
+        d = tempfile.mkdtemp(prefix="hoard_")
+        hoard.output_dir = d
+        t = time.perf_counter()
+        for k in range(a.steps):
+            hoard.write_to_file(G, 0.0, k, f"frame_{hoard.cycle_string(k)}",
+                                opts=hoard.Options(compression_level=a.level))
+        print(f"hoard n={a.n} files={a.steps} wall_s={time.perf_counter() - t:.4f}")
+        shutil.rmtree(d, ignore_errors=True)
         return
     G = {"kh": lambda: kh(a.n, a.steps, a.mixed), "ot": lambda: ot(a.n, a.steps, a.mixed),
          "blast3d": lambda: blast3d(a.n, rs, a.mhd, a.mixed)}[a.workload]()
