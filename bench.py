@@ -539,6 +539,49 @@ def mixed3d_report(n=256, steps=8, warmup=2):
         G.close()
     out["mixed"]["speedup_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
     out["mixed"]["rel_l1_vs_fp64_per_field"] = [float(x) for x in problems.rel_l1(states["mixed"], states["fp64"])]
+    out["mhd"] = mixed3d_mhd_report(flush, steps=steps, warmup=warmup)
+    return out
+
+
+def mixed3d_mhd_report(flush, n=128, steps=8, warmup=2):
+    """The mixed 3D MHD step against the FP64 one: the n^3 blast (p_in 10) in
+    the uniform field (0.5, 0.3, 0.2), HLLD, MC, outflow; device time per CFL
+    step and the relative L1 per field (cells and face B) after warmup + steps
+    steps from the same initial state."""
+    import torch
+
+    import dragon_b200 as dg
+    from dragon_b200 import workloads
+
+    out = {"workload": f"3D MHD blast {n}^3, p_in 10, B (0.5, 0.3, 0.2), HLLD, MC, outflow"}
+    states = {}
+    for name, mixed in (("fp64", False), ("mixed", True)):
+        G = workloads.blast3d(n, dg.RIEMANN_HLLD, True, mixed)
+        G.advance_steps(warmup)
+        stream = torch.cuda.ExternalStream(G._lib.dragon_gpu_stream(G._h))
+        ev = []
+        torch.cuda.synchronize()
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+            G.advance_steps_async(1)
+            b.record(stream)
+            G.advance_wait()
+            ev.append((a, b))
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in ev) / steps
+        out[name] = {"ms_per_step": ms, "value": n ** 3 / (ms / 1e3), "unit": "cell-updates/s"}
+        g = G.ghosts
+        states[name] = (G.w[g:-g, g:-g, g:-g].reshape(-1, 8).copy(), G.B[g:-g, g:-g, g:-g].reshape(-1, 3).copy())
+        G.close()
+    from dragon_b200 import problems
+    out["mixed"]["speedup_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    out["mixed"]["rel_l1_vs_fp64_per_field"] = [float(x) for x in problems.rel_l1(states["mixed"][0],
+                                                                                 states["fp64"][0])]
+    out["mixed"]["rel_l1_face_B_vs_fp64"] = [float(x) for x in problems.rel_l1(states["mixed"][1], states["fp64"][1])]
     return out
 
 
@@ -921,6 +964,12 @@ def summary_of(d):
         out["mixed_3d_blast_256"] = {"fp64_value": m["fp64"]["value"], "mixed_value": m["mixed"]["value"],
                                      "mixed_speedup": m["mixed"]["speedup_vs_fp64"],
                                      "max_rel_l1_vs_fp64": max(m["mixed"]["rel_l1_vs_fp64_per_field"])}
+        if "mhd" in m:
+            h = m["mhd"]
+            out["mixed_3d_mhd_blast_128"] = {"fp64_value": h["fp64"]["value"], "mixed_value": h["mixed"]["value"],
+                                             "mixed_speedup": h["mixed"]["speedup_vs_fp64"],
+                                             "max_rel_l1_vs_fp64": max(h["mixed"]["rel_l1_vs_fp64_per_field"] +
+                                                                       h["mixed"]["rel_l1_face_B_vs_fp64"])}
     if "learned_guess" in d:
         g = d["learned_guess"]
         out["learned_guess"] = {k: g[k] for k in g if k.startswith(("iteration_reduction", "ceiling_reduction"))}

@@ -6,7 +6,7 @@ dragon_b200/libdragon_gpu.so:
     IEEE division and square root this keeps the FP64 path's arithmetic
     identical to the reference's (compiled without contraction);
   * the mixed-precision kernels (step_mixed.cu, step_mhd_mixed.cu,
-    step1d_mixed.cu, step3d_mixed.cu, batch_mixed.cu) with FMA contraction and fast
+    step1d_mixed.cu, step3d_mixed.cu, step3d_mhd_mixed.cu, batch_mixed.cu) with FMA contraction and fast
     single-precision division / square root; the division, square-root and
     denormal flags act on FP32 only, and the contraction also fuses the FP64
     arithmetic of these files (the mixed path is not held to bit parity).
@@ -29,7 +29,7 @@ BASE = ["-std=c++17", "-O3", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC", "-I" + o
 EXACT = ["--fmad=false"]
 FAST32 = ["--fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
 PER_FILE = {"step_mixed.cu": FAST32, "step_mhd_mixed.cu": FAST32, "step1d_mixed.cu": FAST32,
-            "batch_mixed.cu": FAST32, "step3d_mixed.cu": FAST32}
+            "batch_mixed.cu": FAST32, "step3d_mixed.cu": FAST32, "step3d_mhd_mixed.cu": FAST32}
 
 
 def _sources():

@@ -41,6 +41,9 @@ int launch_step3d_hydro(int solver, const Geo& G, const double* w, double* wout,
 // Mixed FP32/FP64 3D hydro step (step3d_mixed.cu): FP32 intermediates in S's planes.
 int launch_step3d_hydro_mixed(int solver, const Geo& G, const double* w, double* wout, const Hydro3DScratch& S,
                               StepCtl* ctl, const StepArgs& sa, cudaStream_t st);
+// Mixed FP32/FP64 3D MHD step (step3d_mhd_mixed.cu): FP32 half states and fluxes in S's planes.
+int launch_step3d_mhd_mixed(int solver, const Geo& G, const Geo& FG, const double* w, double* wout, const double* B,
+                            double* Bout, const Mhd3DScratch& S, StepCtl* ctl, const StepArgs& sa, cudaStream_t st);
 int launch_step3d_mhd(int solver, const Geo& G, const Geo& FG, const double* w, double* wout, const double* B,
                       double* Bout, const Mhd3DScratch& S, StepCtl* ctl, const StepArgs& sa, cudaStream_t st);
 

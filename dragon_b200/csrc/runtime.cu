@@ -260,8 +260,11 @@ int launch_step(dragon_grid* h, int c) {
                  : launch_step1d(h->mhd, h->solver, h->cg, h->w[c], h->w[c ^ 1], h->ctl, sa, h->stream);
     } else if (h->mhd) {
         if (h->dim == 3) {
-            rc = launch_step3d_mhd(h->solver, h->cg, h->fg, h->w[c], h->w[c ^ 1], h->B[c], h->B[c ^ 1], h->m3_s, h->ctl,
-                                   sa, h->stream);
+            rc = (h->cfg.precision == 1)
+                     ? launch_step3d_mhd_mixed(h->solver, h->cg, h->fg, h->w[c], h->w[c ^ 1], h->B[c], h->B[c ^ 1],
+                                               h->m3_s, h->ctl, sa, h->stream)
+                     : launch_step3d_mhd(h->solver, h->cg, h->fg, h->w[c], h->w[c ^ 1], h->B[c], h->B[c ^ 1], h->m3_s,
+                                         h->ctl, sa, h->stream);
             nk = kMhd3DKernels;
         } else if (h->cfg.precision == 1) {
             const MhdScratchF SF{(float*)h->mhd_s.hs, (float*)h->mhd_s.fx, (float*)h->mhd_s.fy, (float*)h->mhd_s.er,
@@ -743,10 +746,6 @@ int dragon_gpu_grid_create(int dim, int nx, int ny, int nz, double dx, double dy
     if (h->cfg.exact_guess == GUESS_LEARNED && !(dim == 3 && !h->mhd)) {
         delete h;
         return fail(DRAGON_GPU_EUNSUPPORTED, "the learned star-pressure guess is built for 3D hydro grids");
-    }
-    if (h->cfg.precision != 0 && dim == 3 && h->mhd) {
-        delete h;
-        return fail(DRAGON_GPU_EUNSUPPORTED, "the mixed-precision path is built for hydro grids and 1D / 2D MHD grids");
     }
     if (h->cfg.precision != 0 && h->cfg.exact_guess == GUESS_LEARNED) {
         delete h;

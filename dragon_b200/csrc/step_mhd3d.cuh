@@ -70,7 +70,7 @@ __device__ __forceinline__ bool m3_cell(long long t, int lo, int hi_incl, const 
 // K1
 // Two CTAs per SM: natural register use (132; 196 for k_m3_half) leaves one,
 // and the capped builds measured 5 % faster on the 3D MHD step.
-__global__ void __launch_bounds__(256, 2) k_m3_halfstates(Mhd3DArgs A) {
+static __global__ void __launch_bounds__(256, 2) k_m3_halfstates(Mhd3DArgs A) {
     __shared__ int s;
     if (h3_skip(A.ctl, &s)) return;
     int i, j, k;
@@ -216,7 +216,7 @@ __device__ __forceinline__ M3Faces m3_faraday(const Mhd3DArgs& A, int i, int j, 
 }
 
 // K4
-__global__ void __launch_bounds__(256, 2) k_m3_half(Mhd3DArgs A) {
+static __global__ void __launch_bounds__(256, 2) k_m3_half(Mhd3DArgs A) {
     __shared__ int s;
     if (h3_skip(A.ctl, &s)) return;
     int i, j, k;
@@ -299,7 +299,7 @@ __global__ void __launch_bounds__(256, 2) k_m3_half(Mhd3DArgs A) {
 }
 
 // K7
-__global__ void k_m3_update(Mhd3DArgs A) {
+static __global__ void k_m3_update(Mhd3DArgs A) {
     __shared__ int s;
     __shared__ double red[32];
     if (h3_skip(A.ctl, &s)) return;

@@ -3,13 +3,13 @@ profiling and quick checks on a GPU):
 
     python -m dragon_b200.workloads kh      --n 1024 --steps 5 [--mixed]
     python -m dragon_b200.workloads ot      --n 512  --steps 5 [--mixed]
-    python -m dragon_b200.workloads blast3d --n 128  --steps 3 [--riemann exact] [--mhd | --mixed]
+    python -m dragon_b200.workloads blast3d --n 128  --steps 3 [--riemann exact] [--mhd] [--mixed]
     python -m dragon_b200.workloads batch   --n1d 256 --n2d 32 --steps 5 [--mixed]
     python -m dragon_b200.workloads hoard   --n 2048 --steps 2 [--level 4]
 
 kh: 2D shear layer (HLLC, van Leer, periodic); ot: 2D MHD Orszag-Tang (HLLD,
 MC, CT, periodic); blast3d: 3D blast (MC, outflow; HLLC by default, or the
-exact solver, or MHD with a uniform field); batch: uneven 1D hydro + 2D MHD
+exact solver, or MHD with a uniform field; --mixed for either); batch: uneven 1D hydro + 2D MHD
 grids advanced by the batched step; hoard: the kh grid written to `steps`
 files from its device state (write option 3, deflate at --level, 0 for
 contiguous datasets) in a temporary directory. Prints one line with steps and
@@ -60,7 +60,9 @@ def blast3d(n, riemann, mhd, mixed=False):
     w = np.zeros(w5.shape[:-1] + (8,))
     w[..., :5] = w5
     G = _grid.Grid3D(n, n, n, d, d, d, ghosts=3, config=_grid.Config(mhd=True, riemann=_grid.RIEMANN_HLLX,
-                                                                    limiter=_grid.LIMITER_MC))
+                                                                    limiter=_grid.LIMITER_MC,
+                                                                    precision=_grid.PREC_MIXED if mixed else
+                                                                    _grid.PREC_FP64))
     G.w[...] = w
     B = G.B
     B[..., 0], B[..., 1], B[..., 2] = 0.5, 0.3, 0.2

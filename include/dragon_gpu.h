@@ -52,7 +52,7 @@ typedef struct dragon_config {
     double exact_tol;     /* ExactRiemann_Tolerance (1e-12) */
     double cfl_coeff;     /* CFL_coeff (0.3) */
     double timestep_tol;  /* Timestep_Tolerance (1e-14) */
-    int precision;        /* 0: FP64 throughout (bit-faithful), 1: mixed FP32/FP64 (all but 3D MHD) */
+    int precision;        /* 0: FP64 throughout (bit-faithful), 1: mixed FP32/FP64 */
     int exact_guess;      /* start of the exact solver's Newton iteration: 0 the reference's
                              (pL + pR) / 2 (Exact.cpp:47), 1 adaptive PVRS / two-rarefaction /
                              two-shock, 2 learned (dragon_learned.h; 3D grids), 3 a measurement

@@ -1,4 +1,4 @@
-"""The mixed FP32/FP64 1D, 2D and 3D hydro and 1D and 2D MHD paths against the FP64 oracle.
+"""The mixed FP32/FP64 1D, 2D and 3D hydro and MHD paths against the FP64 oracle.
 
 The mixed path runs reconstruction, limiters, the Riemann solves and the CTU
 corrections in FP32 while the state, every pressure recovery, the
@@ -92,9 +92,7 @@ def test_mixed_sod_strong_shock_stays_physical():
     assert np.all(np.isfinite(G.w)) and np.all(l1 <= TOL_MIXED), l1
 
 
-def test_mixed_refused_on_3d_mhd_and_learned_guess():
-    with pytest.raises(dg.grid._lib.DragonGPUError):
-        dg.Grid3D(4, 4, 4, 0.1, 0.1, 0.1, config=dg.Config(mhd=True, precision=dg.PREC_MIXED))
+def test_mixed_refused_with_the_learned_guess():
     with pytest.raises(dg.grid._lib.DragonGPUError):
         dg.Grid3D(4, 4, 4, 0.1, 0.1, 0.1, config=dg.Config(riemann=dg.RIEMANN_EXACT, exact_guess=dg.GUESS_LEARNED,
                                                            precision=dg.PREC_MIXED))
@@ -286,3 +284,94 @@ def test_mixed_orszag_tang_l1_and_divb(riemann, limiter):
     assert np.all(lb <= TOL_MIXED), lb
     assert divb_max(G.B, g, n, dx, dy) * dx < 1e-13
     assert np.any(got != ref)  # really the FP32 path
+
+
+def _mhd3d_oracle(ns, ds, riemann, limiter):
+    from oracle import port, refgrid
+    kw = dict(dim=3, n=ns, d=ds, ghosts=3, mhd=True, riemann=riemann, limiter=limiter)
+    return refgrid.RefGrid(**kw) if refgrid.available("mhd") else port.PortGrid(**kw)
+
+
+def _divb3_dx(B, g, n, ds):
+    """max |div B| * dx over the interior cells."""
+    nx, ny, nz = n
+    s = (slice(g, g + nx), slice(g, g + ny), slice(g, g + nz))
+    d = (B[g + 1:g + nx + 1, g:g + ny, g:g + nz, 0] - B[s + (0,)]) / ds[0] + \
+        (B[g:g + nx, g + 1:g + ny + 1, g:g + nz, 1] - B[s + (1,)]) / ds[1] + \
+        (B[g:g + nx, g:g + ny, g + 1:g + nz + 1, 2] - B[s + (2,)]) / ds[2]
+    return np.abs(d).max() * ds[0]
+
+
+@pytest.mark.parametrize("riemann,limiter", [(dg.RIEMANN_HLLD, dg.LIMITER_MC), (dg.RIEMANN_HLL, dg.LIMITER_MINMOD),
+                                             (dg.RIEMANN_HLLE, dg.LIMITER_VANLEER)])
+def test_mixed_3d_mhd_blast_vs_fp64_oracle(riemann, limiter):
+    """The mixed 3D MHD step (FP32 half states, corrections and solves; FP64
+    edge E, Faraday and update) within the bar of the FP64 oracle on a 14^3
+    blast in a uniform oblique field (outflow, a seeded velocity field), face B
+    included, with div B at FP64 roundoff."""
+    n, g = 14, 3
+    w5, d = problems.blast_3d(n, ghosts=g, p_in=10.0)
+    w = np.zeros(w5.shape[:-1] + (8,))
+    w[..., :5] = w5
+    w[..., 0] = np.where(w[..., 0] > 0, w[..., 0], 1.0)
+    w[..., 1] = np.where(w[..., 1] > 0, w[..., 1], 0.1)
+    w[..., 2:5] = np.random.default_rng(riemann).uniform(-0.1, 0.1, w.shape[:-1] + (3,))
+    B = np.zeros((n + 1 + 2 * g,) * 3 + (3,))
+    B[..., 0], B[..., 1], B[..., 2] = 0.5, 0.3, 0.2
+    ds = (d, d * 1.2, d * 0.9)
+    G = dg.Grid3D(n, n, n, *ds, ghosts=g, config=dg.Config(mhd=True, riemann=riemann, limiter=limiter,
+                                                            precision=dg.PREC_MIXED))
+    R = _mhd3d_oracle((n, n, n), ds, riemann, limiter)
+    G.w[...] = w
+    G.B[...] = B
+    R.set_prim(w)
+    R.set_faceB(B)
+    G.initialize_B_fields()
+    R.initialize_B_fields()
+    for _ in range(5):
+        R.step_cfl()
+    res = G.advance_steps(5)
+    assert res.steps == 5
+    sl = (slice(g, -g),) * 3
+    got, ref = G.w[sl].reshape(-1, 8), R.get_prim()[sl].reshape(-1, 8)
+    assert np.any(got != ref)  # really the FP32 path
+    l1 = problems.rel_l1(got, ref)
+    assert np.all(l1 <= TOL_MIXED), l1
+    lb = problems.rel_l1(G.B[sl].reshape(-1, 3), R.get_faceB()[sl].reshape(-1, 3))
+    assert np.all(lb <= TOL_MIXED), lb
+    assert _divb3_dx(G.B, g, (n, n, n), ds) < 1e-13
+
+
+def test_mixed_3d_mhd_random_periodic_vs_fp64_oracle():
+    """Random states in a perturbed field on a ragged periodic 7 x 8 x 6 grid:
+    every field and face B within the bar after three steps."""
+    ns, g = (7, 8, 6), 3
+    rng = np.random.default_rng(17)
+    shape = tuple(x + 2 * g for x in ns)
+    w = np.zeros(shape + (8,))
+    w[..., 0] = 10 ** rng.uniform(-0.3, 0.3, shape)
+    w[..., 1] = 10 ** rng.uniform(-0.3, 0.3, shape)
+    w[..., 2:5] = rng.uniform(-0.3, 0.3, shape + (3,))
+    B = np.zeros(tuple(x + 1 + 2 * g for x in ns) + (3,))
+    B[..., 0], B[..., 1], B[..., 2] = 0.3, -0.2, 0.1
+    B += rng.uniform(-0.01, 0.01, B.shape)
+    ds = (0.1, 0.12, 0.09)
+    G = dg.Grid3D(*ns, *ds, ghosts=g, config=dg.Config(mhd=True, riemann=dg.RIEMANN_HLLD, limiter=dg.LIMITER_MC,
+                                                                precision=dg.PREC_MIXED))
+    R = _mhd3d_oracle(ns, ds, dg.RIEMANN_HLLD, dg.LIMITER_MC)
+    G.w[...] = w
+    G.B[...] = B
+    R.set_prim(w)
+    R.set_faceB(B)
+    G.boundary = dg.Periodic()
+    R.set_boundary([(dg.boundary.PERIODIC, 63, 1, None)])
+    G.initialize_B_fields()
+    R.initialize_B_fields()
+    for _ in range(3):
+        R.step_cfl()
+    assert G.advance_steps(3).steps == 3
+    sl = (slice(g, -g),) * 3
+    l1 = problems.rel_l1(G.w[sl].reshape(-1, 8), R.get_prim()[sl].reshape(-1, 8))
+    assert np.all(l1 <= TOL_MIXED), l1
+    lb = problems.rel_l1(G.B[sl].reshape(-1, 3), R.get_faceB()[sl].reshape(-1, 3))
+    assert np.all(lb <= TOL_MIXED), lb
