@@ -231,6 +231,12 @@ SIGNATURES = {
     "dragon_gpu_hoard_wait": (ctypes.c_int, [ctypes.c_void_p]),
     "dragon_gpu_hoard_load": (
         ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, c_double_p, ctypes.POINTER(ctypes.c_int)]),
+    "dragon_hoard_write_host": (
+        ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                       c_double_p, ctypes.c_double, ctypes.c_int, c_double_p, c_double_p, ctypes.POINTER(HoardOpts)]),
+    "dragon_hoard_load_host": (
+        ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                       c_double_p, c_double_p, c_double_p, ctypes.POINTER(ctypes.c_int), c_double_p]),
     "dragon_h5_write": (
         ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(H5Attr), ctypes.c_int, ctypes.POINTER(H5Dataset), ctypes.c_int,
                        ctypes.c_int, ctypes.c_int]),

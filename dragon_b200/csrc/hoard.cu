@@ -164,7 +164,22 @@ struct Plan {
     int sh = 0;              // device index shift: g without ghosts, 0 with them
 };
 
-int make_plan(const dragon_grid* h, double t, int cycle, const dragon_hoard_opts& o, Plan* P) {
+// What the file layout depends on: the grid's dimension, extents, ghost
+// width (of the padded arrays), spacing and physics.
+struct Shape {
+    int dim;
+    int n[3];
+    int g;
+    double d[3];
+    bool mhd;
+};
+
+Shape shape_of(const dragon_grid* h) {
+    return Shape{h->dim, {h->n[0], h->n[1], h->n[2]}, h->g, {h->d[0], h->d[1], h->d[2]}, h->mhd};
+}
+
+int make_plan(const Shape& h_, double t, int cycle, const dragon_hoard_opts& o, Plan* P) {
+    const Shape* h = &h_;
     const int opt = o.write_option, red = o.redundant;
     // HDF5Output.cpp:21-30: which representations the option writes
     const bool prims = opt & 1;
@@ -336,7 +351,7 @@ int snapshot(dragon_grid* h, double t, int cycle, const char* path, const dragon
     if (opts) o = *opts;
     else dragon_gpu_hoard_default_opts(&o);
     Plan P;
-    if (int rc = make_plan(h, t, cycle, o, &P)) return rc;
+    if (int rc = make_plan(shape_of(h), t, cycle, o, &P)) return rc;
     if (int rc = ensure_state(h)) return rc;
     HoardState* S = h->hoard;
     const int k = S->next;
@@ -403,6 +418,199 @@ int snapshot(dragon_grid* h, double t, int cycle, const char* path, const dragon
 
 }  // namespace
 
+namespace {
+
+// The datasets of plan P from host arrays in the reference's layout (prim:
+// the padded cells, nf values each; faceB: the padded faces, 3 values each),
+// the same values k_hoard_pack computes, into out (P.total bytes).
+void host_pack(const Shape& S, const Plan& P, const double* prim, const double* faceB, char* out) {
+    const int nf = S.mhd ? 8 : 5, dim = S.dim, g = S.g;
+    for (const auto& ds : P.ds) {
+        const int fc = ds.face ? 1 : 0;
+        int X[3] = {1, 1, 1};  // padded extents of the source array
+        for (int a = 0; a < dim; a++) X[a] = S.n[a] + fc + 2 * g;
+        const int NX = P.ext[0] + fc, NY = dim > 1 ? P.ext[1] + fc : 1, NZ = dim > 2 ? P.ext[2] + fc : 1;
+        const PackItem& it = ds.item;
+        long long e = 0;
+        for (int z = 0; z < NZ; z++)
+            for (int y = 0; y < NY; y++)
+                for (int x = 0; x < NX; x++, e++) {
+                    const size_t c = (size_t(x + P.sh) * X[1] + (dim > 1 ? y + P.sh : 0)) * X[2] + (dim > 2 ? z + P.sh : 0);
+                    double v;
+                    if (ds.face) {
+                        v = faceB[c * 3 + it.arg];
+                    } else {
+                        const double* w = prim + c * nf;
+                        if (it.kind == PK_MOM) {
+                            v = w[2 + it.arg] * w[0];
+                        } else if (it.kind == PK_ENERGY) {
+                            Prim<double> q{w[0], w[1], w[2], w[3], w[4], 0, 0, 0};
+                            if (S.mhd) {
+                                q.Bx = w[5];
+                                q.By = w[6];
+                                q.Bz = w[7];
+                            }
+                            v = S.mhd ? energy<true>(q) : energy<false>(q);
+                        } else {
+                            v = w[it.arg];
+                        }
+                    }
+                    if (it.f32) reinterpret_cast<float*>(out + it.off)[e] = (float)v;
+                    else reinterpret_cast<double*>(out + it.off)[e] = v;
+                }
+    }
+}
+
+// Restart of host arrays in the reference's layout (W: the padded cells, nf
+// values each; FB: the padded faces, 3 values each, MHD 2D / 3D): checks the
+// file against the shape and overwrites the cells and faces of the file's
+// range as HDF5Restart.cpp:61-377 does; the others keep their values.
+int load_into(const Shape& S, const char* path, double* W, double* FB, double* t, int* cycle, double* d_out) {
+    const int nf = S.mhd ? 8 : 5;
+    hoard::File F;
+    std::string err;
+    if (!F.open(path, &err)) return fail_h(DRAGON_GPU_EINVAL, err);
+    auto geti = [&](const char* k, int* v) {
+        double x;
+        if (!F.attr(k, &x, &err)) return false;
+        *v = int(x);
+        return true;
+    };
+    auto getd = [&](const char* k, double* v) { return F.attr(k, v, &err); };
+    int fmt, dim, mhd, ng, wopt, cyc;
+    if (!geti("format_version", &fmt)) return fail_h(DRAGON_GPU_EINVAL, err);
+    if (fmt > 1) return fail_h(DRAGON_GPU_EINVAL, "Please update to the latest version of DRAGON to read this file");
+    if (!geti("dim", &dim)) return fail_h(DRAGON_GPU_EINVAL, err);
+    if (dim != S.dim)
+        return fail_h(DRAGON_GPU_EINVAL, "Expected " + std::to_string(S.dim) + (S.dim == 1 ? " dimension" : " dimensions") +
+                                             " but got " + std::to_string(dim));
+    if (!geti("MHD", &mhd)) return fail_h(DRAGON_GPU_EINVAL, err);
+    if (mhd && !S.mhd) return fail_h(DRAGON_GPU_EINVAL, "File was saved using MHD. Please enable MHD in Config.h");
+    const char* nk[3] = {"nx", "ny", "nz"};
+    const char* dk[3] = {"dx", "dy", "dz"};
+    int n[3] = {1, 1, 1};
+    double d[3] = {0, 0, 0};
+    for (int a = 0; a < dim; a++)
+        if (!geti(nk[a], &n[a])) return fail_h(DRAGON_GPU_EINVAL, err);
+    for (int a = 0; a < dim; a++)
+        if (n[a] != S.n[a]) return fail_h(DRAGON_GPU_EINVAL, "File size does not match the grid size");
+    if (!geti("ng", &ng)) return fail_h(DRAGON_GPU_EINVAL, err);
+    ng = std::min(ng, S.g);
+    for (int a = 0; a < dim; a++)
+        if (!getd(dk[a], &d[a])) return fail_h(DRAGON_GPU_EINVAL, err);
+    double tt;
+    if (!getd("time", &tt) || !geti("cycle", &cyc) || !geti("write_option", &wopt)) return fail_h(DRAGON_GPU_EINVAL, err);
+
+    // the file's range: cells i in [-ng, n + ng) per axis, flattened x fastest
+    int E[3] = {1, 1, 1};
+    for (int a = 0; a < dim; a++) E[a] = n[a] + 2 * ng;
+    const size_t cells = size_t(E[0]) * E[1] * E[2];
+    const size_t faces = size_t(E[0] + 1) * (dim > 1 ? E[1] + 1 : 1) * (dim > 2 ? E[2] + 1 : 1);
+    auto need = [&](const char* key, size_t count, std::vector<double>* v, bool zero_if_missing) {
+        if (!F.has(key)) {
+            if (zero_if_missing) {
+                v->assign(count, 0.0);
+                return true;
+            }
+            err = std::string("no dataset ") + key;
+            return false;
+        }
+        if (!F.read(key, v, &err)) return false;
+        if (v->size() < count) {
+            err = std::string(key) + " is smaller than the grid range it loads";
+            return false;
+        }
+        return true;
+    };
+    std::vector<double> rho, p, vx, vy, vz, Eg, px, py, pz, bx, by, bz, fx, fy, fz;
+    if (!need("/fluid/rho", cells, &rho, false)) return fail_h(DRAGON_GPU_EINVAL, err);
+    const bool cellB = S.mhd && mhd;
+    if (cellB) {
+        // HDF5Restart.cpp: 1D requires cell B; 2D / 3D read zeros where it is absent
+        const bool zmiss = dim > 1;
+        if (!need("/fluid/B/x", cells, &bx, zmiss) || !need("/fluid/B/y", cells, &by, zmiss) ||
+            !need("/fluid/B/z", cells, &bz, zmiss))
+            return fail_h(DRAGON_GPU_EINVAL, err);
+        if (dim > 1 && (!need("/fluid/Bf/x", faces, &fx, true) || !need("/fluid/Bf/y", faces, &fy, true) ||
+                        !need("/fluid/Bf/z", faces, &fz, true)))
+            return fail_h(DRAGON_GPU_EINVAL, err);
+    }
+    const bool from_prim = wopt & 1;
+    if (from_prim) {
+        if (!need("/fluid/p", cells, &p, false) || !need("/fluid/v/x", cells, &vx, false) ||
+            !need("/fluid/v/y", cells, &vy, false) || !need("/fluid/v/z", cells, &vz, false))
+            return fail_h(DRAGON_GPU_EINVAL, err);
+    } else {
+        if (!need("/fluid/E", cells, &Eg, false) || !need("/fluid/momentum/x", cells, &px, false) ||
+            !need("/fluid/momentum/y", cells, &py, false) || !need("/fluid/momentum/z", cells, &pz, false))
+            return fail_h(DRAGON_GPU_EINVAL, err);
+    }
+
+    const bool has_faces = S.mhd && dim > 1;
+    const int g = S.g;
+    int X[3] = {1, 1, 1}, XF[3] = {1, 1, 1};
+    for (int a = 0; a < dim; a++) {
+        X[a] = S.n[a] + 2 * g;
+        XF[a] = S.n[a] + 1 + 2 * g;
+    }
+    auto cell_at = [&](int i, int j, int k) {
+        return ((size_t(i + g) * X[1] + (dim > 1 ? j + g : 0)) * X[2] + (dim > 2 ? k + g : 0)) * nf;
+    };
+    const int jlo = dim > 1 ? -ng : 0, jhi = dim > 1 ? n[1] + ng : 1;
+    const int klo = dim > 2 ? -ng : 0, khi = dim > 2 ? n[2] + ng : 1;
+    for (int k = klo; k < khi; k++)
+        for (int j = jlo; j < jhi; j++)
+            for (int i = -ng; i < n[0] + ng; i++) {
+                const size_t f = (size_t(k - klo) * E[1] + (j - jlo)) * E[0] + (i + ng);
+                double* w = W + cell_at(i, j, k);
+                w[0] = rho[f];
+                if (S.mhd) {
+                    w[5] = cellB ? bx[f] : 0.0;
+                    w[6] = cellB ? by[f] : 0.0;
+                    w[7] = cellB ? bz[f] : 0.0;
+                }
+                if (from_prim) {
+                    w[1] = p[f];
+                    w[2] = vx[f];
+                    w[3] = vy[f];
+                    w[4] = vz[f];
+                } else {
+                    Cons<double> U;
+                    U.rho = w[0];
+                    U.mx = px[f];
+                    U.my = py[f];
+                    U.mz = pz[f];
+                    U.E = Eg[f];
+                    U.Bx = S.mhd ? w[5] : 0.0;
+                    U.By = S.mhd ? w[6] : 0.0;
+                    U.Bz = S.mhd ? w[7] : 0.0;
+                    const Prim<double> q = S.mhd ? to_prim<true>(U) : to_prim<false>(U);
+                    w[1] = q.p;
+                    w[2] = q.vx;
+                    w[3] = q.vy;
+                    w[4] = q.vz;
+                }
+            }
+    if (has_faces) {
+        const int kfhi = dim > 2 ? n[2] + ng : 0;
+        for (int k = klo; k <= kfhi; k++)
+            for (int j = -ng; j <= n[1] + ng; j++)
+                for (int i = -ng; i <= n[0] + ng; i++) {
+                    const size_t f = (size_t(k - klo) * (E[1] + 1) + (j + ng)) * (E[0] + 1) + (i + ng);
+                    const size_t at = ((size_t(i + g) * XF[1] + (j + g)) * XF[2] + (dim > 2 ? k + g : 0)) * 3;
+                    FB[at + 0] = cellB ? fx[f] : 0.0;
+                    FB[at + 1] = cellB ? fy[f] : 0.0;
+                    FB[at + 2] = cellB ? fz[f] : 0.0;
+                }
+    }
+    for (int a = 0; a < 3; a++) d_out[a] = a < dim ? d[a] : 0.0;
+    *t = tt;
+    *cycle = cyc;
+    return 0;
+}
+
+}  // namespace
+
 namespace dgpu_rt {
 void hoard_release(dragon_grid* h) {
     HoardState* S = h->hoard;
@@ -430,6 +638,36 @@ void dragon_gpu_hoard_default_opts(dragon_hoard_opts* o) {
     o->compression = 4;   // HDF5_COMPRESSION_LEVEL
     o->ghosts = 0;
     o->threads = 0;
+}
+
+int dragon_hoard_write_host(const char* path, int dim, int mhd, const int* n3, int ghosts, const double* d3, double t,
+                            int cycle, const double* prim, const double* faceB, const dragon_hoard_opts* opts) {
+    if (!path || !n3 || !d3 || !prim || dim < 1 || dim > 3 || ghosts < 0 || (mhd && dim > 1 && !faceB))
+        return fail_h(DRAGON_GPU_EINVAL, "invalid argument");
+    Shape S{dim, {n3[0], dim > 1 ? n3[1] : 1, dim > 2 ? n3[2] : 1}, ghosts,
+            {d3[0], dim > 1 ? d3[1] : 0.0, dim > 2 ? d3[2] : 0.0}, mhd != 0};
+    for (int a = 0; a < dim; a++)
+        if (S.n[a] < 1) return fail_h(DRAGON_GPU_EINVAL, "invalid extents");
+    dragon_hoard_opts o;
+    if (opts) o = *opts;
+    else dragon_gpu_hoard_default_opts(&o);
+    Plan P;
+    if (int rc = make_plan(S, t, cycle, o, &P)) return rc;
+    std::vector<char> buf(P.total);
+    host_pack(S, P, prim, faceB, buf.data());
+    std::vector<hoard::Dataset> ds;
+    for (const auto& d : P.ds) {
+        hoard::Dataset x;
+        x.path = d.path;
+        x.rank = d.rank;
+        for (int a = 0; a < 3; a++) x.dims[a] = d.dims[a];
+        x.type = d.type;
+        x.data = buf.data() + d.off;
+        ds.push_back(x);
+    }
+    std::string err;
+    if (hoard::write_file(path, P.attrs, ds, o.compression, o.threads, &err)) return fail_h(DRAGON_GPU_EINVAL, err);
+    return 0;
 }
 
 int dragon_gpu_hoard_write_async(dragon_grid* h, double t, int cycle, const char* path, const dragon_hoard_opts* o) {
@@ -460,159 +698,29 @@ int dragon_gpu_hoard_wait(dragon_grid* h) {
 int dragon_gpu_hoard_load(dragon_grid* h, const char* path, double* t, int* cycle) {
     if (!h || !path || !t || !cycle) return fail_h(DRAGON_GPU_EINVAL, "null argument");
     if (h->adv.pending) return fail_h(DRAGON_GPU_EINVAL, "an asynchronous advance is in flight");
-    hoard::File F;
-    std::string err;
-    if (!F.open(path, &err)) return fail_h(DRAGON_GPU_EINVAL, err);
-    auto geti = [&](const char* k, int* v) {
-        double x;
-        if (!F.attr(k, &x, &err)) return false;
-        *v = int(x);
-        return true;
-    };
-    auto getd = [&](const char* k, double* v) { return F.attr(k, v, &err); };
-    int fmt, dim, mhd, ng, wopt, cyc;
-    if (!geti("format_version", &fmt)) return fail_h(DRAGON_GPU_EINVAL, err);
-    if (fmt > 1) return fail_h(DRAGON_GPU_EINVAL, "Please update to the latest version of DRAGON to read this file");
-    if (!geti("dim", &dim)) return fail_h(DRAGON_GPU_EINVAL, err);
-    if (dim != h->dim)
-        return fail_h(DRAGON_GPU_EINVAL, "Expected " + std::to_string(h->dim) + (h->dim == 1 ? " dimension" : " dimensions") +
-                                             " but got " + std::to_string(dim));
-    if (!geti("MHD", &mhd)) return fail_h(DRAGON_GPU_EINVAL, err);
-    if (mhd && !h->mhd) return fail_h(DRAGON_GPU_EINVAL, "File was saved using MHD. Please enable MHD in Config.h");
-    const char* nk[3] = {"nx", "ny", "nz"};
-    const char* dk[3] = {"dx", "dy", "dz"};
-    int n[3] = {1, 1, 1};
-    double d[3] = {0, 0, 0};
-    for (int a = 0; a < dim; a++)
-        if (!geti(nk[a], &n[a])) return fail_h(DRAGON_GPU_EINVAL, err);
-    for (int a = 0; a < dim; a++)
-        if (n[a] != h->n[a]) return fail_h(DRAGON_GPU_EINVAL, "File size does not match the grid size");
-    if (!geti("ng", &ng)) return fail_h(DRAGON_GPU_EINVAL, err);
-    ng = std::min(ng, h->g);
-    for (int a = 0; a < dim; a++)
-        if (!getd(dk[a], &d[a])) return fail_h(DRAGON_GPU_EINVAL, err);
-    double tt;
-    if (!getd("time", &tt) || !geti("cycle", &cyc) || !geti("write_option", &wopt)) return fail_h(DRAGON_GPU_EINVAL, err);
-
-    // the file's range: cells i in [-ng, n + ng) per axis, flattened x fastest
-    int E[3] = {1, 1, 1};
-    for (int a = 0; a < dim; a++) E[a] = n[a] + 2 * ng;
-    const size_t cells = size_t(E[0]) * E[1] * E[2];
-    const size_t faces = size_t(E[0] + 1) * (dim > 1 ? E[1] + 1 : 1) * (dim > 2 ? E[2] + 1 : 1);
-    auto need = [&](const char* key, size_t count, std::vector<double>* v, bool zero_if_missing) {
-        if (!F.has(key)) {
-            if (zero_if_missing) {
-                v->assign(count, 0.0);
-                return true;
-            }
-            err = std::string("no dataset ") + key;
-            return false;
-        }
-        if (!F.read(key, v, &err)) return false;
-        if (v->size() < count) {
-            err = std::string(key) + " is smaller than the grid range it loads";
-            return false;
-        }
-        return true;
-    };
-    std::vector<double> rho, p, vx, vy, vz, Eg, px, py, pz, bx, by, bz, fx, fy, fz;
-    if (!need("/fluid/rho", cells, &rho, false)) return fail_h(DRAGON_GPU_EINVAL, err);
-    const bool cellB = h->mhd && mhd;
-    if (cellB) {
-        // HDF5Restart.cpp: 1D requires cell B; 2D / 3D read zeros where it is absent
-        const bool zmiss = dim > 1;
-        if (!need("/fluid/B/x", cells, &bx, zmiss) || !need("/fluid/B/y", cells, &by, zmiss) ||
-            !need("/fluid/B/z", cells, &bz, zmiss))
-            return fail_h(DRAGON_GPU_EINVAL, err);
-        if (dim > 1 && (!need("/fluid/Bf/x", faces, &fx, true) || !need("/fluid/Bf/y", faces, &fy, true) ||
-                        !need("/fluid/Bf/z", faces, &fz, true)))
-            return fail_h(DRAGON_GPU_EINVAL, err);
-    }
-    const bool from_prim = wopt & 1;
-    if (from_prim) {
-        if (!need("/fluid/p", cells, &p, false) || !need("/fluid/v/x", cells, &vx, false) ||
-            !need("/fluid/v/y", cells, &vy, false) || !need("/fluid/v/z", cells, &vz, false))
-            return fail_h(DRAGON_GPU_EINVAL, err);
-    } else {
-        if (!need("/fluid/E", cells, &Eg, false) || !need("/fluid/momentum/x", cells, &px, false) ||
-            !need("/fluid/momentum/y", cells, &py, false) || !need("/fluid/momentum/z", cells, &pz, false))
-            return fail_h(DRAGON_GPU_EINVAL, err);
-    }
-
     // current state (reference order, dense padded): cells outside the file's
     // range keep their values
-    const int nf = h->nf;
-    std::vector<double> W(dragon_gpu_prim_count(h));
+    std::vector<double> W(dragon_gpu_prim_count(h)), FB(dragon_gpu_faceB_count(h));
     if (int rc = dragon_gpu_download_prim(h, W.data())) return rc;
-    std::vector<double> FB;
-    const bool has_faces = h->mhd && dim > 1;
-    if (has_faces) {
-        FB.resize(dragon_gpu_faceB_count(h));
+    if (!FB.empty())
         if (int rc = dragon_gpu_download_faceB(h, FB.data())) return rc;
-    }
-    const int g = h->g;
-    int X[3] = {1, 1, 1}, XF[3] = {1, 1, 1};
-    for (int a = 0; a < dim; a++) {
-        X[a] = h->n[a] + 2 * g;
-        XF[a] = h->n[a] + 1 + 2 * g;
-    }
-    auto cell_at = [&](int i, int j, int k) {
-        return ((size_t(i + g) * X[1] + (dim > 1 ? j + g : 0)) * X[2] + (dim > 2 ? k + g : 0)) * nf;
-    };
-    const int jlo = dim > 1 ? -ng : 0, jhi = dim > 1 ? n[1] + ng : 1;
-    const int klo = dim > 2 ? -ng : 0, khi = dim > 2 ? n[2] + ng : 1;
-    for (int k = klo; k < khi; k++)
-        for (int j = jlo; j < jhi; j++)
-            for (int i = -ng; i < n[0] + ng; i++) {
-                const size_t f = (size_t(k - klo) * E[1] + (j - jlo)) * E[0] + (i + ng);
-                double* w = W.data() + cell_at(i, j, k);
-                w[0] = rho[f];
-                if (h->mhd) {
-                    w[5] = cellB ? bx[f] : 0.0;
-                    w[6] = cellB ? by[f] : 0.0;
-                    w[7] = cellB ? bz[f] : 0.0;
-                }
-                if (from_prim) {
-                    w[1] = p[f];
-                    w[2] = vx[f];
-                    w[3] = vy[f];
-                    w[4] = vz[f];
-                } else {
-                    Cons<double> U;
-                    U.rho = w[0];
-                    U.mx = px[f];
-                    U.my = py[f];
-                    U.mz = pz[f];
-                    U.E = Eg[f];
-                    U.Bx = h->mhd ? w[5] : 0.0;
-                    U.By = h->mhd ? w[6] : 0.0;
-                    U.Bz = h->mhd ? w[7] : 0.0;
-                    const Prim<double> q = h->mhd ? to_prim<true>(U) : to_prim<false>(U);
-                    w[1] = q.p;
-                    w[2] = q.vx;
-                    w[3] = q.vy;
-                    w[4] = q.vz;
-                }
-            }
-    if (has_faces) {
-        const int kfhi = dim > 2 ? n[2] + ng : 0;
-        for (int k = klo; k <= kfhi; k++)
-            for (int j = -ng; j <= n[1] + ng; j++)
-                for (int i = -ng; i <= n[0] + ng; i++) {
-                    const size_t f = (size_t(k - klo) * (E[1] + 1) + (j + ng)) * (E[0] + 1) + (i + ng);
-                    const size_t at = ((size_t(i + g) * XF[1] + (j + g)) * XF[2] + (dim > 2 ? k + g : 0)) * 3;
-                    FB[at + 0] = cellB ? fx[f] : 0.0;
-                    FB[at + 1] = cellB ? fy[f] : 0.0;
-                    FB[at + 2] = cellB ? fz[f] : 0.0;
-                }
-    }
-    for (int a = 0; a < dim; a++) h->d[a] = d[a];
+    double d[3];
+    if (int rc = load_into(shape_of(h), path, W.data(), FB.empty() ? nullptr : FB.data(), t, cycle, d)) return rc;
+    for (int a = 0; a < h->dim; a++) h->d[a] = d[a];
     if (int rc = dragon_gpu_upload_prim(h, W.data())) return rc;
-    if (has_faces)
+    if (!FB.empty())
         if (int rc = dragon_gpu_upload_faceB(h, FB.data())) return rc;
-    *t = tt;
-    *cycle = cyc;
     return 0;
+}
+
+int dragon_hoard_load_host(const char* path, int dim, int mhd, const int* n3, int ghosts, double* prim, double* faceB,
+                           double* t, int* cycle, double* d3) {
+    if (!path || !n3 || !prim || !t || !cycle || !d3 || dim < 1 || dim > 3 || ghosts < 0 || (mhd && dim > 1 && !faceB))
+        return fail_h(DRAGON_GPU_EINVAL, "invalid argument");
+    Shape S{dim, {n3[0], dim > 1 ? n3[1] : 1, dim > 2 ? n3[2] : 1}, ghosts, {0, 0, 0}, mhd != 0};
+    for (int a = 0; a < dim; a++)
+        if (S.n[a] < 1) return fail_h(DRAGON_GPU_EINVAL, "invalid extents");
+    return load_into(S, path, prim, faceB, t, cycle, d3);
 }
 
 int dragon_h5_write(const char* file, const dragon_h5_attr* attrs, int nattrs, const dragon_h5_dataset* dsets,

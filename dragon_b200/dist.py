@@ -228,6 +228,7 @@ class _DistBase:
         self.rank = tdist.get_rank(group)
         self.parts = tdist.get_world_size(group)
         self.N = tuple(int(x) for x in n)
+        self.d = tuple(float(x) for x in d)
         self.ghosts = valid_ghosts(ghosts, self.config.mhd)
         g = self.ghosts
         sizes = [child_size(self.N[0], self.parts, r) for r in range(self.parts)]

@@ -111,9 +111,21 @@ def restart_file_name(restart_frame: int = 0) -> str:
     return best
 
 
+def _is_dist(grid) -> bool:
+    from . import dist
+    return isinstance(grid, dist._DistBase)
+
+
 def write_to_file(grid, t: float, cycle: int, filename: str, wait: bool = True, opts: Options | None = None) -> None:
     """DRAGONHOARD::writeToFile(grid, t, cycle, filename): writes
-    ``output_dir + "/" + filename + ".h5"`` from the grid's device state."""
+    ``output_dir + "/" + filename + ".h5"`` from the grid's device state.
+
+    For a distributed grid (dragon_b200.dist) every rank calls it: the slabs
+    are gathered, rank 0 writes the file of the whole grid, and the call
+    returns on every rank once the file is complete (``wait`` is ignored)."""
+    if _is_dist(grid):
+        _write_dist(grid, t, cycle, _path(filename) + FILE_EXT, opts or options)
+        return
     lib = grid._lib
     grid._to_device()
     o = (opts or options).to_c()
@@ -130,7 +142,12 @@ def wait(grid) -> None:
 def load_from_file(grid, filename: str) -> tuple[float, int]:
     """DRAGONHOARD::loadFromFile(grid, t, cycle, filename): restarts ``grid``
     from ``output_dir + "/" + filename`` (".h5" appended when missing); returns
-    (t, cycle). The grid's spacing becomes the file's."""
+    (t, cycle). The grid's spacing becomes the file's.
+
+    A distributed grid restarts on every rank from the same file (each rank
+    reads it); its spacing must equal the file's."""
+    if _is_dist(grid):
+        return _load_dist(grid, _path(_with_ext(filename)))
     lib = grid._lib
     grid._to_device()
     path = (_path(_with_ext(filename))).encode()
@@ -143,6 +160,60 @@ def load_from_file(grid, filename: str) -> tuple[float, int]:
         _lib.check(lib.dragon_h5_read_attr(path, k.encode(), ctypes.byref(v)))
         setattr(grid, k, v.value)
     return t.value, cyc.value
+
+
+def write_arrays(path: str, dim: int, mhd: bool, n, ghosts: int, d, t: float, cycle: int, w: np.ndarray,
+                 B: np.ndarray | None = None, opts: Options | None = None) -> None:
+    """The file writeToFile writes, from host arrays of a grid (w: the padded
+    cell array, fields last; B: the padded face array of an MHD 2D / 3D grid)."""
+    lib = _lib.load()
+    n3 = (ctypes.c_int * 3)(*(list(n) + [1] * (3 - len(n))))
+    d3 = (ctypes.c_double * 3)(*(list(d) + [0.0] * (3 - len(d))))
+    wa = np.ascontiguousarray(w, dtype=np.float64)
+    Ba = None if B is None else np.ascontiguousarray(B, dtype=np.float64)
+    o = (opts or options).to_c()
+    _lib.check(lib.dragon_hoard_write_host(path.encode(), int(dim), int(bool(mhd)), n3, int(ghosts), d3, float(t),
+                                           int(cycle), wa.ctypes.data_as(_lib.c_double_p),
+                                           None if Ba is None else Ba.ctypes.data_as(_lib.c_double_p), ctypes.byref(o)))
+
+
+def load_arrays(path: str, dim: int, mhd: bool, n, ghosts: int, w: np.ndarray, B: np.ndarray | None = None):
+    """loadFromFile into host arrays of a grid (modified in place: C-contiguous
+    float64); returns (t, cycle, spacing)."""
+    lib = _lib.load()
+    n3 = (ctypes.c_int * 3)(*(list(n) + [1] * (3 - len(n))))
+    for a in (w, B):
+        if a is not None and (a.dtype != np.float64 or not a.flags.c_contiguous):
+            raise ValueError("arrays must be C-contiguous float64")
+    t = ctypes.c_double()
+    cyc = ctypes.c_int()
+    d3 = (ctypes.c_double * 3)()
+    _lib.check(lib.dragon_hoard_load_host(path.encode(), int(dim), int(bool(mhd)), n3, int(ghosts),
+                                          w.ctypes.data_as(_lib.c_double_p),
+                                          None if B is None else B.ctypes.data_as(_lib.c_double_p), ctypes.byref(t),
+                                          ctypes.byref(cyc), d3))
+    return t.value, cyc.value, tuple(d3[a] for a in range(dim))
+
+
+def _write_dist(grid, t, cycle, path, opts):
+    import torch.distributed as tdist
+    out = grid.gather()
+    w, B = out if isinstance(out, tuple) else (out, None)
+    if grid.rank == 0:
+        write_arrays(path, grid.dim, grid.config.mhd, grid.N, grid.ghosts, grid.d, t, cycle, w, B, opts)
+    tdist.barrier(group=grid.group)
+
+
+def _load_dist(grid, path):
+    out = grid.gather()
+    w, B = out if isinstance(out, tuple) else (out, None)
+    w = np.ascontiguousarray(w)
+    B = None if B is None else np.ascontiguousarray(B)
+    t, cycle, d = load_arrays(path, grid.dim, grid.config.mhd, grid.N, grid.ghosts, w, B)
+    if tuple(d) != tuple(grid.d):
+        raise ValueError(f"the file's spacing {d} differs from the distributed grid's {tuple(grid.d)}")
+    grid.scatter(w, B)
+    return t, cycle
 
 
 writeToFile = write_to_file

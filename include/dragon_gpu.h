@@ -314,6 +314,17 @@ int dragon_gpu_hoard_wait(dragon_grid* g);
  * E converted to primitive values. Returns *t and *cycle. */
 int dragon_gpu_hoard_load(dragon_grid* g, const char* path, double* t, int* cycle);
 
+/* The same file from, and the same restart into, host arrays in this
+ * header's host layout (prim: the padded cells with NF values each; faceB:
+ * the padded faces with 3 values each, MHD 2D / 3D, else may be NULL) of a
+ * grid of `dim` dimensions, extents n3 and `ghosts` ghost layers: what a
+ * host-side grid, or the gathered slabs of a distributed grid, writes and
+ * restarts from. dragon_hoard_load_host returns the file's spacing in d3. */
+int dragon_hoard_write_host(const char* path, int dim, int mhd, const int* n3, int ghosts, const double* d3, double t,
+                            int cycle, const double* prim, const double* faceB, const dragon_hoard_opts* o);
+int dragon_hoard_load_host(const char* path, int dim, int mhd, const int* n3, int ghosts, double* prim, double* faceB,
+                           double* t, int* cycle, double* d3);
+
 /* The HDF5 subset itself, on host arrays (no device involved). */
 #define DRAGON_H5_F64 0
 #define DRAGON_H5_F32 1

@@ -222,10 +222,39 @@ def run_case(name, slab_factory, group=None):
     return w, B, res
 
 
-def serial_run(name, backend="port", fail_first=False):
-    """The serial grid's run of a case: per step the boundary fill, the CFL
-    time, then the step (halved once on the first step when fail_first)."""
+def run_hoard_case(name, slab_factory, out_dir, group=None):
+    """Output and restart of a distributed grid: the case's steps, a frame
+    written from the distributed grid, a fresh distributed grid restarted
+    from it and advanced by the case's steps again."""
+    from dragon_b200 import dist, hoard
     dim, n, d, g, cfg, blist, w0, B0, init_B, steps = case(name)
+    cls = {1: dist.DistGrid1D, 2: dist.DistGrid2D, 3: dist.DistGrid3D}[dim]
+    hoard.output_dir = out_dir
+    G = cls(*n, *d, ghosts=g, config=cfg, group=group, slab_factory=slab_factory)
+    G.scatter(w0, B0)
+    G.boundary = blist
+    if init_B:
+        G.initialize_B_fields()
+    G.advance_steps(steps)
+    hoard.write_to_file(G, 0.5, steps, f"{name}_{hoard.cycle_string(steps)}",
+                        opts=hoard.Options(write_option=7, redundant_vals=2))
+    H = cls(*n, *d, ghosts=g, config=cfg, group=group, slab_factory=slab_factory)
+    H.boundary = blist
+    t, cycle = hoard.load_from_file(H, f"{name}_{hoard.cycle_string(steps)}")
+    if (t, cycle) != (0.5, steps):
+        raise RuntimeError(f"restart returned t={t} cycle={cycle}")
+    res = H.advance_steps(steps)
+    out = H.gather()
+    w, B = (out if isinstance(out, tuple) else (out, None))
+    return w, B, res
+
+
+def serial_run(name, backend="port", fail_first=False, steps=None):
+    """The serial grid's run of a case: per step the boundary fill, the CFL
+    time, then the step (halved once on the first step when fail_first);
+    `steps` overrides the case's step count."""
+    dim, n, d, g, cfg, blist, w0, B0, init_B, case_steps = case(name)
+    steps = case_steps if steps is None else steps
     if backend == "port":
         from oracle.port import PortGrid
         c = cfg
@@ -275,7 +304,10 @@ def main():
                 fail_calls = (1,)
             factory = FailingSlab
     for name in a.cases.split(","):
-        w, B, res = run_case(name, factory)
+        if name.startswith("hoard_"):
+            w, B, res = run_hoard_case(name[len("hoard_"):], factory, a.out)
+        else:
+            w, B, res = run_case(name, factory)
         if rank == 0:
             np.savez(os.path.join(a.out, f"{name}.npz"), w=w, B=B if B is not None else np.zeros(0),
                      steps=res.steps, retries=res.retries, last_dt=res.last_dt)

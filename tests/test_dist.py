@@ -91,6 +91,31 @@ def test_dist_all_or_nothing_retry(tmp_path, oracle_built):
     _check("kh2d_retry", got, dist_worker.serial_run("kh2d_retry", fail_first=True))
 
 
+def test_dist_output_and_restart(tmp_path, oracle_built):
+    """DRAGONHOARD on a distributed grid (2 gloo ranks, oracle slabs): rank 0
+    writes the gathered grid, and the file holds exactly what the serial
+    grid's state writes; a fresh distributed grid restarted from it and
+    advanced again ends where the uninterrupted serial run ends, bit for bit."""
+    import h5subset
+    from dragon_b200 import hoard
+    cases = ["kh2d_periodic", "ot2d_mhd", "blast3d"]
+    got = run_ranks(2, ["hoard_" + c for c in cases], tmp_path)
+    opts = hoard.Options(write_option=7, redundant_vals=2)
+    for name in cases:
+        dim, n, d, g, cfg, _, _, B0, _, steps = dist_worker.case(name)
+        w, B = dist_worker.serial_run(name)
+        ref_path = str(tmp_path / f"serial_{name}.h5")
+        hoard.write_arrays(ref_path, dim, cfg.mhd, n, g, d, 0.5, steps, w, B, opts)
+        fa = h5subset.File(str(tmp_path / f"{name}_{hoard.cycle_string(steps)}.h5"))
+        fb = h5subset.File(ref_path)
+        assert {k: fa.attrs[k] for k in fa.attrs} == {k: fb.attrs[k] for k in fb.attrs}
+        keys = ["/fluid/rho", "/fluid/p", "/fluid/E", "/fluid/v/x", "/fluid/momentum/y"] + \
+            (["/fluid/Bf/x", "/fluid/B/z"] if cfg.mhd else [])
+        for k in keys:
+            np.testing.assert_array_equal(fa[k].read(), fb[k].read(), err_msg=f"{name} {k}")
+        _check("hoard_" + name, got["hoard_" + name], dist_worker.serial_run(name, steps=2 * steps))
+
+
 def test_child_sizes_and_ghosts():
     assert [dist.child_size(10, 3, i) for i in range(3)] == [4, 3, 3]
     assert sum(dist.child_size(1001, 7, i) for i in range(7)) == 1001

@@ -283,3 +283,23 @@ def test_continued_run_ends_where_the_uninterrupted_run_ends(mhd):
     np.testing.assert_array_equal(C.w[g:-g, g:-g], A.w[g:-g, g:-g])
     if mhd:
         np.testing.assert_array_equal(C.B[g:-g, g:-g], A.B[g:-g, g:-g])
+
+
+@pytest.mark.parametrize("dim", [1, 2, 3])
+@pytest.mark.parametrize("mhd", [False, True])
+def test_device_pack_equals_host_writer(tmp_path, dim, mhd):
+    """The file written from the device state and the file the host writer
+    builds from the same state's host arrays hold the same datasets and
+    attributes, bit for bit (write option 7, float redundant values)."""
+    G, n, d = _grid(dim, mhd, seed=40 + dim)
+    o = hoard.Options(write_option=7, redundant_vals=1, write_ghosts=True)
+    hoard.write_to_file(G, 0.5, 5, "dev", opts=o)
+    hoard.write_arrays(str(tmp_path / "host.h5"), dim, mhd, n, G.ghosts, d, 0.5, 5, G.w,
+                       G.B if (mhd and dim > 1) else None, o)
+    fa, a = _files(str(tmp_path / "dev.h5"))
+    fb, b = _files(str(tmp_path / "host.h5"))
+    assert sorted(a) == sorted(b)
+    for k in a:
+        assert a[k].dtype == b[k].dtype
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+    assert {k: fa.attrs[k] for k in fa.attrs} == {k: fb.attrs[k] for k in fb.attrs}

@@ -220,3 +220,102 @@ def test_cycle_string_and_restart_file_name(tmp_path, monkeypatch):
     monkeypatch.setattr(hoard, "output_dir", str(tmp_path / "frame_00003.h5"))
     with pytest.raises(RuntimeError):
         hoard.verify_output_directory()
+
+
+# ---- the host writer and loader against the oracle's restatement ----------------
+
+def _random_grid(dim, mhd, g, seed):
+    rng = np.random.default_rng(seed)
+    n = (7, 5, 4)[:dim]
+    nf = 8 if mhd else 5
+    w = rng.uniform(-1, 1, tuple(x + 2 * g for x in n) + (nf,))
+    w[..., 0] = rng.uniform(0.5, 2.0, w.shape[:-1])
+    w[..., 1] = rng.uniform(0.1, 3.0, w.shape[:-1])
+    B = rng.uniform(-1, 1, tuple(x + 1 + 2 * g for x in n) + (3,)) if (mhd and dim > 1) else None
+    return n, w, B
+
+
+@pytest.mark.parametrize("dim", [1, 2, 3])
+@pytest.mark.parametrize("mhd", [False, True])
+@pytest.mark.parametrize("opt,red,ghosts,level", [(3, 1, False, 4), (7, 2, True, 0), (6, 0, False, 1),
+                                                  (1, 1, True, 4), (3, 0, True, 0)])
+def test_host_writer_matches_oracle(tmp_path, dim, mhd, opt, red, ghosts, level):
+    """dragon_hoard_write_host: the datasets and attributes the oracle's
+    restatement of writeToFile gives, bit for bit (the same plan and values the
+    device pack uses)."""
+    from oracle import hoard_port
+    g = 3 if mhd else 2
+    n, w, B = _random_grid(dim, mhd, g, seed=dim * 100 + opt * 10 + red)
+    d = (0.1, 0.2, 0.3)[:dim]
+    p = str(tmp_path / "h.h5")
+    hoard.write_arrays(p, dim, mhd, n, g, d, 0.25, 12, w, B,
+                       hoard.Options(write_option=opt, redundant_vals=red, compression_level=level, write_ghosts=ghosts))
+    f = h5subset.File(p)
+    want = hoard_port.expected_datasets(w, B, dim, mhd, ghosts, g, opt, red)
+    got = {}
+
+    def walk(grp, prefix):
+        for k in grp.keys():
+            o = grp[k]
+            if isinstance(o, h5subset.Group):
+                walk(o, prefix + "/" + k)
+            else:
+                got[prefix + "/" + k] = o.read()
+    walk(f, "")
+    assert sorted(got) == sorted(want)
+    for k, v in want.items():
+        assert got[k].dtype == v.dtype and got[k].shape == v.shape, k
+        np.testing.assert_array_equal(got[k], v, err_msg=k)
+    assert {k: f.attrs[k] for k in f.attrs} == hoard_port.expected_attrs(dim, mhd, n, d, ghosts, g, 0.25, 12, opt)
+
+
+@pytest.mark.parametrize("dim", [1, 2, 3])
+@pytest.mark.parametrize("mhd", [False, True])
+@pytest.mark.parametrize("opt,red,ghosts", [(6, 1, False), (7, 0, True), (3, 0, False), (1, 2, True)])
+def test_host_loader_matches_oracle(tmp_path, dim, mhd, opt, red, ghosts):
+    """dragon_hoard_load_host: the state the oracle's restatement of
+    loadFromFile restores (conservative restarts, omitted cell B, cells
+    outside the file's range untouched), bit for bit."""
+    from oracle import hoard_port
+    g = 3 if mhd else 2
+    n, w, B = _random_grid(dim, mhd, g, seed=7 + dim + opt)
+    d = (0.1, 0.2, 0.3)[:dim]
+    p = str(tmp_path / "r.h5")
+    hoard.write_arrays(p, dim, mhd, n, g, d, 1.5, 9, w, B,
+                       hoard.Options(write_option=opt, redundant_vals=red, write_ghosts=ghosts))
+    _, w0, B0 = _random_grid(dim, mhd, g, seed=99)
+    w1 = w0.copy()
+    B1 = None if B0 is None else B0.copy()
+    t, cycle, dd = hoard.load_arrays(p, dim, mhd, n, g, w1, B1)
+    assert (t, cycle, dd) == (1.5, 9, d)
+    f = h5subset.File(p)
+    files = {}
+
+    def walk(grp, prefix):
+        for k in grp.keys():
+            o = grp[k]
+            if isinstance(o, h5subset.Group):
+                walk(o, prefix + "/" + k)
+            else:
+                files[prefix + "/" + k] = o.read()
+    walk(f, "")
+    ww, BB = hoard_port.restored_state(w0, B0, files, dim, mhd, mhd, g, g if ghosts else 0, opt)
+    np.testing.assert_array_equal(w1, ww)
+    if BB is not None:
+        np.testing.assert_array_equal(B1, BB)
+
+
+def test_host_loader_checks(tmp_path):
+    """HDF5Restart.cpp's checks on host arrays: dimension, extents, physics."""
+    n, w, _ = _random_grid(2, False, 2, 1)
+    p = str(tmp_path / "c.h5")
+    hoard.write_arrays(p, 2, False, n, 2, (0.1, 0.2), 0.0, 0, w)
+    with pytest.raises(Exception, match="Expected 3 dimensions but got 2"):
+        hoard.load_arrays(p, 3, False, n + (4,), 2, np.zeros((11, 9, 8, 5)))
+    with pytest.raises(Exception, match="File size does not match"):
+        hoard.load_arrays(p, 2, False, (7, 6), 2, np.zeros((11, 10, 5)))
+    nm, wm, Bm = _random_grid(2, True, 3, 2)
+    pm = str(tmp_path / "m.h5")
+    hoard.write_arrays(pm, 2, True, nm, 3, (0.1, 0.2), 0.0, 0, wm, Bm)
+    with pytest.raises(Exception, match="MHD"):
+        hoard.load_arrays(pm, 2, False, nm, 3, np.zeros((13, 11, 5)))
