@@ -189,6 +189,7 @@ int make_plan(const Shape& h_, double t, int cycle, const dragon_hoard_opts& o, 
     if (!(prims || consv))
         return fail_h(DRAGON_GPU_EINVAL, "write option does not write a sufficient description of the fluid");
     if (red < 0 || red > 2) return fail_h(DRAGON_GPU_EINVAL, "redundant-values option must be 0, 1 or 2");
+    if (o.compression > 9) return fail_h(DRAGON_GPU_EINVAL, "compression level must be at most 9 (deflate)");
     const int dim = h->dim;
     const int ng = o.ghosts ? h->g : 0;
     P->sh = h->g - ng;

@@ -191,8 +191,9 @@ void plan_chunks(DsetNode& n) {
     }
 }
 
-// Gathers chunk c of n (zero past the dataset's edge) into raw and deflates it.
-void compress_one(DsetNode& n, uint64_t c, int level, Bytes& raw) {
+// Gathers chunk c of n (zero past the dataset's edge) into raw and deflates
+// it; false when zlib fails.
+bool compress_one(DsetNode& n, uint64_t c, int level, Bytes& raw) {
     const Dataset& d = *n.d;
     const int es = esize_of(d.type);
     const int r = d.rank;
@@ -218,14 +219,16 @@ void compress_one(DsetNode& n, uint64_t c, int level, Bytes& raw) {
     }
     uLongf zn = compressBound(raw.size());
     Bytes z(zn);
-    compress2(z.data(), &zn, raw.data(), raw.size(), level);
+    if (compress2(z.data(), &zn, raw.data(), raw.size(), level) != Z_OK) return false;
     z.resize(zn);
     n.zchunks[c] = std::move(z);
+    return true;
 }
 
 // Deflates every chunk of every chunked dataset: `threads` host threads take
 // chunks from one shared list, so datasets do not wait for one another.
-void compress_all(std::vector<DsetNode>& dn, int level, int threads) {
+// False when any chunk failed.
+bool compress_all(std::vector<DsetNode>& dn, int level, int threads) {
     std::vector<std::pair<uint32_t, uint64_t>> work;
     for (uint32_t i = 0; i < dn.size(); i++) {
         if (!dn[i].chunked) continue;
@@ -233,12 +236,13 @@ void compress_all(std::vector<DsetNode>& dn, int level, int threads) {
         for (uint64_t c = 0; c < dn[i].nchunks; c++) work.push_back({i, c});
     }
     std::atomic<uint64_t> next{0};
+    std::atomic<bool> ok{true};
     auto run = [&]() {
         Bytes raw;
         for (;;) {
             const uint64_t k = next.fetch_add(1);
             if (k >= work.size()) break;
-            compress_one(dn[work[k].first], work[k].second, level, raw);
+            if (!compress_one(dn[work[k].first], work[k].second, level, raw)) ok = false;
         }
     };
     const int nt = std::max(1, std::min<int>(threads, int(std::min<uint64_t>(work.size(), 1024))));
@@ -246,6 +250,7 @@ void compress_all(std::vector<DsetNode>& dn, int level, int threads) {
     for (int t = 1; t < nt; t++) pool.emplace_back(run);
     run();
     for (auto& t : pool) t.join();
+    return ok;
 }
 
 // Key of chunk c: filtered size, filter mask, element offsets (+ a trailing 0).
@@ -337,7 +342,10 @@ int write_file(const std::string& path, const std::vector<Attr>& attrs, const st
         }
 
     // -- compress every chunk
-    compress_all(dn, level, threads);
+    if (!compress_all(dn, level, threads)) {
+        *err = "deflate failed";
+        return -1;
+    }
 
     // -- sizes, then addresses (metadata first, raw data after)
     uint64_t at = 96;  // superblock version 0

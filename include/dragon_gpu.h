@@ -302,8 +302,9 @@ int dragon_gpu_hoard_write(dragon_grid* g, double t, int cycle, const char* path
 /* Snapshots the current state on the grid's stream and returns: the device
  * packs the datasets into one of two staging buffers, a copy stream downloads
  * it while later steps run, and a host thread writes the file. A third call
- * waits for the oldest snapshot's file first. Later steps and boundary calls
- * do not change a snapshot already taken. */
+ * waits for the oldest snapshot's file first; if that file failed, the call
+ * returns its failure (this call's snapshot is taken all the same). Later
+ * steps and boundary calls do not change a snapshot already taken. */
 int dragon_gpu_hoard_write_async(dragon_grid* g, double t, int cycle, const char* path, const dragon_hoard_opts* o);
 /* Waits for every file of g in flight; returns the first failure among them. */
 int dragon_gpu_hoard_wait(dragon_grid* g);

@@ -305,6 +305,15 @@ def test_host_loader_matches_oracle(tmp_path, dim, mhd, opt, red, ghosts):
         np.testing.assert_array_equal(B1, BB)
 
 
+def test_host_writer_rejects_bad_options(tmp_path):
+    n, w, _ = _random_grid(2, False, 2, 3)
+    p = str(tmp_path / "o.h5")
+    for o in (hoard.Options(write_option=2), hoard.Options(write_option=0), hoard.Options(redundant_vals=3),
+              hoard.Options(compression_level=10)):
+        with pytest.raises(Exception):
+            hoard.write_arrays(p, 2, False, n, 2, (0.1, 0.2), 0.0, 0, w, None, o)
+
+
 def test_host_loader_checks(tmp_path):
     """HDF5Restart.cpp's checks on host arrays: dimension, extents, physics."""
     n, w, _ = _random_grid(2, False, 2, 1)
