@@ -699,6 +699,11 @@ int dragon_gpu_hoard_wait(dragon_grid* h) {
 int dragon_gpu_hoard_load(dragon_grid* h, const char* path, double* t, int* cycle) {
     if (!h || !path || !t || !cycle) return fail_h(DRAGON_GPU_EINVAL, "null argument");
     if (h->adv.pending) return fail_h(DRAGON_GPU_EINVAL, "an asynchronous advance is in flight");
+    // the grid's own files still being written are complete first (a restart
+    // may name one of them); their status stays for dragon_gpu_hoard_wait
+    if (h->hoard)
+        for (auto& s : h->hoard->slot)
+            if (s.writer.joinable()) s.writer.join();
     // current state (reference order, dense padded): cells outside the file's
     // range keep their values
     std::vector<double> W(dragon_gpu_prim_count(h)), FB(dragon_gpu_faceB_count(h));

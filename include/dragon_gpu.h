@@ -308,7 +308,8 @@ int dragon_gpu_hoard_write(dragon_grid* g, double t, int cycle, const char* path
 int dragon_gpu_hoard_write_async(dragon_grid* g, double t, int cycle, const char* path, const dragon_hoard_opts* o);
 /* Waits for every file of g in flight; returns the first failure among them. */
 int dragon_gpu_hoard_wait(dragon_grid* g);
-/* Restart (HDF5Restart.cpp:61-377): checks format_version <= 1, dim, MHD
+/* Restart (HDF5Restart.cpp:61-377), after the grid's own files in flight are
+ * complete: checks format_version <= 1, dim, MHD
  * and the extents against the grid, then loads dx/dy/dz (the grid's spacing
  * becomes the file's), the cells and (MHD 2D / 3D) face B of the file's
  * range: primitive values when write_option has bit 1, else rho, momentum and

@@ -303,3 +303,20 @@ def test_device_pack_equals_host_writer(tmp_path, dim, mhd):
         assert a[k].dtype == b[k].dtype
         np.testing.assert_array_equal(a[k], b[k], err_msg=k)
     assert {k: fa.attrs[k] for k in fa.attrs} == {k: fb.attrs[k] for k in fb.attrs}
+
+
+def test_restart_waits_for_the_grids_own_file(tmp_path):
+    """A restart that names a file the same grid is still writing reads the
+    complete file: the load waits for the grid's writers first."""
+    G, n, d = _grid(3, True, seed=77)
+    w0, B0 = G.w.copy(), G.B.copy()
+    hoard.write_to_file(G, 2.0, 4, "inflight", wait=False,
+                        opts=hoard.Options(write_option=1, redundant_vals=2, compression_level=9))
+    G.w[...] = 1.0  # changed after the snapshot, restored by the restart below
+    t, cycle = hoard.load_from_file(G, "inflight")
+    assert (t, cycle) == (2.0, 4)
+    g = G.ghosts
+    sl = (slice(g, -g),) * 3
+    np.testing.assert_array_equal(G.w[sl], w0[sl])
+    np.testing.assert_array_equal(G.B[sl], B0[sl])
+    hoard.wait(G)
