@@ -320,3 +320,27 @@ def test_restart_waits_for_the_grids_own_file(tmp_path):
     np.testing.assert_array_equal(G.w[sl], w0[sl])
     np.testing.assert_array_equal(G.B[sl], B0[sl])
     hoard.wait(G)
+
+
+def test_full_size_snapshot_round_trip(tmp_path):
+    """The 1024^2 shear layer (the benchmark's grid) after 3 steps: a deflated
+    file (1024 chunks of 32 x 32 per dataset, two-level chunk B-trees) restarts
+    a fresh grid to the same interior bit for bit, and equals the host
+    writer's file of the same state."""
+    n = 1024
+    w0, dx, dy = problems.kelvin_helmholtz_2d(n, ghosts=2, seed=1234)
+    G = dg.Grid2D(n, n, dx, dy, ghosts=2)
+    G.w[...] = w0
+    G.boundary = dg.Periodic()
+    G.advance_steps(3)
+    o = hoard.Options(write_option=1, compression_level=4)
+    hoard.write_to_file(G, 0.01, 3, "big", opts=o)
+    H = dg.Grid2D(n, n, dx, dy, ghosts=2)
+    t, cycle = hoard.load_from_file(H, "big")
+    assert (t, cycle) == (0.01, 3)
+    np.testing.assert_array_equal(H.w[2:-2, 2:-2], G.w[2:-2, 2:-2])
+    hoard.write_arrays(str(tmp_path / "host.h5"), 2, False, (n, n), 2, (dx, dy), 0.01, 3, G.w, None, o)
+    _, a = _files(str(tmp_path / "big.h5"))
+    _, b = _files(str(tmp_path / "host.h5"))
+    for k in a:
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
