@@ -223,6 +223,7 @@ SIGNATURES = {
     "dragon_gpu_batch_autotune": (
         ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(BatchTuning), ctypes.POINTER(ctypes.c_double)]),
     "dragon_gpu_batch_advance_steps": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(BatchStats)]),
+    "dragon_gpu_set_origin": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "dragon_gpu_hoard_default_opts": (None, [ctypes.POINTER(HoardOpts)]),
     "dragon_gpu_hoard_write": (
         ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_char_p, ctypes.POINTER(HoardOpts)]),

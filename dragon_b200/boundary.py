@@ -142,11 +142,14 @@ class DeviceGhostFill(GhostFill):
             DeviceGhostFill._compiled[key] = out
         return DeviceGhostFill._compiled[key]
 
-    def bind(self, lib, handle, entry: int):
-        """dragon_gpu_set_user_fill for list entry `entry` of a grid."""
+    def bind(self, lib, handle, entry: int, fill_faces: int | None = None):
+        """dragon_gpu_set_user_fill for list entry `entry` of a grid
+        (fill_faces overrides the element's own, e.g. masked to the faces a
+        slab of a distributed grid owns)."""
         from . import _lib
         arr = (ctypes.c_double * max(1, len(self.params)))(*self.params)
-        _lib.check(lib.dragon_gpu_set_user_fill(handle, entry, self._fill, self.fill_faces, int(self.corners), arr,
+        ff = self.fill_faces if fill_faces is None else int(fill_faces)
+        _lib.check(lib.dragon_gpu_set_user_fill(handle, entry, self._fill, ff, int(self.corners), arr,
                                                 len(self.params)))
 
 

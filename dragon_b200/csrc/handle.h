@@ -112,6 +112,8 @@ struct dragon_grid {
     bool tmap_ok[2][2] = {{false, false}, {false, false}};
     // output snapshots in flight (hoard.cu), created on first use
     HoardState* hoard = nullptr;
+    // global index of cell (0, 0, 0) as user fills see it (dragon_gpu_set_origin)
+    int origin[3] = {0, 0, 0};
 };
 
 namespace dgpu_rt {

@@ -960,6 +960,14 @@ int dragon_gpu_apply_boundary(dragon_grid* h) {
 
 int dragon_gpu_boundary_entries(const dragon_grid* h) { return h ? h->nbc : 0; }
 
+int dragon_gpu_set_origin(dragon_grid* h, int i0, int j0, int k0) {
+    if (!h) return fail(DRAGON_GPU_EINVAL, "null grid");
+    h->origin[0] = i0;
+    h->origin[1] = h->dim > 1 ? j0 : 0;
+    h->origin[2] = h->dim > 2 ? k0 : 0;
+    return 0;
+}
+
 int dragon_gpu_apply_boundary_range(dragon_grid* h, int first, int count) {
     if (h && h->adv.pending) return fail(DRAGON_GPU_EINVAL, "an asynchronous advance is in flight");
     if (!h || first < 0 || count < 0 || first + count > h->nbc) return fail(DRAGON_GPU_EINVAL, "entry range out of bounds");

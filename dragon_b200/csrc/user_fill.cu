@@ -158,6 +158,7 @@ struct dragon_fill_ctx {
     double d[3];                          /* dx, dy, dz */
     int dim, n[3], g, nf, nparams;
     int axis, side;                       /* the face being filled: axis 0..2, side 0 low / 1 high */
+    int off[3];                           /* global index of cell (0, 0, 0): a slab's place in a distributed grid */
     __device__ long long cell(int i, int j, int k) const {
         return dim == 1 ? (long long)(i + g)
              : dim == 2 ? (long long)(i + g) * pitch + (j + g)
@@ -221,6 +222,7 @@ struct FillCtx {
     double d[3];
     int dim, n[3], g, nf, nparams;
     int axis, side;
+    int off[3];
 };
 
 bool valid_identifier(const char* s) {
@@ -373,6 +375,7 @@ int launch_user_fill(dragon_grid* h, int c, int entry, double* w_buf) {
     x.g = h->g;
     x.nf = h->nf;
     x.nparams = b.nparams;
+    for (int a = 0; a < 3; a++) x.off[a] = h->origin[a];
     const int* err = &h->ctl->err;
     const int* done = &h->ctl->done;
     int corners = b.corners;

@@ -90,6 +90,8 @@ class SlabProgram:
 
     def __init__(self, blist: BoundaryList, rank: int, parts: int, dim: int):
         self.entries: list[tuple[int, int, int, list[float]]] = []
+        # device user fills by entry: (element, the faces it fills on this slab)
+        self.fills: dict[int, tuple[object, int]] = {}
         self.wrap_at: int | None = None
         self.wrap_corners = True
         own = ALL_FACES & ~X
@@ -100,8 +102,6 @@ class SlabProgram:
         els = list(blist)
         if any(e.is_custom for e in els):
             raise NotImplementedError("boundary elements with a host apply() are not supported on a DistGrid")
-        if any(e.kind == USER for e in els):
-            raise NotImplementedError("device user fills (DeviceGhostFill) are not supported on a DistGrid")
         uncovered = ALL_FACES
         for e in els:
             uncovered &= ~_normalised_faces(e)
@@ -119,6 +119,10 @@ class SlabProgram:
                 rest = f & ~X
                 if rest and dim > 1:
                     self.entries.append((PERIODIC, rest, int(e.corners), [0.0] * 8))
+            elif e.kind == USER:
+                # a device fill visits the faces of the global box this slab touches
+                self.fills[len(self.entries)] = (e, e.fill_faces & own)
+                self.entries.append((USER, f & own, int(e.corners), [0.0] * 8))
             else:
                 self.entries.append((e.kind, f & own, int(e.corners), st[:8]))
         self.entries.append((IGNORE, ALL_FACES, 1, [0.0] * 8))
@@ -140,7 +144,12 @@ class GpuSlab:
         self.has_faces = self.grid._B is not None
         self.on_device = torch.cuda.is_available()
 
-    def set_entries(self, entries):
+    def set_origin(self, offset):
+        """The slab's place in the global grid, for its device user fills."""
+        o = list(offset) + [0] * (3 - len(offset))
+        _lib.check(self.L.dragon_gpu_set_origin(self.h, int(o[0]), int(o[1]), int(o[2])))
+
+    def set_entries(self, entries, fills=None):
         arr = (_lib.BCDesc * max(1, len(entries)))()
         for k, (t, faces, corners, st) in enumerate(entries):
             arr[k].type = t
@@ -151,6 +160,8 @@ class GpuSlab:
         _lib.check(self.L.dragon_gpu_set_boundary(self.h, arr, len(entries)))
         if int(self.L.dragon_gpu_boundary_entries(self.h)) != len(entries):
             raise RuntimeError("device boundary list does not match the slab program")
+        for k, (el, ff) in (fills or {}).items():
+            el.bind(self.L, self.h, k, fill_faces=ff)
 
     def apply_range(self, first, count):
         if count <= 0:
@@ -242,12 +253,14 @@ class _DistBase:
         if self.slab.ghosts != g:
             raise RuntimeError("slab ghost width differs from the distributed grid's")
         self.nl = sizes[self.rank]
+        if hasattr(self.slab, "set_origin"):
+            self.slab.set_origin((self.offset,))
         self.has_faces = self.slab.has_faces
         nccl = tdist.get_backend(group) == "nccl"
         self.comm_device = torch.device("cuda", torch.cuda.current_device()) if nccl else torch.device("cpu")
         self._boundary = BoundaryList()
         self._program = SlabProgram(self._boundary, self.rank, self.parts, self.dim)
-        self.slab.set_entries(self._program.entries)
+        self.slab.set_entries(self._program.entries, self._program.fills)
         self._bufs = {}
 
     # -- topology -------------------------------------------------------------
@@ -268,7 +281,7 @@ class _DistBase:
     def boundary(self, b):
         self._boundary = as_list(b)
         self._program = SlabProgram(self._boundary, self.rank, self.parts, self.dim)
-        self.slab.set_entries(self._program.entries)
+        self.slab.set_entries(self._program.entries, self._program.fills)
 
     # -- halo exchange ----------------------------------------------------------
     def _buf(self, key, count):

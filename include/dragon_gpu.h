@@ -149,7 +149,10 @@ int dragon_gpu_apply_boundary_range(dragon_grid* g, int first, int count);
  * the face. dragon_fill_ctx gives the padded state: c.get(f, i, j, k) /
  * c.set(f, i, j, k, v) on primitive field f (DRAGON_RHO, DRAGON_P,
  * DRAGON_VX..VZ, DRAGON_BX..BZ), c.getB / c.setB on face B (MHD 2D / 3D),
- * c.n[3], c.g, c.d[3], c.dim and c.params[0 .. c.nparams). One thread walks
+ * c.n[3], c.g, c.d[3], c.dim, c.params[0 .. c.nparams) and c.off[3], the
+ * global index of the grid's cell (0, 0, 0) (non-zero for the slab of a
+ * distributed grid: dragon_gpu_set_origin; a global x position is
+ * (c.off[0] + i + 0.5) * c.d[0]). One thread walks
  * the ghost layers of a transverse point of one face outward (layer 1 first),
  * transverse points and the two faces of an axis run in parallel, the axes
  * one after another; a fill writes only the ghost cell (and its face B) it is
@@ -174,6 +177,10 @@ const char* dragon_gpu_user_fill_log(const dragon_user_fill* f);
  * destroyed or have had their boundary list set again. */
 int dragon_gpu_set_user_fill(dragon_grid* g, int entry, dragon_user_fill* f, int fill_faces, int corners,
                              const double* params, int nparams);
+/* The global index of the grid's cell (0, 0, 0), as user fills see it in
+ * dragon_fill_ctx::off: a DistGrid child's offset in its parent
+ * (Refinement/DistGrid.cpp:41-111 computes it per child); 0 for a whole grid. */
+int dragon_gpu_set_origin(dragon_grid* g, int i0, int j0, int k0);
 /* Grid::initialize_B_fields (MHD/B_fields.cpp:117-149) */
 int dragon_gpu_initialize_B_fields(dragon_grid* g);
 

@@ -46,8 +46,39 @@ def _edge_ghosts(w, g):
     return np.pad(inner, [(g, g)] * (w.ndim - 1) + [(0, 0)], mode="edge")
 
 
+# Device user fills for the distributed-grid case below: the y faces take the
+# nearest interior row with vy set from the global x position (c.off[0] is the
+# slab's place in the grid), the X- face is a jet of fixed state where
+# |y - 0.5| < 0.2.
+Y_FILL = """
+__device__ void yfill(const dragon_fill_ctx& c, int i, int j, int k) {
+    const int js = c.side == 0 ? 0 : c.n[1] - 1;
+    for (int f = 0; f < c.nf; f++) c.set(f, i, j, k, c.get(f, i, js, k));
+    const double x = (c.off[0] + i + 0.5) * c.d[0];
+    c.set(DRAGON_VY, i, j, k, c.params[0] * x * (1.0 - x));
+}
+"""
+JET_FILL = """
+__device__ void jet(const dragon_fill_ctx& c, int i, int j, int k) {
+    for (int f = 0; f < c.nf; f++) c.set(f, i, j, k, c.get(f, 0, j, k));
+    if (fabs((j + 0.5) * c.d[1] - 0.5) < 0.2) {
+        c.set(DRAGON_RHO, i, j, k, 2.0);
+        c.set(DRAGON_P, i, j, k, 3.0);
+        c.set(DRAGON_VX, i, j, k, 1.5);
+    }
+}
+"""
+
+
 def case(name):
     """(dim, n, d, ghosts, Config, boundary, w0, B0 or None, init_B, steps)."""
+    if name == "kh2d_device_fills":
+        w, dx, dy = problems.kelvin_helmholtz_2d(24, ghosts=2, seed=9, ny=20)
+        w = _edge_ghosts(w, 2)
+        cfg = gr.Config(riemann=gr.RIEMANN_HLLC, limiter=gr.LIMITER_MC)
+        b = (bd.DeviceGhostFill(Y_FILL, "yfill", faces="Y", params=[0.4]) +
+             bd.DeviceGhostFill(JET_FILL, "jet", faces="X-") + bd.Outflow("X+"))
+        return 2, (24, 20), (dx, dy), 2, cfg, b, w, None, False, 4
     if name == "kh2d_periodic":
         w, dx, dy = problems.kelvin_helmholtz_2d(24, ghosts=2, seed=7, ny=20)
         cfg = gr.Config(riemann=gr.RIEMANN_HLLC, limiter=gr.LIMITER_VANLEER)
@@ -120,7 +151,9 @@ class PortSlab:
         self.saved = None
         self.calls = 0
 
-    def set_entries(self, entries):
+    def set_entries(self, entries, fills=None):
+        if fills:
+            raise NotImplementedError("device user fills need GPU slabs")
         self.entries = list(entries)
 
     def apply_range(self, first, count):

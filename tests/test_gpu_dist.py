@@ -42,6 +42,18 @@ def test_gpu_dist_matches_serial(world, tmp_path):
             np.testing.assert_array_equal(got[name]["B"], B, err_msg=name)
 
 
+@pytest.mark.parametrize("world", [2, 3])
+def test_gpu_dist_device_fills(world, tmp_path):
+    """Device user fills (NVRTC) on the slabs of a distributed grid: each slab
+    runs them on the faces of the global box it touches, with its global
+    origin in the fill context, and the distributed run equals the serial
+    grid's bit for bit (one fill depends on the global x position)."""
+    got = run_ranks(world, ["kh2d_device_fills"], tmp_path, slab="gpu")
+    w, _ = dist_worker.serial_run("kh2d_device_fills", backend="gpu")
+    np.testing.assert_array_equal(got["kh2d_device_fills"]["w"], w)
+    assert int(got["kh2d_device_fills"]["retries"]) == 0
+
+
 def _ot_grid(n=20):
     """A 2D MHD grid (n x n+4, 3 ghosts) holding distinct values everywhere."""
     G = gr.Grid2D(n, n + 4, 1.0 / n, 1.0 / n, ghosts=3, config=gr.Config(mhd=True))
