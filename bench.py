@@ -740,6 +740,9 @@ def hoard_report(n=1024, reps=8, intervals=(50, 250), frames=6):
             hoard.wait(G)
             with torch.cuda.stream(stream):
                 flush.fill_(1.0)
+                # a fixed ~1 ms device delay, so the host has enqueued the pack
+                # before the start event fires and the events time the kernel alone
+                torch.cuda._sleep(2_000_000)
                 a = torch.cuda.Event(enable_timing=True)
                 b = torch.cuda.Event(enable_timing=True)
                 a.record(stream)
