@@ -95,6 +95,8 @@ DistGrid::DistGrid(int dim, const int* n, const double* d, int ghosts, SlabComm&
     dragon_gpu_grid_info(h_, &dd, nn, &gg, &nf);
     if (gg != g_ || nf != kNF) throw std::logic_error("slab grid does not match the distributed grid");
     faces_ = kMHD && dim >= 2;
+    // user fills see global coordinates (dragon_fill_ctx::off)
+    check(dragon_gpu_set_origin(h_, off_, 0, 0));
     program();
 }
 
@@ -121,10 +123,10 @@ void DistGrid::program() {
     if (rank_ == parts_ - 1) own |= Boundary::X_positive;
     if (boundary.has_user_elements())
         throw std::logic_error("boundary elements with a host apply() are not supported on a DistGrid");
-    for (size_t k = 0; k < boundary.size(); k++)
-        if (boundary[k].device_type() == DRAGON_BC_USER)
-            throw std::logic_error("device user fills (Boundary::DeviceFill) are not supported on a DistGrid");
     std::vector<dragon_bc_desc> e;
+    // device user fills by entry, each filling the global faces this slab touches
+    std::vector<std::tuple<const void*, int, std::vector<double>>> fills;
+    std::vector<std::pair<int, const Boundary::DeviceFill*>> fill_at;
     auto entry = [](int type, int faces, int corners, const double* st) {
         dragon_bc_desc d;
         std::memset(&d, 0, sizeof(d));
@@ -147,17 +149,31 @@ void DistGrid::program() {
             e.push_back(entry(5, 0, 1, nullptr));
             const int rest = f & ~Boundary::X;
             if (rest && dim_ > 1) e.push_back(entry(4, rest, wrap_corners_, nullptr));
+        } else if (el.device_type() == DRAGON_BC_USER) {
+            const auto* df = dynamic_cast<const Boundary::DeviceFill*>(&el);
+            if (!df) throw std::logic_error("a user boundary entry that is not a Boundary::DeviceFill");
+            fill_at.push_back({(int)e.size(), df});
+            fills.emplace_back(df->compiled(), df->fill_faces & own, df->params);
+            e.push_back(entry(DRAGON_BC_USER, f & own, el.get_corners() ? 1 : 0, nullptr));
         } else {
             e.push_back(entry(el.device_type(), f & own, el.get_corners() ? 1 : 0, el.device_state()));
         }
     }
     e.push_back(entry(5, kAllFaces, 1, nullptr));
     entries_ = e;
-    if (pushed_.size() == e.size() && std::memcmp(pushed_.data(), e.data(), sizeof(dragon_bc_desc) * e.size()) == 0)
+    if (pushed_.size() == e.size() && std::memcmp(pushed_.data(), e.data(), sizeof(dragon_bc_desc) * e.size()) == 0 &&
+        pushed_fills_ == fills)
         return;
     check(dragon_gpu_set_boundary(h_, e.data(), (int)e.size()));
     if (dragon_gpu_boundary_entries(h_) != (int)e.size()) throw std::logic_error("device list differs from the slab list");
+    for (size_t q = 0; q < fill_at.size(); q++) {
+        const auto* df = fill_at[q].second;
+        const auto& pr = std::get<2>(fills[q]);
+        check(dragon_gpu_set_user_fill(h_, fill_at[q].first, df->compiled(), std::get<1>(fills[q]),
+                                       df->get_corners() ? 1 : 0, pr.empty() ? nullptr : pr.data(), (int)pr.size()));
+    }
     pushed_ = e;
+    pushed_fills_ = fills;
 }
 
 // Layers sent to / received from the neighbour across `side` (0 low x, 1 high

@@ -23,6 +23,7 @@
 #pragma once
 
 #include <memory>
+#include <tuple>
 #include <vector>
 
 #include "dragon.hpp"
@@ -120,6 +121,8 @@ private:
     std::vector<dragon_bc_desc> entries_;
     int wrap_at_ = -1, wrap_corners_ = 1;
     std::vector<dragon_bc_desc> pushed_;
+    // device user fills bound with the pushed list: (fill, faces filled on this slab, params) per entry
+    std::vector<std::tuple<const void*, int, std::vector<double>>> pushed_fills_;
     double* dbuf_ = nullptr;  // device send / receive buffers
     size_t dbuf_count_ = 0;
     int steps_ = 0, retries_ = 0;

@@ -93,7 +93,7 @@ static Case make_case(const std::string& name) {
     Case c{};
     std::mt19937_64 rng(1234);
     std::uniform_real_distribution<double> u(-0.01, 0.01);
-    if (name == "kh" || name == "walls") {
+    if (name == "kh" || name == "walls" || name == "fills") {
         c.dim = 2;
         c.n[0] = 40;
         c.n[1] = 24;
@@ -173,9 +173,31 @@ static Case make_case(const std::string& name) {
     return c;
 }
 
+// Device user fills (NVRTC): the y faces take the nearest interior row with vy
+// from the global x position (c.off[0]: the slab's place), X- is a jet.
+static const char* kYFill = R"(
+__device__ void yfill(const dragon_fill_ctx& c, int i, int j, int k) {
+    const int js = c.side == 0 ? 0 : c.n[1] - 1;
+    for (int f = 0; f < c.nf; f++) c.set(f, i, j, k, c.get(f, i, js, k));
+    const double x = (c.off[0] + i + 0.5) * c.d[0];
+    c.set(DRAGON_VY, i, j, k, c.params[0] * x * (1.0 - x));
+})";
+static const char* kJet = R"(
+__device__ void jet(const dragon_fill_ctx& c, int i, int j, int k) {
+    for (int f = 0; f < c.nf; f++) c.set(f, i, j, k, c.get(f, 0, j, k));
+    if (fabs((j + 0.5) * c.d[1] - 0.5) < 0.2) {
+        c.set(DRAGON_RHO, i, j, k, 2.0);
+        c.set(DRAGON_P, i, j, k, 3.0);
+        c.set(DRAGON_VX, i, j, k, 1.5);
+    }
+})";
+
 static void set_boundary(Boundary::BoundaryList& b, const std::string& name) {
     if (name == "kh" || name == "ot") b = Boundary::Periodic();
     else if (name == "walls") b = Boundary::Outflow("Y", false) + Boundary::Reflective("X");
+    else if (name == "fills")
+        b = Boundary::DeviceFill(kYFill, "yfill", Boundary::Y, Boundary::Y, {0.4}) +
+            Boundary::DeviceFill(kJet, "jet", Boundary::X_negative, Boundary::X_negative) + Boundary::Outflow("X+");
 }
 
 // The serial grid's run through the same C++ API (Grid::advance_steps).
@@ -194,6 +216,11 @@ static void serial(const std::string& name, const Case& c, std::vector<Primitive
     }
     std::vector<dragon_bc_desc> d = G->boundary.descriptors();
     if (dragon_gpu_set_boundary(h, d.data(), (int)d.size())) std::abort();
+    for (size_t k = 0; k < G->boundary.size(); k++)
+        if (const auto* df = dynamic_cast<const Boundary::DeviceFill*>(&G->boundary[k]))
+            if (dragon_gpu_set_user_fill(h, (int)k, df->compiled(), df->fill_faces, df->get_corners() ? 1 : 0,
+                                         df->params.empty() ? nullptr : df->params.data(), (int)df->params.size()))
+                std::abort();
     dragon_advance_stats st;
     if (dragon_gpu_advance_steps(h, c.steps, &st)) {
         std::fprintf(stderr, "serial: %s\n", dragon_gpu_last_error());

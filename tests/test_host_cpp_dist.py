@@ -52,9 +52,11 @@ def _run(exe, *args):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["kh", "walls", "blast3d"])
+@pytest.mark.parametrize("case", ["kh", "walls", "blast3d", "fills"])
 @pytest.mark.parametrize("ranks", [1, 2, 3])
 def test_cpp_dist_threads_match_serial(dist_test, case, ranks):
+    """P slabs against the serial grid, bit for bit; "fills" carries device
+    user fills (NVRTC), one of them depending on the global x position."""
     if not cuda_ok():
         pytest.fail("CUDA device required")
     _run(dist_test[False], "threads", str(ranks), case)
