@@ -84,8 +84,11 @@ class SlabProgram:
     over the globally uncovered faces (BoundaryList.hpp:97-104), each masked to
     the faces of the global box the slab touches. An element periodic in x
     leaves an Ignore placeholder where the exchange runs (its y / z part stays
-    a device entry right after it). A final Ignore over every face keeps the
-    device from adding an implicit Outflow on faces between slabs.
+    a device entry right after it). A device user fill (DeviceGhostFill) stays
+    a device entry that fills the global faces the slab touches; the slab's
+    grid carries its global origin for the fill's coordinates. A final Ignore
+    over every face keeps the device from adding an implicit Outflow on faces
+    between slabs.
     """
 
     def __init__(self, blist: BoundaryList, rank: int, parts: int, dim: int):
